@@ -1,0 +1,315 @@
+"""Benchmark of the plain 3D FP32 stepper (SSP-RK3 step of WENO-Z / Godunov / cPML / ADE band).
+
+Workload (one GPU): a 500 x 400 x 200-cell shoebox (10 x 8 x 4 m at h = 0.02 m; 506 x 406 x 206
+padded cells), 5 seeded rigid box obstacles, 6 seeded passive ADE wall materials with 2 real
+poles + 2 complex pairs, a 20-cell cPML on one open face, a Gaussian pressure pulse (sigma = 2
+cells), c = 343 m/s, rho = 1.2 kg/m^3, CFL 0.5, 16 receivers. A step is one full SSP-RK3 time step
+of every cell. Inputs are synthetic and seeded. The field sets (3 x 4 x 183 MB) exceed L2, so no
+flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl fz|reference] [--room NX NY NZ]
+
+--impl reference times the CPU restatement of the reference update loop (the reference has no
+CPU solver of its own; its CUDA solver has no library interface) on bounded z-slab samples of
+the same room. Multi-GPU: independent replicas, one per rank (the north star is one GPU per
+solve; a 2nd GPU solves its own room), max time over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Gcell-updates/s (SSP-RK3 cell updates of the room per second, whole job)"
+UNIT = "Gcell/s"
+BYTES_PER_CELL_STEP = 131  # FP32: 4 fields x 4 B read/write over 3 stages (128 B) + 1 B class x 3
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="fz", choices=["fz", "reference"])
+    ap.add_argument("--room", type=int, nargs=3, default=[500, 400, 200])
+    ap.add_argument("--e2e-steps", type=int, default=12000, help="length of the end-to-end job")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    return ap.parse_args()
+
+
+def dist_setup(n):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return rank, world, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        import torch
+        pg.barrier()
+        torch.cuda.synchronize()
+
+
+def max_over_ranks(pg, x):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for nm, v in zip(names, r[4:8]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def workload(room):
+    from fases_b200 import materials as mats
+    from fases_b200 import scenes
+    b = scenes.benchmark_room(room_cells=tuple(room))
+    b["packed"] = mats.pack(b["materials"])
+    return b
+
+
+def make_solver(b, precision, capacity):
+    from fases_b200 import Solver, params
+    prm = params(h=b["h"], c=b["c"], rho=b["rho"], dt=b["dt"], pml=b["pml"], pml_cells=20, precision=precision,
+                 device=0)
+    s = Solver(prm)
+    sc = b["scene"]
+    s.load_geometry(sc.S, sc.oid)
+    m = b["packed"]
+    s.set_materials(m["Rinf"], m["A"], m["zeta"], m["B"], m["Cc"], m["alpha"], m["beta"])
+    s.set_receivers(b["receivers"], capacity)
+    s.set_fields(p=b["p0"])
+    return s
+
+
+def cpu_baseline(room, steps=6, threads=None):
+    """The FP64 CPU restatement on a z-slab sample of the room (same x-y extent, 24 cells high)."""
+    from fases_b200 import materials as mats
+    from fases_b200 import scenes
+    from oracle.oracle import Oracle
+    threads = threads or os.cpu_count()
+    slab = (room[0], room[1], 24)
+    b = scenes.benchmark_room(room_cells=slab, n_obstacles=0, n_receivers=2)
+    sc = b["scene"]
+    o = Oracle(sc.S, sc.oid, b["h"], b["c"], b["rho"], b["dt"], pml=b["pml"], materials=mats.pack(b["materials"]),
+               rec_cells=b["receivers"], max_steps=steps + 1)
+    o.set_fields(p=b["p0"])
+    o.run(1, threads=threads)
+    t = time.perf_counter()
+    o.run(steps, threads=threads)
+    dtm = time.perf_counter() - t
+    cells = slab[0] * slab[1] * slab[2]
+    return {"value": cells * steps / dtm / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{steps} FP64 steps of a {slab[0]}x{slab[1]}x{slab[2]}-cell z-slab of the room, "
+                      f"{threads} OpenMP threads, {dtm:.1f} s"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    room = args.room
+    from fases_b200 import materials as mats
+    from fases_b200 import scenes
+    from oracle.oracle import Oracle
+    threads = os.cpu_count()
+    slab = (room[0], room[1], 16)
+    b = scenes.benchmark_room(room_cells=slab, n_obstacles=0, n_receivers=2)
+    sc = b["scene"]
+    o = Oracle(sc.S, sc.oid, b["h"], b["c"], b["rho"], b["dt"], pml=b["pml"], materials=mats.pack(b["materials"]),
+               rec_cells=b["receivers"], max_steps=args.steps + args.warmup + 1)
+    o.set_fields(p=b["p0"])
+    o.run(args.warmup, threads=threads)
+    t = time.perf_counter()
+    o.run(args.steps, threads=threads)
+    dtm = time.perf_counter() - t
+    cells = slab[0] * slab[1] * slab[2]
+    v = cells * args.steps / dtm / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dtm * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": f"plain 3D shoebox {room[0]}x{room[1]}x{room[2]}, sampled as a {slab[2]}-cell z-slab",
+                   "room_cells": room, "sample_cells": list(slab)},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} FP64 steps of a {slab[0]}x{slab[1]}x{slab[2]}-cell z-slab per run"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local, pg = dist_setup(args.gpus)
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if world > 1:
+        os.environ["CUDA_VISIBLE_DEVICES"] = os.environ.get("CUDA_VISIBLE_DEVICES", str(local))
+    room = args.room
+    b = workload(room)
+    room_cells = int(room[0]) * int(room[1]) * int(room[2])
+    nsteps_total = args.warmup + args.steps
+    s = make_solver(b, args.precision, nsteps_total + 1)
+    info = s.info()
+    s.run(args.warmup)
+    barrier(pg)
+    s.profile(True)
+    with Clocks(local) as clk:
+        ms = s.run_timed(args.steps)
+    prof = s.profile_read()
+    s.profile(False)
+    ms = max_over_ranks(pg, ms)
+    stage_ms = sum(prof[k][0] for k in ("stage0", "stage1", "stage2"))
+    stage_launches = sum(prof[k][1] for k in ("stage0", "stage1", "stage2"))
+    launches = sum(v[1] for v in prof.values())
+    value = world * room_cells * args.steps / (ms / 1e3) / 1e9
+    # roofline of the dominant kernel (the fused stage kernel): algorithmic bytes per launch over
+    # its average launch time
+    bytes_per_launch = room_cells * BYTES_PER_CELL_STEP / 3.0
+    achieved = bytes_per_launch / (stage_ms / stage_launches / 1e3) / 1e9
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")) as f:
+            tr = json.load(f)
+            traffic = tr.get("dram_bytes_per_launch_full_room")
+    except Exception:
+        pass
+    ir_bench = s.ir()
+    finite = bool(np.all(np.isfinite(ir_bench)))
+    s.close()
+
+    # end to end through the public API: host buffers in, full job, receiver traces out
+    barrier(pg)
+    from fases_b200 import Solver, params
+    sc = b["scene"]
+    m = b["packed"]
+    ne = args.e2e_steps
+    t0 = time.perf_counter()
+    prm = params(h=b["h"], c=b["c"], rho=b["rho"], dt=b["dt"], pml=b["pml"], pml_cells=20, precision=args.precision)
+    e = Solver(prm)
+    e.load_geometry(sc.S, sc.oid)
+    e.set_materials(m["Rinf"], m["A"], m["zeta"], m["B"], m["Cc"], m["alpha"], m["beta"])
+    e.set_receivers(b["receivers"], ne)
+    e.set_fields(p=b["p0"])
+    e.run(ne)
+    ir = e.ir()
+    vel = e.vel()
+    t_e2e = time.perf_counter() - t0
+    e.close()
+    t_e2e = max_over_ranks(pg, t_e2e)
+    h2d = sc.S.nbytes + sc.oid.nbytes + b["p0"].nbytes + sum(np.asarray(v).nbytes for v in m.values())
+    d2h = ir.nbytes + vel.nbytes
+    e2e = {"value": world * room_cells * ne / t_e2e / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d / ne,
+           "d2h_bytes_per_step": d2h / ne, "steps": ne, "seconds": t_e2e,
+           "timer": "host wall clock around create, geometry/material/field upload, run, IR/VEL readback"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(room)
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {ex}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic (seeded)",
+            "config": {"workload": f"plain 3D shoebox {room[0]}x{room[1]}x{room[2]} cells (h=0.02 m), 5 rigid "
+                                   f"obstacles, 6 ADE walls (2 real + 2 complex poles), 20-cell cPML on one face, "
+                                   f"Gaussian pulse, 16 receivers, FP32 state / FP64 ADE",
+                       "room_cells": room_cells, "padded_cells": int(np.prod(info["dims"])),
+                       "band_cells": info["n_band"], "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (3 field sets of 4 x 183 MB)",
+                       "value_per_padded_cell": value * np.prod(info["dims"]) / room_cells},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "k_stage (fused WENO-Z/Godunov/RK/cPML/source), 131/3 B per room cell per launch",
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback"},
+            "kernel_ms": {k: v[0] / max(v[1], 1) for k, v in prof.items()},
+            "clocks": clk.summary(),
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "cpu_baseline": cpu,
+            "finite": finite,
+        }
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

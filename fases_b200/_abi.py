@@ -1,0 +1,127 @@
+"""ctypes binding of libfz.so (include/fz.h).
+
+The library is loaded from this package directory. There is no fallback: if libfz.so is missing
+or does not load, importing the solver raises, so a machine without the CUDA build fails loudly
+instead of silently running something else.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfz.so")
+
+FZ_OK = 0
+FZ_EINVAL = -1
+FZ_ENOMEM = -2
+FZ_ECUDA = -3
+FZ_EIO = -4
+FZ_EPARSE = -5
+FZ_ESTATE = -6
+FZ_ETIMEOUT = -7
+FZ_ENONFINITE = -8
+FZ_ENODEV = -9
+FZ_FP32 = 0
+FZ_FP64 = 1
+FZ_SRC_PCS = 0
+FZ_SRC_RICKER = 1
+FZ_SRC_SINE = 2
+
+ERROR_NAMES = {
+    FZ_EINVAL: "FZ_EINVAL", FZ_ENOMEM: "FZ_ENOMEM", FZ_ECUDA: "FZ_ECUDA", FZ_EIO: "FZ_EIO",
+    FZ_EPARSE: "FZ_EPARSE", FZ_ESTATE: "FZ_ESTATE", FZ_ETIMEOUT: "FZ_ETIMEOUT",
+    FZ_ENONFINITE: "FZ_ENONFINITE", FZ_ENODEV: "FZ_ENODEV",
+}
+
+
+class FzParams(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_int32),
+        ("precision", C.c_int32),
+        ("device", C.c_int32),
+        ("pml_cells", C.c_int32),
+        ("pml", C.c_int32 * 6),
+        ("h", C.c_double),
+        ("c", C.c_double),
+        ("rho", C.c_double),
+        ("dt", C.c_double),
+        ("tol_cells", C.c_double),
+    ]
+
+
+class FzError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERROR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+_P = C.c_void_p
+_i32 = C.c_int32
+_i64 = C.c_int64
+_dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int32)
+_i64p = C.POINTER(C.c_int64)
+_u8p = C.POINTER(C.c_uint8)
+
+# name -> (restype, argtypes); the exported surface of include/fz.h
+SIGNATURES = {
+    "fz_params_init": (C.c_int, [C.POINTER(FzParams)]),
+    "fz_create": (C.c_int, [C.POINTER(FzParams), C.POINTER(_P)]),
+    "fz_destroy": (None, [_P]),
+    "fz_load_geometry_raw": (C.c_int, [_P, _fp, _u8p, _i32, _i32, _i32]),
+    "fz_set_materials": (C.c_int, [_P, _i32, _i32, _i32, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
+    "fz_set_sources": (C.c_int, [_P, _i32, _ip, _dp, _i32, _dp, _dp, _i64]),
+    "fz_set_receivers": (C.c_int, [_P, _i32, _ip, _i64]),
+    "fz_set_fields": (C.c_int, [_P, _dp, _dp, _dp, _dp]),
+    "fz_run": (C.c_int, [_P, _i64]),
+    "fz_run_timed": (C.c_int, [_P, _i64, _dp]),
+    "fz_sync": (C.c_int, [_P, _i64]),
+    "fz_steps_done": (C.c_int, [_P, _i64p]),
+    "fz_get_ir": (C.c_int, [_P, _fp, _i64]),
+    "fz_get_ir64": (C.c_int, [_P, _dp, _i64]),
+    "fz_get_vel": (C.c_int, [_P, _fp, _i64]),
+    "fz_get_fields": (C.c_int, [_P, _dp, _dp, _dp, _dp]),
+    "fz_energy": (C.c_int, [_P, _dp]),
+    "fz_write_outputs": (C.c_int, [_P, C.c_char_p, _i32, C.c_char_p]),
+    "fz_info": (C.c_int, [_P, _ip, _i64p, _i64p]),
+    "fz_profile_enable": (C.c_int, [_P, _i32]),
+    "fz_profile_read": (C.c_int, [_P, _dp, _i64p, _i32]),
+    "fz_load_project": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, _i32, _i32,
+                                  C.POINTER(_P), _i64p]),
+    "fz_source_waveform": (C.c_int, [_i32, C.c_double, C.c_double, C.c_double, _i64, C.c_double,
+                                     C.c_double, _dp, _dp, _dp]),
+    "fz_last_error": (C.c_int, [_P, C.c_char_p, C.c_size_t]),
+    "fz_global_error": (C.c_int, [C.c_char_p, C.c_size_t]),
+}
+
+_lib = None
+
+
+def lib():
+    """The loaded libfz.so (raises OSError if it is not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"libfz.so not built at {LIB_PATH}: run fases_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def last_error(handle=None) -> str:
+    buf = C.create_string_buffer(4096)
+    if handle:
+        lib().fz_last_error(handle, buf, len(buf))
+    else:
+        lib().fz_global_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(rc, handle=None):
+    if rc != FZ_OK:
+        raise FzError(rc, last_error(handle))
+    return rc

@@ -1,0 +1,40 @@
+"""Build recipe for libfz.so, the sm_100a stepper behind include/fz.h.
+
+Compiles the CUDA kernels and the C++ host code in fases_b200/csrc/ with nvcc into
+fases_b200/libfz.so (in-tree, so the library travels with the repository to the GPU host).
+"""
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libfz.so")
+SOURCES = ["fz_kernels.cu", "fz_api.cpp", "fz_project.cpp"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _stale() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
+    deps.append(os.path.join(HERE, "..", "include", "fz.h"))
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and not _stale():
+        return LIB
+    cmd = ["nvcc", "-std=c++17", "-O3", *ARCH, "-lineinfo", "-shared",
+           "-Xcompiler", "-fPIC,-ffp-contract=off", "-I", os.path.join(HERE, "..", "include")]
+    if verbose:
+        cmd += ["-Xptxas", "-v"]
+    cmd += [os.path.join(CSRC, f) for f in SOURCES]
+    cmd += ["-o", LIB]
+    subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    import sys
+    print(build(force=True, verbose="-v" in sys.argv))

@@ -1,0 +1,901 @@
+// fz_api.cpp -- C ABI of the stepper (include/fz.h): handle lifetime, geometry and band setup,
+// materials, sources, receivers, the step loop with CUDA graphs, bounded waits and readback.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "fz_internal.h"
+#include "fz_kernels.h"
+
+using fz::XOFF;
+using fz::GHOST;
+
+namespace {
+thread_local std::string g_err;
+}
+
+namespace fzi {
+int set_error(fz_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  g_err = msg;
+  return code;
+}
+int set_global_error(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+int cuda_fail(fz_handle* h, cudaError_t e, const char* what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+  return set_error(h, (e == cudaErrorMemoryAllocation) ? FZ_ENOMEM : FZ_ECUDA, m);
+}
+}  // namespace fzi
+
+using fzi::cuda_fail;
+using fzi::set_error;
+
+#define FZ_CUDA(h, call, what)                       \
+  do {                                               \
+    cudaError_t e__ = (call);                        \
+    if (e__ != cudaSuccess) return cuda_fail(h, e__, what); \
+  } while (0)
+
+namespace {
+
+template <class T>
+void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+int64_t dev_index(const fz_handle* h, int i, int j, int k) {
+  return (int64_t)XOFF + i + h->Sx * ((int64_t)j + (int64_t)h->Ny * k);
+}
+
+int64_t ref_index(const fz_handle* h, int i, int j, int k) {
+  return (int64_t)i + (int64_t)h->Nx * ((int64_t)j + (int64_t)h->Ny * k);
+}
+
+void free_graphs(fz_handle* h) {
+  for (auto& g : h->graph) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
+}
+
+void free_device(fz_handle* h) {
+  free_graphs(h);
+  for (auto& set : h->U)
+    for (auto& f : set) dfree(f);
+  dfree(h->d_cls);
+  for (auto& p : h->d_pml_coef) dfree(p);
+  for (auto& p : h->d_psi) dfree(p);
+  dfree(h->d_bcell);
+  dfree(h->d_bcorner);
+  dfree(h->d_bgeo);
+  dfree(h->d_bnrm);
+  dfree(h->d_bmat);
+  for (auto& set : h->d_ade)
+    for (auto& p : set) dfree(p);
+  dfree(h->d_mat);
+  dfree(h->d_src_cell);
+  dfree(h->d_src_coef);
+  dfree(h->d_src_freq);
+  dfree(h->d_us);
+  dfree(h->d_rec_cell);
+  dfree(h->d_ir);
+  dfree(h->d_vel);
+}
+
+// Per-axis cPML coefficient table, restated from functions3D.cuh:689-723 (evaluated once here in
+// FP64 instead of powf/expf/logf per cell and stage).
+template <class R>
+std::vector<fz::PmlCoef<R>> pml_table(int N, int lo, int hi, const fz_params& p) {
+  const int d = p.pml_cells, ng = GHOST;
+  const double lnR0 = std::log(1.0 / 1e-7), m = 2.0;
+  const double kappa_max = 5.0, alpha_max = M_PI * 20.0, alpha_min = 0.1 * alpha_max;
+  const double pref = 0.5 * p.c * (m + 1.0) * lnR0 / ((double)d * p.h);
+  std::vector<fz::PmlCoef<R>> t((size_t)N);
+  for (int i = 0; i < N; i++) {
+    const double xm = std::min(1.0, std::max(0.0, ((double)(ng + d) - i) / d));
+    const double xp = std::min(1.0, std::max(0.0, (i - ((double)(N - 1 - ng) - d)) / d));
+    const double sig = lo * pref * std::pow(xm, m) + hi * pref * std::pow(xp, m);
+    const double dep = lo * xm + hi * xp;
+    const double kap = 1.0 + (kappa_max - 1.0) * std::pow(dep, m);
+    const double alp = alpha_min + (alpha_max - alpha_min) * (1.0 - dep);
+    const bool in = (lo && i >= ng && i < ng + d) || (hi && i >= N - ng - d && i <= N - 1 - ng);
+    fz::PmlCoef<R> c;
+    c.tile = in ? ((i < ng + d) ? (i - ng) : (i - (N - ng - d) + d)) : -1;
+    c.kinv1 = (R)(1.0 / kap - 1.0);
+    const double b = std::exp(-(alp + sig / kap) * p.dt);
+    c.b = (R)b;
+    c.ca = (R)((sig > 0.0) ? (sig / (kap * (sig + kap * alp))) * (b - 1.0) : 0.0);
+    t[(size_t)i] = c;
+  }
+  return t;
+}
+
+template <class R>
+int upload_pml(fz_handle* h) {
+  const fz_params& p = h->prm;
+  // axis x: L (lo) / R (hi); y: B (lo) / F (hi); z: D (lo) / U (hi)
+  const int lo[3] = {p.pml[3] != 0, p.pml[5] != 0, p.pml[1] != 0};
+  const int hi[3] = {p.pml[2] != 0, p.pml[4] != 0, p.pml[0] != 0};
+  const int n[3] = {h->Nx, h->Ny, h->Nz};
+  typedef typename fz::Pair<R>::T P;
+  const int64_t d2 = 2 * (int64_t)p.pml_cells;
+  const int64_t tile_n[3] = {d2 * h->Ny * h->Nz, (int64_t)h->Nx * d2 * h->Nz, (int64_t)h->Nx * h->Ny * d2};
+  for (int a = 0; a < 3; a++) {
+    auto t = pml_table<R>(n[a], lo[a], hi[a], p);
+    FZ_CUDA(h, cudaMalloc(&h->d_pml_coef[a], t.size() * sizeof(t[0])), "cudaMalloc(pml table)");
+    FZ_CUDA(h, cudaMemcpy(h->d_pml_coef[a], t.data(), t.size() * sizeof(t[0]), cudaMemcpyHostToDevice),
+            "cudaMemcpy(pml table)");
+    if (lo[a] || hi[a]) {
+      FZ_CUDA(h, cudaMalloc(&h->d_psi[a], (size_t)tile_n[a] * sizeof(P)), "cudaMalloc(psi)");
+      FZ_CUDA(h, cudaMemset(h->d_psi[a], 0, (size_t)tile_n[a] * sizeof(P)), "cudaMemset(psi)");
+    }
+  }
+  return FZ_OK;
+}
+
+// Immersed band list (functions3D.cuh:462-512 evaluated once per cell instead of per stage).
+// Band cells: interior cells [3, N-3)^3 with oid not in {0, 0xFF} (the BC kernel's condition,
+// functions3D.cuh:464-478, with bmap >= 0 <=> oid not in {0, 0xFF}, common/filterABC.h:99-105).
+template <class R>
+int build_band(fz_handle* h) {
+  const int Nx = h->Nx, Ny = h->Ny, Nz = h->Nz;
+  const double hh = h->prm.h, tol = h->prm.tol_cells * h->prm.h;
+  const float* S = h->S_host.data();
+  const uint8_t* oid = h->oid_host.data();
+  std::vector<int64_t> cell, corner;
+  std::vector<R> geo, nrm;
+  std::vector<int32_t> mat;
+  h->band_cell_ref.clear();
+  auto Sat = [&](int i, int j, int k) { return (double)S[ref_index(h, i, j, k)]; };
+  for (int k = GHOST; k < Nz - GHOST; k++)
+    for (int j = GHOST; j < Ny - GHOST; j++)
+      for (int i = GHOST; i < Nx - GHOST; i++) {
+        const int64_t rc = ref_index(h, i, j, k);
+        const uint8_t o = oid[rc];
+        if (o == 0 || o == 0xFF) continue;
+        const double s = S[rc];
+        const double gx = (Sat(i + 1, j, k) - Sat(i - 1, j, k)) * (0.5 / hh);
+        const double gy = (Sat(i, j + 1, k) - Sat(i, j - 1, k)) * (0.5 / hh);
+        const double gz = (Sat(i, j, k + 1) - Sat(i, j, k - 1)) * (0.5 / hh);
+        const double gn = std::max(std::sqrt(gx * gx + gy * gy + gz * gz), 1e-12);
+        const double nx = -gx / gn, ny = -gy / gn, nz = -gz / gn;
+        const double Cx = (i + 0.5) * hh, Cy = (j + 0.5) * hh, Cz = (k + 0.5) * hh;
+        const double Wx = Cx + s * nx, Wy = Cy + s * ny, Wz = Cz + s * nz;
+        const double l = s + 2.0 * hh;
+        const double Dx = Wx - l * nx, Dy = Wy - l * ny, Dz = Wz - l * nz;
+        const double fx = Dx / hh - 0.5, fy = Dy / hh - 0.5, fzz = Dz / hh - 0.5;
+        int bi = (int)std::floor(fx), bj = (int)std::floor(fy), bk = (int)std::floor(fzz);
+        bi = std::max(0, std::min(bi, Nx - 2));
+        bj = std::max(0, std::min(bj, Ny - 2));
+        bk = std::max(0, std::min(bk, Nz - 2));
+        double chi;
+        if (s >= tol) chi = 0.0;
+        else if (s <= hh) chi = 1.0;
+        else {
+          const double r = (s - hh) / (tol - hh);
+          chi = 1.0 - r * r * (3.0 - 2.0 * r);
+        }
+        cell.push_back(dev_index(h, i, j, k));
+        corner.push_back(dev_index(h, bi, bj, bk));
+        geo.push_back((R)(fx - bi));
+        geo.push_back((R)(fy - bj));
+        geo.push_back((R)(fzz - bk));
+        geo.push_back((R)chi);
+        nrm.push_back((R)nx);
+        nrm.push_back((R)ny);
+        nrm.push_back((R)nz);
+        nrm.push_back((R)0);
+        mat.push_back((int32_t)o - 1);
+        h->band_cell_ref.push_back(rc);
+      }
+  h->nB = (int64_t)cell.size();
+  h->band_mat = mat;
+  if (h->nB == 0) return FZ_OK;
+  FZ_CUDA(h, cudaMalloc(&h->d_bcell, cell.size() * 8), "cudaMalloc(band)");
+  FZ_CUDA(h, cudaMalloc(&h->d_bcorner, corner.size() * 8), "cudaMalloc(band)");
+  FZ_CUDA(h, cudaMalloc(&h->d_bgeo, geo.size() * sizeof(R)), "cudaMalloc(band)");
+  FZ_CUDA(h, cudaMalloc(&h->d_bnrm, nrm.size() * sizeof(R)), "cudaMalloc(band)");
+  FZ_CUDA(h, cudaMalloc(&h->d_bmat, mat.size() * 4), "cudaMalloc(band)");
+  FZ_CUDA(h, cudaMemcpy(h->d_bcell, cell.data(), cell.size() * 8, cudaMemcpyHostToDevice), "band H2D");
+  FZ_CUDA(h, cudaMemcpy(h->d_bcorner, corner.data(), corner.size() * 8, cudaMemcpyHostToDevice), "band H2D");
+  FZ_CUDA(h, cudaMemcpy(h->d_bgeo, geo.data(), geo.size() * sizeof(R), cudaMemcpyHostToDevice), "band H2D");
+  FZ_CUDA(h, cudaMemcpy(h->d_bnrm, nrm.data(), nrm.size() * sizeof(R), cudaMemcpyHostToDevice), "band H2D");
+  FZ_CUDA(h, cudaMemcpy(h->d_bmat, mat.data(), mat.size() * 4, cudaMemcpyHostToDevice), "band H2D");
+  return FZ_OK;
+}
+
+template <class R>
+int finalize(fz_handle* h) {
+  if (h->finalized) return FZ_OK;
+  if (!h->have_geometry) return set_error(h, FZ_ESTATE, "fz_run before fz_load_geometry_raw");
+  // materials: every band cell must name a loaded material (the reference indexes R_inf[oid-1]
+  // without a check, main3D.cu:579 + functions3D.cuh:525)
+  for (size_t b = 0; b < h->band_mat.size(); b++)
+    if (h->band_mat[b] >= h->nMat)
+      return set_error(h, FZ_EINVAL,
+                       "band cell " + std::to_string(h->band_cell_ref[b]) + " has material id " +
+                           std::to_string(h->band_mat[b] + 1) + " but only " + std::to_string(h->nMat) +
+                           " materials are set");
+  const int nm = std::max(1, h->nMat);
+  if (h->Rinf.empty()) {
+    h->K = 1;
+    h->L = 1;
+    h->Rinf.assign(nm, 0.0);
+    h->A.assign(nm, 0.0); h->zeta.assign(nm, 0.0);
+    h->B.assign(nm, 0.0); h->C.assign(nm, 0.0); h->alpha.assign(nm, 0.0); h->beta.assign(nm, 0.0);
+  }
+  std::vector<double> packed;
+  for (auto* v : {&h->Rinf, &h->A, &h->zeta, &h->B, &h->C, &h->alpha, &h->beta})
+    packed.insert(packed.end(), v->begin(), v->end());
+  FZ_CUDA(h, cudaMalloc(&h->d_mat, packed.size() * 8), "cudaMalloc(materials)");
+  FZ_CUDA(h, cudaMemcpy(h->d_mat, packed.data(), packed.size() * 8, cudaMemcpyHostToDevice), "materials H2D");
+  // ADE states (3 rotating sets, main3D.cu:683-709), zeroed
+  if (h->nB > 0) {
+    const size_t nk = (size_t)h->nB * h->K, nl = (size_t)h->nB * h->L;
+    for (int s = 0; s < 3; s++) {
+      FZ_CUDA(h, cudaMalloc(&h->d_ade[s][0], nk * 8), "cudaMalloc(ADE)");
+      FZ_CUDA(h, cudaMalloc(&h->d_ade[s][1], nl * 8), "cudaMalloc(ADE)");
+      FZ_CUDA(h, cudaMalloc(&h->d_ade[s][2], nl * 8), "cudaMalloc(ADE)");
+      FZ_CUDA(h, cudaMemset(h->d_ade[s][0], 0, nk * 8), "cudaMemset(ADE)");
+      FZ_CUDA(h, cudaMemset(h->d_ade[s][1], 0, nl * 8), "cudaMemset(ADE)");
+      FZ_CUDA(h, cudaMemset(h->d_ade[s][2], 0, nl * 8), "cudaMemset(ADE)");
+    }
+  }
+  // sources
+  if (h->nsrc > 0) {
+    std::vector<int64_t> cells;
+    std::vector<R> coef, freq;
+    const double As = 6.0 * h->prm.h * h->prm.h;
+    for (int s = 0; s < h->nsrc; s++) {
+      const int i = h->src_ijk[3 * s], j = h->src_ijk[3 * s + 1], k = h->src_ijk[3 * s + 2];
+      const int64_t g = dev_index(h, i, j, k);
+      cells.push_back(g);
+      coef.push_back((R)(h->prm.dt * h->prm.c * h->prm.c * h->src_val[s] * h->prm.rho * As /
+                         (h->prm.h * h->prm.h * h->prm.h)));
+      freq.push_back((R)(h->src_freq.empty() ? 0.0 : h->src_freq[s]));
+      h->cls_host[g] |= fz::CLS_SOURCE;
+    }
+    FZ_CUDA(h, cudaMalloc(&h->d_src_cell, cells.size() * 8), "cudaMalloc(src)");
+    FZ_CUDA(h, cudaMalloc(&h->d_src_coef, coef.size() * sizeof(R)), "cudaMalloc(src)");
+    FZ_CUDA(h, cudaMalloc(&h->d_src_freq, freq.size() * sizeof(R)), "cudaMalloc(src)");
+    FZ_CUDA(h, cudaMemcpy(h->d_src_cell, cells.data(), cells.size() * 8, cudaMemcpyHostToDevice), "src H2D");
+    FZ_CUDA(h, cudaMemcpy(h->d_src_coef, coef.data(), coef.size() * sizeof(R), cudaMemcpyHostToDevice), "src H2D");
+    FZ_CUDA(h, cudaMemcpy(h->d_src_freq, freq.data(), freq.size() * sizeof(R), cudaMemcpyHostToDevice), "src H2D");
+    if (!h->u_s.empty()) {
+      std::vector<R> us(h->u_s.begin(), h->u_s.end());
+      h->n_us = (int64_t)us.size();
+      FZ_CUDA(h, cudaMalloc(&h->d_us, us.size() * sizeof(R)), "cudaMalloc(u_s)");
+      FZ_CUDA(h, cudaMemcpy(h->d_us, us.data(), us.size() * sizeof(R), cudaMemcpyHostToDevice), "u_s H2D");
+    }
+    FZ_CUDA(h, cudaMemcpy(h->d_cls, h->cls_host.data(), h->cls_host.size(), cudaMemcpyHostToDevice), "cls H2D");
+  }
+  // receivers
+  if (h->nrec > 0) {
+    std::vector<int64_t> cells;
+    for (int r = 0; r < h->nrec; r++)
+      cells.push_back(dev_index(h, h->rec_ijk[3 * r], h->rec_ijk[3 * r + 1], h->rec_ijk[3 * r + 2]));
+    FZ_CUDA(h, cudaMalloc(&h->d_rec_cell, cells.size() * 8), "cudaMalloc(rec)");
+    FZ_CUDA(h, cudaMemcpy(h->d_rec_cell, cells.data(), cells.size() * 8, cudaMemcpyHostToDevice), "rec H2D");
+    const size_t n = (size_t)h->nrec * (size_t)std::max<int64_t>(1, h->rec_cap);
+    FZ_CUDA(h, cudaMalloc(&h->d_ir, n * 8), "cudaMalloc(ir)");
+    FZ_CUDA(h, cudaMalloc(&h->d_vel, n * 3 * 8), "cudaMalloc(vel)");
+    FZ_CUDA(h, cudaMemset(h->d_ir, 0, n * 8), "cudaMemset(ir)");
+    FZ_CUDA(h, cudaMemset(h->d_vel, 0, n * 3 * 8), "cudaMemset(vel)");
+  }
+  // launch geometry: z chunks so that the grid fills the GPU several times over
+  int occ = 1;
+  FZ_CUDA(h, fz::stage_occupancy<R>(&occ), "occupancy");
+  occ = std::max(1, occ);
+  const int ntx = (h->Nx - 2 * GHOST + fz::TX - 1) / fz::TX;
+  const int nty = (h->Ny - 2 * GHOST + fz::TY - 1) / fz::TY;
+  const int nzi = h->Nz - 2 * GHOST;
+  const int64_t slots = (int64_t)h->nsm * occ;
+  int nkz = (int)std::max<int64_t>(1, (4 * slots + (int64_t)ntx * nty - 1) / ((int64_t)ntx * nty));
+  nkz = std::min(nkz, std::max(1, nzi / 8));
+  h->kz_chunk = (nzi + nkz - 1) / nkz;
+  nkz = (nzi + h->kz_chunk - 1) / h->kz_chunk;
+  h->stage_grid = dim3((unsigned)ntx, (unsigned)nty, (unsigned)nkz);
+  h->finalized = true;
+  return FZ_OK;
+}
+
+template <class R>
+fz::StageArgs<R> stage_args(fz_handle* h, int stage) {
+  typedef typename fz::Pair<R>::T P;
+  fz::StageArgs<R> a;
+  std::memset(&a, 0, sizeof(a));
+  R* const* u0 = (R* const*)h->U[h->i0];
+  R* const* u1 = (R* const*)h->U[h->i1];
+  R* const* u2 = (R* const*)h->U[h->i2];
+  R* const* in = (stage == 0) ? u0 : (stage == 1) ? u1 : u2;
+  R* const* out = (stage == 1) ? u2 : u1;
+  a.pi = in[0]; a.ui = in[1]; a.vi = in[2]; a.wi = in[3];
+  a.pb = u0[0]; a.ub = u0[1]; a.vb = u0[2]; a.wb = u0[3];
+  a.po = out[0]; a.uo = out[1]; a.vo = out[2]; a.wo = out[3];
+  a.cls = h->d_cls;
+  a.Nx = h->Nx; a.Ny = h->Ny; a.Nz = h->Nz;
+  a.Sx = h->Sx; a.plane = h->plane;
+  a.kz_chunk = h->kz_chunk;
+  const fz_params& p = h->prm;
+  a.dt_h = (R)(p.dt / p.h);
+  a.frc2 = (R)(0.5 * p.rho * p.c * p.c);
+  a.firho = (R)(0.5 / p.rho);
+  a.fc = (R)(0.5 * p.c);
+  a.inv_h = (R)(1.0 / p.h);
+  const double w = (stage == 0) ? 1.0 : (stage == 1) ? 0.25 : 2.0 / 3.0;
+  a.wdt = (R)(w * p.dt);
+  a.pml_on = h->pml_on ? 1 : 0;
+  a.pml_d2 = 2 * p.pml_cells;
+  a.pcx = (const fz::PmlCoef<R>*)h->d_pml_coef[0];
+  a.pcy = (const fz::PmlCoef<R>*)h->d_pml_coef[1];
+  a.pcz = (const fz::PmlCoef<R>*)h->d_pml_coef[2];
+  a.psix = (P*)h->d_psi[0];
+  a.psiy = (P*)h->d_psi[1];
+  a.psiz = (P*)h->d_psi[2];
+  a.nsrc = h->nsrc;
+  a.src_cell = h->d_src_cell;
+  a.src_coef = (const R*)h->d_src_coef;
+  a.src_freq = (const R*)h->d_src_freq;
+  a.u_s = (const R*)h->d_us;
+  a.n_us = h->n_us;
+  a.src_opt = h->src_opt;
+  a.src_w = (R)w;
+  a.nn_mul = 2;
+  a.nn_add = (stage == 0) ? 0 : (stage == 1) ? 2 : 1;  // main3D.cu:1288, 1296, 1304
+  a.half_dt = (R)(0.5 * p.dt);
+  a.step = h->d_step;
+  return a;
+}
+
+template <class R>
+fz::BandArgs<R> band_args(fz_handle* h, int stage) {
+  fz::BandArgs<R> b;
+  std::memset(&b, 0, sizeof(b));
+  R* const* u0 = (R* const*)h->U[h->i0];
+  R* const* u1 = (R* const*)h->U[h->i1];
+  R* const* u2 = (R* const*)h->U[h->i2];
+  R* const* in = (stage == 0) ? u0 : (stage == 1) ? u1 : u2;
+  R* const* out = (stage == 1) ? u2 : u1;
+  b.nB = h->nB;
+  b.cell = h->d_bcell; b.corner = h->d_bcorner;
+  b.geo = (const R*)h->d_bgeo; b.nrm = (const R*)h->d_bnrm; b.mat = h->d_bmat;
+  b.pi = in[0]; b.ui = in[1]; b.vi = in[2]; b.wi = in[3];
+  b.po = out[0]; b.uo = out[1]; b.vo = out[2]; b.wo = out[3];
+  b.Sx = h->Sx; b.plane = h->plane;
+  b.Z0 = h->prm.rho * h->prm.c;
+  b.dt = h->prm.dt;
+  // ADE stage coefficients (a, b, c) and state roles (left, middle, right), main3D.cu:1290-1306
+  static const double abc[3][3] = {{0, 1, 1}, {3, 1, 4}, {1, 2, 3}};
+  b.a_ssp = abc[stage][0]; b.b_ssp = abc[stage][1]; b.inv_c_ssp = 1.0 / abc[stage][2];
+  int L_, M_, R_;
+  if (stage == 0) { L_ = h->ph_cur; M_ = h->ph_old; R_ = h->ph_old; }
+  else if (stage == 1) { L_ = h->ph_nu; M_ = h->ph_old; R_ = h->ph_cur; }
+  else { L_ = h->ph_cur; M_ = h->ph_old; R_ = h->ph_nu; }
+  b.phL = h->d_ade[L_][0]; b.phM = h->d_ade[M_][0]; b.phR = h->d_ade[R_][0];
+  b.s1L = h->d_ade[L_][1]; b.s1M = h->d_ade[M_][1]; b.s1R = h->d_ade[R_][1];
+  b.s2L = h->d_ade[L_][2]; b.s2M = h->d_ade[M_][2]; b.s2R = h->d_ade[R_][2];
+  b.K = h->K; b.L = h->L;
+  const int nm = std::max(1, h->nMat);
+  const double* m = h->d_mat;
+  b.Rinf = m; m += nm;
+  b.A = m; m += (size_t)nm * h->K;
+  b.zeta = m; m += (size_t)nm * h->K;
+  b.B = m; m += (size_t)nm * h->L;
+  b.C = m; m += (size_t)nm * h->L;
+  b.alpha = m; m += (size_t)nm * h->L;
+  b.beta = m;
+  return b;
+}
+
+struct Timer {
+  fz_handle* h;
+  int kind;
+  cudaEvent_t a = nullptr, b = nullptr;
+  Timer(fz_handle* h_, int k) : h(h_), kind(k) {
+    if (!h->profiling) return;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, h->stream);
+  }
+  ~Timer() {
+    if (!h->profiling) return;
+    cudaEventRecord(b, h->stream);
+    h->timings.push_back({kind, a, b});
+  }
+};
+
+// One time step (main3D.cu:1280-1319 + receivers 1399-1414).
+template <class R>
+cudaError_t enqueue_step(fz_handle* h) {
+  cudaError_t e;
+  for (int st = 0; st < 3; st++) {
+    {
+      Timer t(h, st);
+      e = fz::launch_stage<R>(st, stage_args<R>(h, st), h->stage_grid, h->stream);
+      if (e != cudaSuccess) return e;
+    }
+    if (h->nB > 0) {
+      Timer t(h, 3);
+      e = fz::launch_band<R>(band_args<R>(h, st), h->stream);
+      if (e != cudaSuccess) return e;
+    }
+  }
+  {
+    Timer t(h, 4);
+    R* const* u1 = (R* const*)h->U[h->i1];
+    e = fz::launch_receivers<R>(u1[0], u1[1], u1[2], u1[3], h->d_rec_cell, h->nrec, h->d_ir, h->d_vel,
+                                h->rec_cap, h->d_step, h->stream);
+    if (e != cudaSuccess) return e;
+  }
+  std::swap(h->i0, h->i1);
+  std::swap(h->ph_old, h->ph_cur);
+  return cudaSuccess;
+}
+
+template <class R>
+int run_steps(fz_handle* h, int64_t nsteps) {
+  int rc = finalize<R>(h);
+  if (rc != FZ_OK) return rc;
+  int64_t done = 0;
+  const int G = h->graph_steps;
+  if (!h->profiling && G > 0 && (G % 2) == 0) {
+    while (nsteps - done >= G) {
+      const int par = h->i0;  // buffer assignment repeats every 2 steps
+      if (!h->graph[par]) {
+        cudaGraph_t g = nullptr;
+        FZ_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        cudaError_t e = cudaSuccess;
+        for (int s = 0; s < G && e == cudaSuccess; s++) e = enqueue_step<R>(h);
+        cudaError_t e2 = cudaStreamEndCapture(h->stream, &g);
+        if (e != cudaSuccess) return cuda_fail(h, e, "capture step");
+        if (e2 != cudaSuccess) return cuda_fail(h, e2, "end capture");
+        e = cudaGraphInstantiate(&h->graph[par], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return cuda_fail(h, e, "graph instantiate");
+        // capture advanced the host-side rotation by G (even) steps: back where it started
+      }
+      FZ_CUDA(h, cudaGraphLaunch(h->graph[par], h->stream), "graph launch");
+      done += G;
+      h->steps_enqueued += G;
+    }
+  }
+  for (; done < nsteps; done++) {
+    cudaError_t e = enqueue_step<R>(h);
+    if (e != cudaSuccess) return cuda_fail(h, e, "step launch");
+    h->steps_enqueued += 1;
+  }
+  return FZ_OK;
+}
+
+template <class R>
+int load_geometry(fz_handle* h, const float* S, const uint8_t* oid, int Nx, int Ny, int Nz) {
+  free_device(h);
+  h->finalized = false;
+  h->Nx = Nx; h->Ny = Ny; h->Nz = Nz;
+  h->Sx = ((int64_t)Nx + XOFF + 31) / 32 * 32;
+  h->plane = h->Sx * Ny;
+  h->ncell_dev = h->plane * Nz;
+  if (h->Lx == 0) { h->Lx = Nx * h->prm.h; h->Ly = Ny * h->prm.h; h->Lz = Nz * h->prm.h; }
+  const size_t N = (size_t)Nx * Ny * Nz;
+  h->S_host.assign(S, S + N);
+  h->oid_host.assign(oid, oid + N);
+  const size_t bytes = (size_t)h->ncell_dev * sizeof(R);
+  for (int s = 0; s < 3; s++)
+    for (int f = 0; f < 4; f++) {
+      FZ_CUDA(h, cudaMalloc(&h->U[s][f], bytes), "cudaMalloc(fields)");
+      FZ_CUDA(h, cudaMemset(h->U[s][f], 0, bytes), "cudaMemset(fields)");
+    }
+  // cell classes: update where the stage kernels would not return early (functions3D.cuh:1091-1097)
+  h->cls_host.assign((size_t)h->ncell_dev, 0);
+  int64_t nup = 0;
+  const float hf = (float)h->prm.h;
+  for (int k = GHOST; k < Nz - GHOST; k++)
+    for (int j = GHOST; j < Ny - GHOST; j++)
+      for (int i = GHOST; i < Nx - GHOST; i++)
+        if (!(S[ref_index(h, i, j, k)] < hf)) {
+          h->cls_host[(size_t)dev_index(h, i, j, k)] = fz::CLS_UPDATE;
+          nup++;
+        }
+  h->n_update = nup;
+  FZ_CUDA(h, cudaMalloc(&h->d_cls, h->cls_host.size()), "cudaMalloc(cls)");
+  FZ_CUDA(h, cudaMemcpy(h->d_cls, h->cls_host.data(), h->cls_host.size(), cudaMemcpyHostToDevice), "cls H2D");
+  h->pml_on = false;
+  for (int f = 0; f < 6; f++) h->pml_on = h->pml_on || (h->prm.pml[f] != 0);
+  int rc = upload_pml<R>(h);
+  if (rc != FZ_OK) return rc;
+  rc = build_band<R>(h);
+  if (rc != FZ_OK) return rc;
+  h->i0 = 0; h->i1 = 1; h->i2 = 2;
+  h->ph_old = 0; h->ph_cur = 1; h->ph_nu = 2;
+  FZ_CUDA(h, cudaMemset(h->d_step, 0, sizeof(int64_t)), "reset step");
+  h->steps_enqueued = 0;
+  h->have_geometry = true;
+  return FZ_OK;
+}
+
+template <class R>
+int get_fields(fz_handle* h, double* p, double* u, double* v, double* w) {
+  const size_t rowb = (size_t)h->Nx * sizeof(R);
+  const size_t N = (size_t)h->Nx * h->Ny * h->Nz;
+  std::vector<R> tmp(N);
+  double* outs[4] = {p, u, v, w};
+  for (int f = 0; f < 4; f++) {
+    if (!outs[f]) continue;
+    const R* src = (const R*)h->U[h->i0][f] + XOFF;
+    FZ_CUDA(h, cudaMemcpy2D(tmp.data(), rowb, src, (size_t)h->Sx * sizeof(R), rowb,
+                            (size_t)h->Ny * h->Nz, cudaMemcpyDeviceToHost), "fields D2H");
+    for (size_t c = 0; c < N; c++) outs[f][c] = (double)tmp[c];
+  }
+  return FZ_OK;
+}
+
+template <class R>
+int set_fields(fz_handle* h, const double* p, const double* u, const double* v, const double* w) {
+  const size_t rowb = (size_t)h->Nx * sizeof(R);
+  const size_t N = (size_t)h->Nx * h->Ny * h->Nz;
+  std::vector<R> tmp(N);
+  const double* ins[4] = {p, u, v, w};
+  for (int f = 0; f < 4; f++) {
+    R* dst = (R*)h->U[h->i0][f] + XOFF;
+    if (!ins[f]) {
+      FZ_CUDA(h, cudaMemset(h->U[h->i0][f], 0, (size_t)h->ncell_dev * sizeof(R)), "fields zero");
+      continue;
+    }
+    for (size_t c = 0; c < N; c++) tmp[c] = (R)ins[f][c];
+    FZ_CUDA(h, cudaMemcpy2D(dst, (size_t)h->Sx * sizeof(R), tmp.data(), rowb, rowb,
+                            (size_t)h->Ny * h->Nz, cudaMemcpyHostToDevice), "fields H2D");
+  }
+  return FZ_OK;
+}
+
+template <class R>
+int energy(fz_handle* h, double* E) {
+  FZ_CUDA(h, cudaMemsetAsync(h->d_scratch, 0, sizeof(double), h->stream), "energy reset");
+  R* const* u0 = (R* const*)h->U[h->i0];
+  const double rc2 = h->prm.rho * h->prm.c * h->prm.c;
+  FZ_CUDA(h, fz::launch_energy<R>(u0[0], u0[1], u0[2], u0[3], h->ncell_dev, 1.0 / rc2, h->prm.rho,
+                                  h->d_scratch, h->nsm, h->stream), "energy launch");
+  int rc = fz_sync(h, 0);
+  if (rc != FZ_OK) return rc;
+  FZ_CUDA(h, cudaMemcpy(E, h->d_scratch, sizeof(double), cudaMemcpyDeviceToHost), "energy D2H");
+  return FZ_OK;
+}
+
+bool check_handle(fz_handle* h) { return h != nullptr; }
+
+}  // namespace
+
+// ==========================================================================================
+// C ABI
+// ==========================================================================================
+extern "C" {
+
+int fz_params_init(fz_params* p) {
+  if (!p) return fzi::set_global_error(FZ_EINVAL, "fz_params_init: NULL");
+  std::memset(p, 0, sizeof(*p));
+  p->abi_version = FZ_ABI_VERSION;
+  p->precision = FZ_FP32;
+  p->device = 0;
+  p->pml_cells = 20;
+  p->h = 0.02;
+  // main3D.cu:450-456 at 20 degC, in the reference's float arithmetic
+  const float Temp = 20.0f + 273.15f;
+  p->c = (double)std::sqrt(1.4f * 287.05f * Temp);
+  p->rho = (double)1.225f;
+  p->dt = 0.5 * p->h / p->c;
+  p->tol_cells = 3.0;
+  return FZ_OK;
+}
+
+int fz_create(const fz_params* p, fz_handle** out) {
+  if (!p || !out) return fzi::set_global_error(FZ_EINVAL, "fz_create: NULL argument");
+  *out = nullptr;
+  if (p->abi_version != FZ_ABI_VERSION)
+    return fzi::set_global_error(FZ_EINVAL, "fz_create: abi_version mismatch");
+  if (!(p->h > 0) || !(p->c > 0) || !(p->rho > 0) || !(p->dt > 0) || p->pml_cells < 1 ||
+      (p->precision != FZ_FP32 && p->precision != FZ_FP64) || !(p->tol_cells > 1.0))
+    return fzi::set_global_error(FZ_EINVAL, "fz_create: invalid parameter (h, c, rho, dt > 0; pml_cells >= 1; "
+                                            "precision FZ_FP32/FZ_FP64; tol_cells > 1)");
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev <= 0)
+    return fzi::set_global_error(FZ_ENODEV, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  if (p->device < 0 || p->device >= ndev) return fzi::set_global_error(FZ_ENODEV, "fz_create: bad device ordinal");
+  fz_handle* h = new (std::nothrow) fz_handle();
+  if (!h) return fzi::set_global_error(FZ_ENOMEM, "fz_create: out of host memory");
+  h->prm = *p;
+  h->device = p->device;
+  h->fp64 = (p->precision == FZ_FP64);
+  h->rsize = h->fp64 ? 8 : 4;
+  e = cudaSetDevice(h->device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = h->fp64 ? fz::stage_setup<double>() : fz::stage_setup<float>();
+  if (e == cudaSuccess) e = cudaMalloc(&h->d_step, sizeof(int64_t));
+  if (e == cudaSuccess) e = cudaMemset(h->d_step, 0, sizeof(int64_t));
+  if (e == cudaSuccess) e = cudaMalloc(&h->d_scratch, 64);
+  if (e != cudaSuccess) {
+    int rc = fzi::set_global_error(FZ_ECUDA, std::string("fz_create: ") + cudaGetErrorString(e));
+    fz_destroy(h);
+    return rc;
+  }
+  *out = h;
+  return FZ_OK;
+}
+
+void fz_destroy(fz_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (auto& t : h->timings) {
+    cudaEventDestroy(t.a);
+    cudaEventDestroy(t.b);
+  }
+  free_device(h);
+  dfree(h->d_step);
+  dfree(h->d_scratch);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+int fz_load_geometry_raw(fz_handle* h, const float* S, const uint8_t* oid, int32_t Nx, int32_t Ny,
+                         int32_t Nz) {
+  if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  if (!S || !oid) return set_error(h, FZ_EINVAL, "fz_load_geometry_raw: NULL array");
+  const int minn = 2 * GHOST + 1;
+  if (Nx < minn || Ny < minn || Nz < minn)
+    return set_error(h, FZ_EINVAL, "fz_load_geometry_raw: grid must be at least 7 cells per axis");
+  if (h->prm.pml_cells * 2 + 2 * GHOST > std::min(Nx, std::min(Ny, Nz)) &&
+      (h->prm.pml[0] || h->prm.pml[1] || h->prm.pml[2] || h->prm.pml[3] || h->prm.pml[4] || h->prm.pml[5]))
+    ;  // narrow domains with overlapping PML bands follow the reference's index rule
+  cudaSetDevice(h->device);
+  return h->fp64 ? load_geometry<double>(h, S, oid, Nx, Ny, Nz) : load_geometry<float>(h, S, oid, Nx, Ny, Nz);
+}
+
+int fz_set_materials(fz_handle* h, int32_t nMat, int32_t K, int32_t L, const double* Rinf, const double* A,
+                     const double* zeta, const double* B, const double* C, const double* alpha,
+                     const double* beta) {
+  if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  if (h->finalized) return set_error(h, FZ_ESTATE, "fz_set_materials after the first fz_run");
+  if (nMat < 0 || nMat > 254 || K < 0 || L < 0) return set_error(h, FZ_EINVAL, "fz_set_materials: bad sizes");
+  if (nMat > 0 && !Rinf) return set_error(h, FZ_EINVAL, "fz_set_materials: NULL Rinf");
+  if (K > 0 && nMat > 0 && (!A || !zeta)) return set_error(h, FZ_EINVAL, "fz_set_materials: NULL A/zeta");
+  if (L > 0 && nMat > 0 && (!B || !C || !alpha || !beta))
+    return set_error(h, FZ_EINVAL, "fz_set_materials: NULL B/C/alpha/beta");
+  // K_m, L_m >= 1 as main3D.cu:602-603; missing poles are zero-filled as read_fit_file leaves them
+  const int Kc = std::max(1, K), Lc = std::max(1, L), nm = std::max(1, nMat);
+  h->nMat = nMat; h->K = Kc; h->L = Lc;
+  h->Rinf.assign(nm, 0.0);
+  h->A.assign((size_t)nm * Kc, 0.0); h->zeta.assign((size_t)nm * Kc, 0.0);
+  h->B.assign((size_t)nm * Lc, 0.0); h->C.assign((size_t)nm * Lc, 0.0);
+  h->alpha.assign((size_t)nm * Lc, 0.0); h->beta.assign((size_t)nm * Lc, 0.0);
+  for (int m = 0; m < nMat; m++) {
+    h->Rinf[m] = Rinf[m];
+    for (int k = 0; k < K; k++) {
+      h->A[(size_t)m * Kc + k] = A[(size_t)m * K + k];
+      h->zeta[(size_t)m * Kc + k] = zeta[(size_t)m * K + k];
+    }
+    for (int l = 0; l < L; l++) {
+      const size_t d = (size_t)m * Lc + l, s = (size_t)m * L + l;
+      h->B[d] = B[s]; h->C[d] = C[s]; h->alpha[d] = alpha[s]; h->beta[d] = beta[s];
+    }
+  }
+  h->have_materials = true;
+  return FZ_OK;
+}
+
+int fz_set_sources(fz_handle* h, int32_t n, const int32_t* cell_ijk, const double* sval, int32_t src_opt,
+                   const double* freq, const double* u_s, int64_t n_us) {
+  if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  if (h->finalized) return set_error(h, FZ_ESTATE, "fz_set_sources after the first fz_run");
+  if (!h->have_geometry) return set_error(h, FZ_ESTATE, "fz_set_sources before fz_load_geometry_raw");
+  if (n < 0 || (n > 0 && (!cell_ijk || !sval))) return set_error(h, FZ_EINVAL, "fz_set_sources: bad arguments");
+  if (src_opt < 0 || src_opt > 2) return set_error(h, FZ_EINVAL, "fz_set_sources: src_opt must be 0, 1 or 2");
+  if (n > 0 && src_opt == 2 && !freq) return set_error(h, FZ_EINVAL, "fz_set_sources: sine sources need freq");
+  if (n > 0 && src_opt != 2 && (!u_s || n_us < 1))
+    return set_error(h, FZ_EINVAL, "fz_set_sources: PCS/Ricker sources need u_s");
+  for (int s = 0; s < n; s++) {
+    const int i = cell_ijk[3 * s], j = cell_ijk[3 * s + 1], k = cell_ijk[3 * s + 2];
+    if (i < 0 || i >= h->Nx || j < 0 || j >= h->Ny || k < 0 || k >= h->Nz)
+      return set_error(h, FZ_EINVAL, "fz_set_sources: source cell outside the grid");
+  }
+  h->nsrc = n;
+  h->src_ijk.assign(cell_ijk, cell_ijk + 3 * (size_t)n);
+  h->src_val.assign(sval, sval + n);
+  h->src_freq.assign((size_t)n, 0.0);
+  if (freq) h->src_freq.assign(freq, freq + n);
+  h->src_opt = src_opt;
+  h->u_s.clear();
+  if (u_s && n_us > 0) h->u_s.assign(u_s, u_s + n_us);
+  return FZ_OK;
+}
+
+int fz_set_receivers(fz_handle* h, int32_t n, const int32_t* cell_ijk, int64_t capacity_steps) {
+  if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  if (h->finalized) return set_error(h, FZ_ESTATE, "fz_set_receivers after the first fz_run");
+  if (!h->have_geometry) return set_error(h, FZ_ESTATE, "fz_set_receivers before fz_load_geometry_raw");
+  if (n < 0 || (n > 0 && !cell_ijk) || capacity_steps < 0)
+    return set_error(h, FZ_EINVAL, "fz_set_receivers: bad arguments");
+  for (int r = 0; r < n; r++) {
+    const int i = cell_ijk[3 * r], j = cell_ijk[3 * r + 1], k = cell_ijk[3 * r + 2];
+    // main3D.cu:942-944: a receiver outside the domain stops the run
+    if (i < 0 || i >= h->Nx || j < 0 || j >= h->Ny || k < 0 || k >= h->Nz)
+      return set_error(h, FZ_EINVAL, "fz_set_receivers: receiver outside the domain");
+  }
+  h->nrec = n;
+  h->rec_ijk.assign(cell_ijk, cell_ijk + 3 * (size_t)n);
+  h->rec_cap = capacity_steps;
+  return FZ_OK;
+}
+
+int fz_set_fields(fz_handle* h, const double* p, const double* u, const double* v, const double* w) {
+  if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  if (!h->have_geometry) return set_error(h, FZ_ESTATE, "fz_set_fields before fz_load_geometry_raw");
+  int rc = fz_sync(h, 0);
+  if (rc != FZ_OK) return rc;
+  cudaSetDevice(h->device);
+  return h->fp64 ? set_fields<double>(h, p, u, v, w) : set_fields<float>(h, p, u, v, w);
+}
+
+int fz_run(fz_handle* h, int64_t nsteps) {
+  if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  if (nsteps < 0) return set_error(h, FZ_EINVAL, "fz_run: negative step count");
+  cudaSetDevice(h->device);
+  return h->fp64 ? run_steps<double>(h, nsteps) : run_steps<float>(h, nsteps);
+}
+
+int fz_run_timed(fz_handle* h, int64_t nsteps, double* ms) {
+  if (!check_handle(h) || !ms) return fzi::set_global_error(FZ_EINVAL, "NULL argument");
+  cudaSetDevice(h->device);
+  int rc = fz_sync(h, 0);
+  if (rc != FZ_OK) return rc;
+  cudaEvent_t a = nullptr, b = nullptr;
+  FZ_CUDA(h, cudaEventCreate(&a), "event");
+  cudaError_t e = cudaEventCreate(&b);
+  if (e != cudaSuccess) { cudaEventDestroy(a); return cuda_fail(h, e, "event"); }
+  e = cudaEventRecord(a, h->stream);
+  rc = (e == cudaSuccess) ? fz_run(h, nsteps) : cuda_fail(h, e, "event record");
+  if (rc == FZ_OK) {
+    e = cudaEventRecord(b, h->stream);
+    rc = (e == cudaSuccess) ? fz_sync(h, 0) : cuda_fail(h, e, "event record");
+  }
+  if (rc == FZ_OK) {
+    float x = 0.f;
+    e = cudaEventElapsedTime(&x, a, b);
+    if (e == cudaSuccess) *ms = x; else rc = cuda_fail(h, e, "event elapsed");
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return rc;
+}
+
+int fz_sync(fz_handle* h, int64_t timeout_ms) {
+  if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  if (timeout_ms <= 0) timeout_ms = 600000;
+  cudaSetDevice(h->device);
+  const auto t0 = std::chrono::steady_clock::now();
+  int sleep_us = 20;
+  for (;;) {
+    cudaError_t e = cudaStreamQuery(h->stream);
+    if (e == cudaSuccess) return FZ_OK;
+    if (e != cudaErrorNotReady) return cuda_fail(h, e, "stream");
+    const auto ms =
+        std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0).count();
+    if (ms > timeout_ms) return set_error(h, FZ_ETIMEOUT, "fz_sync: device work did not finish in time");
+    std::this_thread::sleep_for(std::chrono::microseconds(sleep_us));
+    sleep_us = std::min(sleep_us * 2, 2000);
+  }
+}
+
+int fz_steps_done(fz_handle* h, int64_t* n) {
+  if (!check_handle(h) || !n) return fzi::set_global_error(FZ_EINVAL, "NULL argument");
+  int rc = fz_sync(h, 0);
+  if (rc != FZ_OK) return rc;
+  FZ_CUDA(h, cudaMemcpy(n, h->d_step, sizeof(int64_t), cudaMemcpyDeviceToHost), "step D2H");
+  return FZ_OK;
+}
+
+static int get_samples(fz_handle* h, double* out64, float* out32, int64_t cap, bool vel) {
+  if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  int rc = fz_sync(h, 0);
+  if (rc != FZ_OK) return rc;
+  int64_t n = 0;
+  FZ_CUDA(h, cudaMemcpy(&n, h->d_step, sizeof(int64_t), cudaMemcpyDeviceToHost), "step D2H");
+  n = std::min(n, h->rec_cap);
+  const int comp = vel ? 3 : 1;
+  const int64_t need = (int64_t)h->nrec * n * comp;
+  if (cap < need) return set_error(h, FZ_EINVAL, "output buffer too small: need " + std::to_string(need));
+  if (need == 0) return FZ_OK;
+  std::vector<double> tmp((size_t)h->nrec * h->rec_cap * comp);
+  FZ_CUDA(h, cudaMemcpy(tmp.data(), vel ? h->d_vel : h->d_ir, tmp.size() * 8, cudaMemcpyDeviceToHost), "IR D2H");
+  for (int r = 0; r < h->nrec; r++)
+    for (int64_t t = 0; t < n * comp; t++) {
+      const double x = tmp[(size_t)r * h->rec_cap * comp + t];
+      const size_t o = (size_t)r * n * comp + t;
+      if (out64) out64[o] = x;
+      if (out32) out32[o] = (float)x;
+    }
+  return FZ_OK;
+}
+
+int fz_get_ir(fz_handle* h, float* out, int64_t cap) { return get_samples(h, nullptr, out, cap, false); }
+int fz_get_ir64(fz_handle* h, double* out, int64_t cap) { return get_samples(h, out, nullptr, cap, false); }
+int fz_get_vel(fz_handle* h, float* out, int64_t cap) { return get_samples(h, nullptr, out, cap, true); }
+
+int fz_get_fields(fz_handle* h, double* p, double* u, double* v, double* w) {
+  if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  if (!h->have_geometry) return set_error(h, FZ_ESTATE, "fz_get_fields before fz_load_geometry_raw");
+  int rc = fz_sync(h, 0);
+  if (rc != FZ_OK) return rc;
+  return h->fp64 ? get_fields<double>(h, p, u, v, w) : get_fields<float>(h, p, u, v, w);
+}
+
+int fz_energy(fz_handle* h, double* E) {
+  if (!check_handle(h) || !E) return fzi::set_global_error(FZ_EINVAL, "NULL argument");
+  if (!h->have_geometry) return set_error(h, FZ_ESTATE, "fz_energy before fz_load_geometry_raw");
+  cudaSetDevice(h->device);
+  return h->fp64 ? energy<double>(h, E) : energy<float>(h, E);
+}
+
+int fz_info(fz_handle* h, int32_t* dims, int64_t* n_band, int64_t* n_update) {
+  if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  if (dims) { dims[0] = h->Nx; dims[1] = h->Ny; dims[2] = h->Nz; }
+  if (n_band) *n_band = h->nB;
+  if (n_update) *n_update = h->n_update;
+  return FZ_OK;
+}
+
+int fz_profile_enable(fz_handle* h, int32_t on) {
+  if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  h->profiling = (on != 0);
+  return FZ_OK;
+}
+
+int fz_profile_read(fz_handle* h, double* ms, int64_t* launches, int32_t nkinds) {
+  if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  int rc = fz_sync(h, 0);
+  if (rc != FZ_OK) return rc;
+  for (auto& t : h->timings) {
+    float x = 0.f;
+    if (cudaEventElapsedTime(&x, t.a, t.b) == cudaSuccess && t.kind >= 0 && t.kind < 8) {
+      h->prof_ms[t.kind] += x;
+      h->prof_n[t.kind] += 1;
+    }
+    cudaEventDestroy(t.a);
+    cudaEventDestroy(t.b);
+  }
+  h->timings.clear();
+  for (int k = 0; k < nkinds && k < 8; k++) {
+    if (ms) ms[k] = h->prof_ms[k];
+    if (launches) launches[k] = h->prof_n[k];
+  }
+  for (int k = 0; k < 8; k++) { h->prof_ms[k] = 0; h->prof_n[k] = 0; }
+  return FZ_OK;
+}
+
+int fz_last_error(fz_handle* h, char* buf, size_t cap) {
+  if (!buf || cap == 0) return FZ_EINVAL;
+  const std::string& s = h ? h->err : g_err;
+  std::snprintf(buf, cap, "%s", s.c_str());
+  return FZ_OK;
+}
+
+int fz_global_error(char* buf, size_t cap) {
+  if (!buf || cap == 0) return FZ_EINVAL;
+  std::snprintf(buf, cap, "%s", g_err.c_str());
+  return FZ_OK;
+}
+
+}  // extern "C"

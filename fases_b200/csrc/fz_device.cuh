@@ -1,0 +1,139 @@
+// fz_device.cuh -- device-side types shared by the stepping kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fz {
+
+// Device grid layout. Cell (i,j,k) of the padded reference grid (ghost band of 3 cells,
+// 3D-solver/include/parsing3D.h:128) lives at XOFF + i + Sx*(j + Ny*k). XOFF = 29 puts the first
+// updated cell (i = 3) on a 128-byte boundary, and Sx is a multiple of 32 elements, so every
+// warp-wide row segment of a stage tile is one aligned 128-byte line (FP32).
+constexpr int XOFF = 29;
+constexpr int GHOST = 3;
+
+// Stage-kernel tile: 32 x 16 cells per CTA, one thread per (i, j) column, streaming along z.
+constexpr int TX = 32;
+constexpr int TY = 16;
+constexpr int HX = 4;  // x halo held in shared memory (3 needed; 4 keeps rows 16-byte aligned)
+constexpr int HY = 3;  // y halo
+constexpr int PW = TX + 2 * HX;  // 40 tile columns
+constexpr int PH = TY + 2 * HY;  // 22 tile rows
+constexpr int NTHREADS = TX * TY;
+
+// Cell-class bits (one byte per cell, replaces the reference's 4-byte S read per stage).
+constexpr uint8_t CLS_UPDATE = 1;  // interior cell with S >= h: written by the stage kernels
+constexpr uint8_t CLS_SOURCE = 2;  // a point source sits here
+
+// Per-axis cPML coefficients at one index along the axis (functions3D.cuh:681-756), precomputed
+// on the host once instead of powf/expf per cell and stage.
+template <class R>
+struct PmlCoef {
+  int32_t tile;  // index in the 2d-thick psi tile along this axis, -1 outside the band
+  R kinv1;       // 1/kappa - 1
+  R b;           // exp(-(alpha + sigma/kappa) dt)
+  R ca;          // sigma/(kappa (sigma + kappa alpha)) (b - 1), 0 where sigma = 0
+};
+
+template <class R>
+struct Pair;
+template <>
+struct Pair<float> {
+  typedef float2 T;
+};
+template <>
+struct Pair<double> {
+  typedef double2 T;
+};
+
+// Arguments of one stage launch.
+template <class R>
+struct StageArgs {
+  typedef typename Pair<R>::T P;
+  const R* pi;  // stage input U_in
+  const R* ui;
+  const R* vi;
+  const R* wi;
+  const R* pb;  // U0 (stages 1 and 2)
+  const R* ub;
+  const R* vb;
+  const R* wb;
+  R* po;  // stage output
+  R* uo;
+  R* vo;
+  R* wo;
+  const uint8_t* cls;
+  int32_t Nx, Ny, Nz;
+  int64_t Sx;     // row pitch (elements)
+  int64_t plane;  // Sx * Ny
+  int32_t kz_chunk;
+  R dt_h;   // dt / h
+  R frc2;   // 0.5 * rho * c^2
+  R firho;  // 0.5 / rho
+  R fc;     // 0.5 * c
+  R inv_h;  // 1 / h
+  R wdt;    // stage weight * dt (cPML correction weight)
+  // cPML (pml_on = 0: no face enabled)
+  int32_t pml_on;
+  int32_t pml_d2;  // 2 * pml_cells
+  const PmlCoef<R>* pcx;
+  const PmlCoef<R>* pcy;
+  const PmlCoef<R>* pcz;
+  P* psix;  // (psi_px, psi_ux) pairs [2d x Ny x Nz]
+  P* psiy;  // (psi_py, psi_vy) pairs [Nx x 2d x Nz]
+  P* psiz;  // (psi_pz, psi_wz) pairs [Nx x Ny x 2d]
+  // sources
+  int32_t nsrc;
+  const int64_t* src_cell;  // device index
+  const R* src_coef;        // dt c^2 sval rho A_s / h^3
+  const R* src_freq;
+  const R* u_s;
+  int64_t n_us;
+  int32_t src_opt;
+  R src_w;      // stage weight of the injection (1, 1/4, 2/3)
+  int32_t nn_mul, nn_add;  // nn = nn_mul * n + nn_add
+  R half_dt;
+  const int64_t* step;  // device step counter n
+};
+
+// Immersed band cells (compact list in the reference's build_boundary_map order).
+template <class R>
+struct BandArgs {
+  int64_t nB;
+  const int64_t* cell;    // device index of the band cell
+  const int64_t* corner;  // device index of the trilinear base corner
+  const R* geo;           // [4*nB]: sx, sy, sz, chi
+  const R* nrm;           // [4*nB]: nx, ny, nz, unused
+  const int32_t* mat;     // material id (oid - 1)
+  const R* pi;            // stage input (probe source)
+  const R* ui;
+  const R* vi;
+  const R* wi;
+  R* po;  // stage output (blended in place)
+  R* uo;
+  R* vo;
+  R* wo;
+  int64_t Sx, plane;
+  double Z0, dt;
+  double a_ssp, b_ssp, inv_c_ssp;
+  int32_t K, L;
+  const double* Rinf;
+  const double* A;
+  const double* zeta;
+  const double* B;
+  const double* C;
+  const double* alpha;
+  const double* beta;
+  // ADE states, state q of band cell b at [q*nB + b]
+  double* phL;
+  const double* phM;
+  const double* phR;
+  double* s1L;
+  const double* s1M;
+  const double* s1R;
+  double* s2L;
+  const double* s2M;
+  const double* s2R;
+};
+
+}  // namespace fz

@@ -1,0 +1,108 @@
+// fz_internal.h -- host-side state of a solver handle (private to libfz.so).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/fz.h"
+#include "fz_device.cuh"
+
+struct fz_timing_rec {
+  int kind;
+  cudaEvent_t a, b;
+};
+
+struct fz_handle {
+  fz_params prm{};
+  std::string err;
+  int device = 0;
+  int nsm = 0;
+  cudaStream_t stream = nullptr;
+  bool fp64 = false;
+  size_t rsize = 4;  // sizeof(real)
+
+  // grid
+  int Nx = 0, Ny = 0, Nz = 0;
+  int64_t Sx = 0, plane = 0, ncell_dev = 0;
+  double Lx = 0, Ly = 0, Lz = 0;  // padded domain size for header.txt
+  bool have_geometry = false;
+  std::vector<float> S_host;
+  std::vector<uint8_t> oid_host;
+  int64_t n_update = 0;
+
+  // device fields: U[set][field], set 0..2, field p,u,v,w
+  void* U[3][4] = {{nullptr}};
+  int i0 = 0, i1 = 1, i2 = 2;
+  uint8_t* d_cls = nullptr;
+  std::vector<uint8_t> cls_host;
+
+  // cPML
+  bool pml_on = false;
+  void* d_pml_coef[3] = {nullptr, nullptr, nullptr};
+  void* d_psi[3] = {nullptr, nullptr, nullptr};
+
+  // immersed band
+  int64_t nB = 0;
+  std::vector<int64_t> band_cell_ref;  // reference-layout cell index (for the material check)
+  std::vector<int32_t> band_mat;
+  int64_t* d_bcell = nullptr;
+  int64_t* d_bcorner = nullptr;
+  void* d_bgeo = nullptr;
+  void* d_bnrm = nullptr;
+  int32_t* d_bmat = nullptr;
+  double* d_ade[3][3] = {{nullptr}};  // [set][phi, psi1, psi2]
+  int ph_old = 0, ph_cur = 1, ph_nu = 2;
+
+  // materials
+  int nMat = 0, K = 1, L = 1;
+  std::vector<double> Rinf, A, zeta, B, C, alpha, beta;
+  double* d_mat = nullptr;  // packed: Rinf | A | zeta | B | C | alpha | beta
+  bool have_materials = false;
+
+  // sources
+  int nsrc = 0;
+  std::vector<int32_t> src_ijk;
+  std::vector<double> src_val, src_freq, u_s;
+  int src_opt = 0;
+  int64_t* d_src_cell = nullptr;
+  void* d_src_coef = nullptr;
+  void* d_src_freq = nullptr;
+  void* d_us = nullptr;
+  int64_t n_us = 0;
+
+  // receivers
+  int nrec = 0;
+  std::vector<int32_t> rec_ijk;
+  int64_t rec_cap = 0;
+  int64_t* d_rec_cell = nullptr;
+  double* d_ir = nullptr;
+  double* d_vel = nullptr;
+
+  // step counter and bookkeeping
+  int64_t* d_step = nullptr;
+  double* d_scratch = nullptr;
+  int64_t steps_enqueued = 0;
+  bool finalized = false;
+  int kz_chunk = 0;
+  dim3 stage_grid;
+
+  // graphs, keyed by buffer parity
+  int graph_steps = 10;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+
+  // profiling
+  bool profiling = false;
+  std::vector<fz_timing_rec> timings;
+  double prof_ms[8] = {0};
+  int64_t prof_n[8] = {0};
+
+  // output bookkeeping
+  std::string scene_name;
+};
+
+namespace fzi {
+int set_error(fz_handle* h, int code, const std::string& msg);
+int set_global_error(int code, const std::string& msg);
+int cuda_fail(fz_handle* h, cudaError_t e, const char* what);
+}  // namespace fzi

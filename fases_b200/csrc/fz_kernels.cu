@@ -1,0 +1,527 @@
+// fz_kernels.cu -- sm_100a stepping kernels of the FASES time-domain solver hot path.
+//
+// One SSP-RK3 step of the reference (3D-solver/core/main3D.cu:1280-1319) is nine launches there:
+// three stage kernels (functions3D.cuh:1086-1327), three source injections (1039-1047) and three
+// full-grid immersed-boundary passes (462-565). Here it is seven: three fused stage kernels
+// (WENO-Z reconstruction once per face, Godunov flux, RK combination, cPML and source injection
+// in one pass), three sparse band kernels that touch only the immersed band cells, and one
+// receiver gather.
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "fz_device.cuh"
+#include "fz_kernels.h"
+
+namespace fz {
+
+// ------------------------------------------------------------------------------------------
+// Pair arithmetic. A pair holds the same quantity for two variables (pressure and the velocity
+// component normal to the sweep), so every WENO-Z and flux operation runs on both at once. In
+// FP32 these are the sm_100 paired instructions (add/mul/fma .f32x2).
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ float2 pmk(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ double2 pmk(double a, double b) { return make_double2(a, b); }
+__device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 pmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 psub(float2 a, float2 b) {
+  return __ffma2_rn(b, make_float2(-1.f, -1.f), a);
+}
+__device__ __forceinline__ float2 pabs(float2 a) { return make_float2(fabsf(a.x), fabsf(a.y)); }
+__device__ __forceinline__ float frcp(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float2 prcp(float2 a) { return make_float2(frcp(a.x), frcp(a.y)); }
+__device__ __forceinline__ float2 pswap(float2 a) { return make_float2(a.y, a.x); }
+
+__device__ __forceinline__ double2 padd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 pmul(double2 a, double2 b) { return make_double2(a.x * b.x, a.y * b.y); }
+__device__ __forceinline__ double2 pfma(double2 a, double2 b, double2 c) {
+  return make_double2(fma(a.x, b.x, c.x), fma(a.y, b.y, c.y));
+}
+__device__ __forceinline__ double2 psub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 pabs(double2 a) { return make_double2(fabs(a.x), fabs(a.y)); }
+__device__ __forceinline__ double2 prcp(double2 a) { return make_double2(1.0 / a.x, 1.0 / a.y); }
+__device__ __forceinline__ double2 pswap(double2 a) { return make_double2(a.y, a.x); }
+
+template <class R>
+__device__ __forceinline__ typename Pair<R>::T psplat(R x) {
+  return pmk(x, x);
+}
+
+// ------------------------------------------------------------------------------------------
+// WENO-Z reconstruction at one cell centre (Borges, Carmona, Costa & Don 2008, q = 1), the scheme
+// of functions3D.cuh:763-1001 with the tables of main3D.cu:834-843 and eps = 1e-10 (main3D.cu:770).
+//
+// The reference evaluates V-(i+1/2) (idx = 1) and V+(i-1/2) (idx = 0) of a cell in two separate
+// calls; both use the same three smoothness indicators and the same factors (1 + tau/(beta+eps)),
+// and differ only in the linear weights d (mirrored) and the candidate rows. This evaluates them
+// together, written on first differences a..d of the five-point stencil:
+//   candidates:  u_i + delta_r,   V = u_i + sum_r w_r delta_r,   w_r = d_r q_r / sum d q
+//   12/13 beta_r = (second difference)^2 + 3/13 (one-sided first-derivative term)^2
+// (the 12/13 scaling is absorbed into eps).
+// ------------------------------------------------------------------------------------------
+template <class R>
+__device__ __forceinline__ void weno_center(typename Pair<R>::T qm2, typename Pair<R>::T qm1,
+                                            typename Pair<R>::T q0, typename Pair<R>::T qp1,
+                                            typename Pair<R>::T qp2, typename Pair<R>::T& vm,
+                                            typename Pair<R>::T& vp) {
+  typedef typename Pair<R>::T P;
+  const P a = psub(qm1, qm2), b = psub(q0, qm1), c = psub(qp1, q0), d = psub(qp2, qp1);
+  const P D2 = psub(b, a), D1 = psub(c, b), D0 = psub(d, c);  // second differences
+  const P E2 = pfma(b, psplat<R>(R(2)), D2);                  // u_{i-2} - 4u_{i-1} + 3u_i
+  const P E1 = padd(b, c);                                    // -(u_{i-1} - u_{i+1})
+  const P E0 = pfma(c, psplat<R>(R(-2)), D0);                 // 3u_i - 4u_{i+1} + u_{i+2} (sign)
+  const P k313 = psplat<R>(R(3.0 / 13.0));
+  const P B0 = pfma(D0, D0, pmul(pmul(E0, k313), E0));
+  const P B1 = pfma(D1, D1, pmul(pmul(E1, k313), E1));
+  const P B2 = pfma(D2, D2, pmul(pmul(E2, k313), E2));
+  const P eps = psplat<R>(R(1e-10 * 12.0 / 13.0));
+  const P tau = pabs(psub(B0, B2));
+  const P one = psplat<R>(R(1));
+  const P q0w = pfma(tau, prcp(padd(B0, eps)), one);
+  const P q1w = pfma(tau, prcp(padd(B1, eps)), one);
+  const P q2w = pfma(tau, prcp(padd(B2, eps)), one);
+  // normalisers: V- uses d = (3/10, 3/5, 1/10), V+ the mirrored (1/10, 3/5, 3/10)
+  const P Sm = pfma(q2w, psplat<R>(R(0.1)), pfma(q1w, psplat<R>(R(0.6)), pmul(q0w, psplat<R>(R(0.3)))));
+  const P Sp = pfma(q2w, psplat<R>(R(0.3)), pfma(q1w, psplat<R>(R(0.6)), pmul(q0w, psplat<R>(R(0.1)))));
+  // d_r * delta_r for both faces
+  const P em0 = pfma(c, psplat<R>(R(0.2)), pmul(d, psplat<R>(R(-0.05))));
+  const P em1 = pfma(b, psplat<R>(R(0.1)), pmul(c, psplat<R>(R(0.2))));
+  const P em2 = pfma(a, psplat<R>(R(-1.0 / 30.0)), pmul(b, psplat<R>(R(1.0 / 12.0))));
+  const P ep0 = pfma(c, psplat<R>(R(-1.0 / 12.0)), pmul(d, psplat<R>(R(1.0 / 30.0))));
+  const P ep1 = pfma(b, psplat<R>(R(-0.2)), pmul(c, psplat<R>(R(-0.1))));
+  const P ep2 = pfma(a, psplat<R>(R(0.05)), pmul(b, psplat<R>(R(-0.2))));
+  const P Nm = pfma(q2w, em2, pfma(q1w, em1, pmul(q0w, em0)));
+  const P Np = pfma(q2w, ep2, pfma(q1w, ep1, pmul(q0w, ep0)));
+  vm = pfma(Nm, prcp(Sm), q0);
+  vp = pfma(Np, prcp(Sp), q0);
+}
+
+// Godunov (exact Riemann) flux of linear acoustics for a (pressure, normal velocity) pair
+// (functions3D.cuh:56-78):  F_p = 1/2 (rho c^2 (q+ + q-) - c (p+ - p-)),
+//                           F_q = 1/2 ((p+ + p-)/rho - c (q+ - q-)).
+template <class R>
+__device__ __forceinline__ typename Pair<R>::T godunov(typename Pair<R>::T vm, typename Pair<R>::T vp,
+                                                       typename Pair<R>::T kA, typename Pair<R>::T kC) {
+  const typename Pair<R>::T sum = padd(vm, vp), dif = psub(vp, vm);
+  return pfma(dif, kC, pmul(pswap(sum), kA));
+}
+
+// ------------------------------------------------------------------------------------------
+// Fused stage kernel. CTA = 32 x 16 columns marching in z over kz_chunk planes.
+//  - z: a register queue of (p, w) over five planes; the z-centre of plane k+1 is evaluated once
+//    and its two face values are used by the flux above plane k and (next iteration) below k+1.
+//  - x, y: plane k of (p,u) and (p,v) is staged in shared memory with a 3-cell halo; every
+//    x- and y-centre is evaluated once (the reference evaluates every face from both sides) and
+//    exchanged through shared memory.
+// STAGE 0: U1 = U0 + dt L(U0); 1: U2 = 3/4 U0 + 1/4 (U1 + dt L(U1)); 2: U1 = (U0 + 2 (U2 + dt L(U2)))/3
+// (functions3D.cuh:1149-1152, 1230-1233, 1311-1314), cPML with weights 1, 1/4, 2/3 and the psi
+// advance in stage 2 (functions3D.cuh:1157-1162, 1237-1242, 1320-1325), then the point sources of
+// the stage (main3D.cu:1288, 1296, 1304).
+// ------------------------------------------------------------------------------------------
+template <class R, int STAGE>
+__global__ void __launch_bounds__(NTHREADS, 1) k_stage(const StageArgs<R> A) {
+  typedef typename Pair<R>::T P;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  P* TU = reinterpret_cast<P*>(smem_raw);  // [PH][PW] (p, u)
+  P* TV = TU + PH * PW;                    // [PH][PW] (p, v)
+  P* XCm = TV + PH * PW;                   // [TY][TX+2] V- (upper x face) of x-centres i0-1 .. i0+TX
+  P* XCp = XCm + TY * (TX + 2);            // [TY][TX+2] V+ (lower x face)
+  P* YCm = XCp + TY * (TX + 2);            // [TY+2][TX] V- of y-centres j0-1 .. j0+TY
+  P* YCp = YCm + (TY + 2) * TX;            // [TY+2][TX] V+
+
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int lt = ty * TX + tx;
+  const int i0 = GHOST + blockIdx.x * TX, j0 = GHOST + blockIdx.y * TY;
+  const int i = i0 + tx, j = j0 + ty;
+  const int kb = GHOST + blockIdx.z * A.kz_chunk;
+  const int ke = min(kb + A.kz_chunk, A.Nz - GHOST);
+  if (kb >= ke) return;
+  const int64_t Sx = A.Sx, plane = A.plane;
+  const bool col_ok = (j < A.Ny) && (XOFF + i < Sx);
+  const int64_t col = XOFF + i + Sx * (int64_t)j;
+  const bool valid = (i < A.Nx - GHOST) && (j < A.Ny - GHOST);
+
+  const P kA = pmk(A.frc2, A.firho);
+  const P kC = psplat<R>(-A.fc);
+
+  auto ld_pw = [&](int kk) -> P {
+    if (!col_ok) return psplat<R>(R(0));
+    const int64_t g = col + plane * kk;
+    return pmk(A.pi[g], A.wi[g]);
+  };
+
+  // z prologue: centres kb-1 and kb give the flux through face kb-1/2 and V-(kb+1/2).
+  P z0 = ld_pw(kb - 3), z1 = ld_pw(kb - 2), z2 = ld_pw(kb - 1), z3 = ld_pw(kb), z4 = ld_pw(kb + 1);
+  P z5 = ld_pw(kb + 2);
+  P zm, zp, vmB, vpB;
+  weno_center<R>(z0, z1, z2, z3, z4, zm, zp);
+  weno_center<R>(z1, z2, z3, z4, z5, vmB, vpB);
+  P Fz_lo = godunov<R>(zm, vpB, kA, kC);
+  zm = vmB;
+  // queue: planes k-1, k, k+1, k+2
+  P qa = z2, qb = z3, qc = z4, qd = z5;
+
+  for (int k = kb; k < ke; ++k) {
+    // ---- z: centre k+1 -> flux through face k+1/2
+    const P qe = ld_pw(k + 3);
+    P vmC, vpC;
+    weno_center<R>(qa, qb, qc, qd, qe, vmC, vpC);
+    const P Fz_hi = godunov<R>(zm, vpC, kA, kC);
+
+    // ---- stage plane k of (p,u,v) into shared memory with halo
+    __syncthreads();
+    for (int e = lt; e < PH * PW; e += NTHREADS) {
+      const int r = e / PW, q = e - r * PW;
+      const int gj = j0 - HY + r, gc = XOFF + i0 - HX + q;
+      R p = R(0), u = R(0), v = R(0);
+      if (gj < A.Ny && gc < Sx) {
+        const int64_t g = gc + Sx * (int64_t)gj + plane * k;
+        p = A.pi[g];
+        u = A.ui[g];
+        v = A.vi[g];
+      }
+      TU[e] = pmk(p, u);
+      TV[e] = pmk(p, v);
+    }
+    __syncthreads();
+
+    // ---- x and y centres of this thread's cell
+    P xm, xp, ym, yp;
+    {
+      const P* row = TU + (ty + HY) * PW + (tx + HX);
+      weno_center<R>(row[-2], row[-1], row[0], row[1], row[2], xm, xp);
+      XCm[ty * (TX + 2) + tx + 1] = xm;
+      XCp[ty * (TX + 2) + tx + 1] = xp;
+      const P* cl = TV + (ty + HY) * PW + (tx + HX);
+      weno_center<R>(cl[-2 * PW], cl[-PW], cl[0], cl[PW], cl[2 * PW], ym, yp);
+      YCm[(ty + 1) * TX + tx] = ym;
+      YCp[(ty + 1) * TX + tx] = yp;
+    }
+    // ---- halo centres: warp 0 the x edges (i0-1, i0+TX) of all 16 rows, warps 1-2 the y edge
+    //      rows (j0-1, j0+TY)
+    if (lt < TX) {
+      const int r = lt >> 1, side = lt & 1;
+      const int c = side ? (HX + TX) : (HX - 1);
+      const P* row = TU + (r + HY) * PW + c;
+      P em, ep;
+      weno_center<R>(row[-2], row[-1], row[0], row[1], row[2], em, ep);
+      const int slot = r * (TX + 2) + (side ? TX + 1 : 0);
+      XCm[slot] = em;
+      XCp[slot] = ep;
+    } else if (lt < 3 * TX) {
+      const int e = lt - TX;
+      const int r = (e < TX) ? -1 : TY;
+      const int c = e & (TX - 1);
+      const P* cl = TV + (r + HY) * PW + (c + HX);
+      P em, ep;
+      weno_center<R>(cl[-2 * PW], cl[-PW], cl[0], cl[PW], cl[2 * PW], em, ep);
+      YCm[(r + 1) * TX + c] = em;
+      YCp[(r + 1) * TX + c] = ep;
+    }
+    __syncthreads();
+
+    // ---- face fluxes of this cell
+    const P Fx_lo = godunov<R>(XCm[ty * (TX + 2) + tx], xp, kA, kC);
+    const P Fx_hi = godunov<R>(xm, XCp[ty * (TX + 2) + tx + 2], kA, kC);
+    const P Fy_lo = godunov<R>(YCm[ty * TX + tx], yp, kA, kC);
+    const P Fy_hi = godunov<R>(ym, YCp[(ty + 2) * TX + tx], kA, kC);
+
+    if (valid) {
+      const int64_t g = col + plane * k;
+      const uint8_t cls = A.cls[g];
+      if (cls & CLS_UPDATE) {
+        // flux differences (times h): .x pressure part, .y velocity part
+        const P Lx = psub(Fx_lo, Fx_hi), Ly = psub(Fy_lo, Fy_hi), Lz = psub(Fz_lo, Fz_hi);
+        const R Lp = Lx.x + Ly.x + Lz.x;
+        const R p_in = qb.x, w_in = qb.y;
+        const R u_in = TU[(ty + HY) * PW + tx + HX].y, v_in = TV[(ty + HY) * PW + tx + HX].y;
+        R pn, un, vn, wn;
+        if (STAGE == 0) {
+          pn = p_in + A.dt_h * Lp;
+          un = u_in + A.dt_h * Lx.y;
+          vn = v_in + A.dt_h * Ly.y;
+          wn = w_in + A.dt_h * Lz.y;
+        } else if (STAGE == 1) {
+          pn = R(0.75) * A.pb[g] + R(0.25) * (p_in + A.dt_h * Lp);
+          un = R(0.75) * A.ub[g] + R(0.25) * (u_in + A.dt_h * Lx.y);
+          vn = R(0.75) * A.vb[g] + R(0.25) * (v_in + A.dt_h * Ly.y);
+          wn = R(0.75) * A.wb[g] + R(0.25) * (w_in + A.dt_h * Lz.y);
+        } else {
+          const R third = R(1.0 / 3.0), two3 = R(2.0 / 3.0);
+          pn = third * A.pb[g] + two3 * (p_in + A.dt_h * Lp);
+          un = third * A.ub[g] + two3 * (u_in + A.dt_h * Lx.y);
+          vn = third * A.vb[g] + two3 * (v_in + A.dt_h * Ly.y);
+          wn = third * A.wb[g] + two3 * (w_in + A.dt_h * Lz.y);
+        }
+        if (A.pml_on) {
+          // cPML (functions3D.cuh:725-755): field += w dt ((1/kappa - 1) D + psi), psi frozen
+          // within the step and advanced once, in stage 2, by recursive convolution.
+          const PmlCoef<R> cx = A.pcx[i], cy = A.pcy[j], cz = A.pcz[k];
+          const int64_t d2 = A.pml_d2;
+          if (cx.tile >= 0) {
+            const int64_t X = cx.tile + d2 * ((int64_t)j + (int64_t)A.Ny * k);
+            const P ps = A.psix[X];
+            const R Dp = Lx.x * A.inv_h, Du = Lx.y * A.inv_h;
+            pn += A.wdt * (cx.kinv1 * Dp + ps.x);
+            un += A.wdt * (cx.kinv1 * Du + ps.y);
+            if (STAGE == 2) A.psix[X] = pmk(cx.b * ps.x + cx.ca * Dp, cx.b * ps.y + cx.ca * Du);
+          }
+          if (cy.tile >= 0) {
+            const int64_t Y = (int64_t)i + (int64_t)A.Nx * ((int64_t)cy.tile + d2 * k);
+            const P ps = A.psiy[Y];
+            const R Dp = Ly.x * A.inv_h, Dv = Ly.y * A.inv_h;
+            pn += A.wdt * (cy.kinv1 * Dp + ps.x);
+            vn += A.wdt * (cy.kinv1 * Dv + ps.y);
+            if (STAGE == 2) A.psiy[Y] = pmk(cy.b * ps.x + cy.ca * Dp, cy.b * ps.y + cy.ca * Dv);
+          }
+          if (cz.tile >= 0) {
+            const int64_t Z = (int64_t)i + (int64_t)A.Nx * ((int64_t)j + (int64_t)A.Ny * cz.tile);
+            const P ps = A.psiz[Z];
+            const R Dp = Lz.x * A.inv_h, Dw = Lz.y * A.inv_h;
+            pn += A.wdt * (cz.kinv1 * Dp + ps.x);
+            wn += A.wdt * (cz.kinv1 * Dw + ps.y);
+            if (STAGE == 2) A.psiz[Z] = pmk(cz.b * ps.x + cz.ca * Dp, cz.b * ps.y + cz.ca * Dw);
+          }
+        }
+        if (cls & CLS_SOURCE) {
+          const int64_t n = *A.step;
+          const int64_t nn = A.nn_mul * n + A.nn_add;
+          for (int s = 0; s < A.nsrc; ++s) {
+            if (A.src_cell[s] != g) continue;
+            R amp;
+            if (A.src_opt == 2) {
+              const double ph = 2.0 * 3.14159265358979323846 * (double)A.src_freq[s] * (double)nn *
+                                (double)A.half_dt;
+              amp = (R)sin(ph);
+            } else {
+              amp = (nn < A.n_us) ? (R)A.u_s[nn] : R(0);
+            }
+            pn += A.src_w * A.src_coef[s] * amp;
+          }
+        }
+        A.po[g] = pn;
+        A.uo[g] = un;
+        A.vo[g] = vn;
+        A.wo[g] = wn;
+      } else if (cls & CLS_SOURCE) {
+        // A source in a cell the stage kernels skip still adds to the stale output value, as
+        // kernel_inject_src_SSP does (functions3D.cuh:1046).
+        const int64_t n = *A.step;
+        const int64_t nn = A.nn_mul * n + A.nn_add;
+        R pn = A.po[g];
+        for (int s = 0; s < A.nsrc; ++s) {
+          if (A.src_cell[s] != g) continue;
+          R amp;
+          if (A.src_opt == 2) {
+            const double ph = 2.0 * 3.14159265358979323846 * (double)A.src_freq[s] * (double)nn *
+                              (double)A.half_dt;
+            amp = (R)sin(ph);
+          } else {
+            amp = (nn < A.n_us) ? (R)A.u_s[nn] : R(0);
+          }
+          pn += A.src_w * A.src_coef[s] * amp;
+        }
+        A.po[g] = pn;
+      }
+    }
+
+    Fz_lo = Fz_hi;
+    zm = vmC;
+    qa = qb;
+    qb = qc;
+    qc = qd;
+    qd = qe;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Immersed ADE band (functions3D.cuh:462-565 + ADE_solver 426-459), one thread per band cell of
+// the compact list. Probe geometry (normal, trilinear corner and weights at C - 2h n, chi) is
+// precomputed once on the host. The probe reads the stage-input fields, which no kernel of this
+// stage writes; the blend reads and writes only the band cell itself.
+// ------------------------------------------------------------------------------------------
+template <class R>
+__device__ __forceinline__ R trilin(const R* __restrict__ f, int64_t q, int64_t Sx, int64_t plane, R sx,
+                                    R sy, R sz) {
+  const R c00 = f[q] * (R(1) - sx) + f[q + 1] * sx;
+  const R c10 = f[q + Sx] * (R(1) - sx) + f[q + Sx + 1] * sx;
+  const R c01 = f[q + plane] * (R(1) - sx) + f[q + plane + 1] * sx;
+  const R c11 = f[q + plane + Sx] * (R(1) - sx) + f[q + plane + Sx + 1] * sx;
+  const R c0 = c00 * (R(1) - sy) + c10 * sy, c1 = c01 * (R(1) - sy) + c11 * sy;
+  return c0 * (R(1) - sz) + c1 * sz;
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_band(const BandArgs<R> B) {
+  const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B.nB) return;
+  const int64_t cell = B.cell[b], q = B.corner[b];
+  const R sx = B.geo[4 * b + 0], sy = B.geo[4 * b + 1], sz = B.geo[4 * b + 2], chi = B.geo[4 * b + 3];
+  const R nx = B.nrm[4 * b + 0], ny = B.nrm[4 * b + 1], nz = B.nrm[4 * b + 2];
+  const R pD = trilin<R>(B.pi, q, B.Sx, B.plane, sx, sy, sz);
+  const R uD = trilin<R>(B.ui, q, B.Sx, B.plane, sx, sy, sz);
+  const R vD = trilin<R>(B.vi, q, B.Sx, B.plane, sx, sy, sz);
+  const R wD = trilin<R>(B.wi, q, B.Sx, B.plane, sx, sy, sz);
+  const R un = uD * nx + vD * ny + wD * nz;
+  const R utx = uD - un * nx, uty = vD - un * ny, utz = wD - un * nz;
+  const double wout = (double)pD + B.Z0 * (double)un;  // outgoing characteristic
+  const int m = B.mat[b];
+  const int64_t nB = B.nB;
+  double sumA = 0.0, sumBC = 0.0;
+  for (int k = 0; k < B.K; ++k) {
+    const int mi = m * B.K + k;
+    const int64_t si = (int64_t)k * nB + b;
+    const double r = B.phR[si];
+    const double Lphi = wout - B.zeta[mi] * r;
+    const double v = (B.a_ssp * B.phM[si] + B.b_ssp * (r + B.dt * Lphi)) * B.inv_c_ssp;
+    B.phL[si] = v;
+    sumA += B.A[mi] * v;
+  }
+  for (int l = 0; l < B.L; ++l) {
+    const int mi = m * B.L + l;
+    const int64_t si = (int64_t)l * nB + b;
+    const double r1 = B.s1R[si], r2 = B.s2R[si];
+    const double L1 = wout - (B.alpha[mi] * r1 + B.beta[mi] * r2);
+    const double L2 = B.beta[mi] * r1 - B.alpha[mi] * r2;
+    const double n1 = (B.a_ssp * B.s1M[si] + B.b_ssp * (r1 + B.dt * L1)) * B.inv_c_ssp;
+    const double n2 = (B.a_ssp * B.s2M[si] + B.b_ssp * (r2 + B.dt * L2)) * B.inv_c_ssp;
+    B.s1L[si] = n1;
+    B.s2L[si] = n2;
+    sumBC += B.B[mi] * n1 + B.C[mi] * n2;
+  }
+  const double win = B.Rinf[m] * wout + sumA + sumBC;  // incoming characteristic
+  const R pb = (R)(0.5 * (win + wout));
+  const R unb = (R)((wout - win) / (2.0 * B.Z0));
+  const R ub = unb * nx + utx, vb = unb * ny + uty, wb = unb * nz + utz;
+  const R omc = R(1) - chi;
+  B.uo[cell] = omc * B.uo[cell] + chi * ub;
+  B.vo[cell] = omc * B.vo[cell] + chi * vb;
+  B.wo[cell] = omc * B.wo[cell] + chi * wb;
+  B.po[cell] = omc * B.po[cell] + chi * pb;
+}
+
+// Receiver gather after the last stage of a step (main3D.cu:1399-1414), into a device buffer;
+// then advances the device step counter. One block.
+template <class R>
+__global__ void k_receivers(const R* __restrict__ p, const R* __restrict__ u, const R* __restrict__ v,
+                            const R* __restrict__ w, const int64_t* __restrict__ rcell, int nrec,
+                            double* ir, double* vel, int64_t cap, int64_t* step) {
+  const int64_t n = *step;
+  if (n < cap) {
+    for (int r = threadIdx.x; r < nrec; r += blockDim.x) {
+      const int64_t c = rcell[r];
+      const int64_t o = (int64_t)r * cap + n;
+      ir[o] = (double)p[c];
+      vel[3 * o + 0] = (double)u[c];
+      vel[3 * o + 1] = (double)v[c];
+      vel[3 * o + 2] = (double)w[c];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *step = n + 1;
+}
+
+// FP64 energy 0.5 sum(p^2/(rho c^2) + rho |u|^2) (functions3D.cuh:111-129). Padding cells are
+// zero, so summing the whole allocation sums the grid.
+template <class R>
+__global__ void k_energy(const R* __restrict__ p, const R* __restrict__ u, const R* __restrict__ v,
+                         const R* __restrict__ w, int64_t n, double inv_rc2, double rho, double* out) {
+  double s = 0.0;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    const double pp = p[c], uu = u[c], vv = v[c], ww = w[c];
+    s += pp * pp * inv_rc2 + rho * (uu * uu + vv * vv + ww * ww);
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) atomicAdd(out, 0.5 * s);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Launchers
+// ------------------------------------------------------------------------------------------
+template <class R>
+size_t stage_smem_bytes() {
+  typedef typename Pair<R>::T P;
+  return sizeof(P) * (2 * PH * PW + 2 * TY * (TX + 2) + 2 * (TY + 2) * TX);
+}
+
+template <class R>
+cudaError_t stage_setup() {
+  const int bytes = (int)stage_smem_bytes<R>();
+  cudaError_t e;
+  e = cudaFuncSetAttribute(k_stage<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_stage<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_stage<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+template <class R>
+cudaError_t stage_occupancy(int* blocks_per_sm) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_stage<R, 0>, NTHREADS,
+                                                        stage_smem_bytes<R>());
+}
+
+template <class R>
+cudaError_t launch_stage(int stage, const StageArgs<R>& a, dim3 grid, cudaStream_t s) {
+  const dim3 block(TX, TY, 1);
+  const size_t smem = stage_smem_bytes<R>();
+  if (stage == 0)
+    k_stage<R, 0><<<grid, block, smem, s>>>(a);
+  else if (stage == 1)
+    k_stage<R, 1><<<grid, block, smem, s>>>(a);
+  else
+    k_stage<R, 2><<<grid, block, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <class R>
+cudaError_t launch_band(const BandArgs<R>& a, cudaStream_t s) {
+  if (a.nB <= 0) return cudaSuccess;
+  const int bs = 256;
+  const int64_t nb = (a.nB + bs - 1) / bs;
+  k_band<R><<<(unsigned)nb, bs, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <class R>
+cudaError_t launch_receivers(const R* p, const R* u, const R* v, const R* w, const int64_t* rcell, int nrec,
+                             double* ir, double* vel, int64_t cap, int64_t* step, cudaStream_t s) {
+  k_receivers<R><<<1, 256, 0, s>>>(p, u, v, w, rcell, nrec, ir, vel, cap, step);
+  return cudaGetLastError();
+}
+
+template <class R>
+cudaError_t launch_energy(const R* p, const R* u, const R* v, const R* w, int64_t n, double inv_rc2,
+                          double rho, double* out, int nsm, cudaStream_t s) {
+  k_energy<R><<<nsm * 4, 256, 0, s>>>(p, u, v, w, n, inv_rc2, rho, out);
+  return cudaGetLastError();
+}
+
+#define FZ_INSTANTIATE(R)                                                                          \
+  template size_t stage_smem_bytes<R>();                                                           \
+  template cudaError_t stage_setup<R>();                                                           \
+  template cudaError_t stage_occupancy<R>(int*);                                                   \
+  template cudaError_t launch_stage<R>(int, const StageArgs<R>&, dim3, cudaStream_t);              \
+  template cudaError_t launch_band<R>(const BandArgs<R>&, cudaStream_t);                           \
+  template cudaError_t launch_receivers<R>(const R*, const R*, const R*, const R*, const int64_t*, \
+                                           int, double*, double*, int64_t, int64_t*,               \
+                                           cudaStream_t);                                          \
+  template cudaError_t launch_energy<R>(const R*, const R*, const R*, const R*, int64_t, double,   \
+                                        double, double*, int, cudaStream_t);
+
+FZ_INSTANTIATE(float)
+FZ_INSTANTIATE(double)
+
+}  // namespace fz

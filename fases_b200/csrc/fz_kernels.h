@@ -1,0 +1,28 @@
+// fz_kernels.h -- host-callable launchers of the sm_100a stepping kernels (fz_kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fz_device.cuh"
+
+namespace fz {
+
+template <class R>
+size_t stage_smem_bytes();
+template <class R>
+cudaError_t stage_setup();
+template <class R>
+cudaError_t stage_occupancy(int* blocks_per_sm);
+template <class R>
+cudaError_t launch_stage(int stage, const StageArgs<R>& a, dim3 grid, cudaStream_t s);
+template <class R>
+cudaError_t launch_band(const BandArgs<R>& a, cudaStream_t s);
+template <class R>
+cudaError_t launch_receivers(const R* p, const R* u, const R* v, const R* w, const int64_t* rcell,
+                             int nrec, double* ir, double* vel, int64_t cap, int64_t* step,
+                             cudaStream_t s);
+template <class R>
+cudaError_t launch_energy(const R* p, const R* u, const R* v, const R* w, int64_t n, double inv_rc2,
+                          double rho, double* out, int nsm, cudaStream_t s);
+
+}  // namespace fz

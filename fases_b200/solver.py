@@ -1,0 +1,240 @@
+"""Python mirror of the fases3D solver interface, on top of libfz.so.
+
+`Solver` is the library form of one `fases3D` FVM run (3D-solver/core/main3D.cu:26-1449):
+geometry (S, oid) -> materials -> sources -> receivers -> `run(nsteps)` -> receiver traces and the
+reference output files. `Solver.from_project` takes the same four paths as the `fases3D` command
+line and reads the reference's project files.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _abi
+from ._abi import FzParams, check, lib
+
+
+def _dptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+
+
+def params(h=0.02, c=None, rho=None, dt=None, cfl=0.5, pml=(0, 0, 0, 0, 0, 0), pml_cells=20,
+           precision="fp32", device=0, tol_cells=3.0):
+    """Solver parameters. c/rho default to the reference's 20 degC air (main3D.cu:450-456);
+    dt = cfl*h/c (main3D.cu:729-730). pml = (U, D, R, L, F, B) face keys (main3D.cu:155-160)."""
+    p = FzParams()
+    check(lib().fz_params_init(C.byref(p)))
+    p.precision = _abi.FZ_FP64 if precision == "fp64" else _abi.FZ_FP32
+    p.device = int(device)
+    p.pml_cells = int(pml_cells)
+    for f in range(6):
+        p.pml[f] = int(bool(pml[f]))
+    p.h = float(h)
+    if c is not None:
+        p.c = float(c)
+    if rho is not None:
+        p.rho = float(rho)
+    p.dt = float(dt) if dt is not None else float(cfl) * p.h / p.c
+    p.tol_cells = float(tol_cells)
+    return p
+
+
+class Solver:
+    """One GPU solver instance (a libfz handle). Not thread-safe; one CUDA stream."""
+
+    def __init__(self, prm: FzParams = None, _handle=None, **kw):
+        self._h = None
+        if _handle is not None:
+            self._h = _handle
+        else:
+            prm = prm if prm is not None else params(**kw)
+            h = C.c_void_p()
+            check(lib().fz_create(C.byref(prm), C.byref(h)))
+            self._h = h
+        self._nrec = 0
+        self._cap = 0
+
+    # -- lifetime --------------------------------------------------------------------------
+    def close(self):
+        if self._h:
+            lib().fz_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _chk(self, rc):
+        return check(rc, self._h)
+
+    # -- setup -----------------------------------------------------------------------------
+    def load_geometry(self, S, oid):
+        """S: float32 [Nz,Ny,Nx] signed distance (air > 0); oid: uint8 [Nz,Ny,Nx] material id + 1
+        (0xFF none) -- the reference's output/S.bin and output/oid.bin as 3-D arrays."""
+        S = np.ascontiguousarray(S, dtype=np.float32)
+        oid = np.ascontiguousarray(oid, dtype=np.uint8)
+        if S.shape != oid.shape or S.ndim != 3:
+            raise ValueError("S and oid must be 3-D arrays of the same shape [Nz, Ny, Nx]")
+        Nz, Ny, Nx = S.shape
+        self._chk(lib().fz_load_geometry_raw(
+            self._h, S.ctypes.data_as(C.POINTER(C.c_float)), oid.ctypes.data_as(C.POINTER(C.c_uint8)),
+            Nx, Ny, Nz))
+        self.shape = (Nz, Ny, Nx)
+
+    def set_materials(self, Rinf, A=None, zeta=None, B=None, Cc=None, alpha=None, beta=None):
+        """Per material m: Rinf[m], real poles A/zeta[m, K], complex pairs B/C/alpha/beta[m, L]."""
+        Rinf = np.ascontiguousarray(Rinf, dtype=np.float64).reshape(-1)
+        n = Rinf.size
+        def arr(x):
+            if x is None:
+                return np.zeros((n, 0))
+            return np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(n, -1))
+        A, zeta, B, Cc, alpha, beta = map(arr, (A, zeta, B, Cc, alpha, beta))
+        K, L = A.shape[1], B.shape[1]
+        self._chk(lib().fz_set_materials(self._h, n, K, L, _dptr(Rinf), _dptr(A), _dptr(zeta), _dptr(B),
+                                         _dptr(Cc), _dptr(alpha), _dptr(beta)))
+
+    def set_sources(self, cells, sval, src_opt=0, u_s=None, freq=None):
+        cells = np.ascontiguousarray(cells, dtype=np.int32).reshape(-1, 3)
+        sval = np.ascontiguousarray(sval, dtype=np.float64).reshape(-1)
+        us = None if u_s is None else np.ascontiguousarray(u_s, dtype=np.float64)
+        fr = None if freq is None else np.ascontiguousarray(freq, dtype=np.float64)
+        self._chk(lib().fz_set_sources(self._h, cells.shape[0], cells.ctypes.data_as(C.POINTER(C.c_int32)),
+                                       _dptr(sval), int(src_opt), _dptr(fr), _dptr(us),
+                                       0 if us is None else us.size))
+
+    def set_receivers(self, cells, capacity_steps):
+        cells = np.ascontiguousarray(cells, dtype=np.int32).reshape(-1, 3)
+        self._chk(lib().fz_set_receivers(self._h, cells.shape[0], cells.ctypes.data_as(C.POINTER(C.c_int32)),
+                                         int(capacity_steps)))
+        self._nrec = cells.shape[0]
+        self._cap = int(capacity_steps)
+
+    def set_fields(self, p=None, u=None, v=None, w=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (p, u, v, w)]
+        self._chk(lib().fz_set_fields(self._h, *[_dptr(a) for a in arrs]))
+
+    # -- stepping --------------------------------------------------------------------------
+    def run(self, nsteps, sync=True, timeout_ms=0):
+        self._chk(lib().fz_run(self._h, int(nsteps)))
+        if sync:
+            self.sync(timeout_ms)
+
+    def run_timed(self, nsteps):
+        """Runs nsteps and returns their device time in ms (CUDA events on the solver's stream)."""
+        ms = C.c_double()
+        self._chk(lib().fz_run_timed(self._h, int(nsteps), C.byref(ms)))
+        return ms.value
+
+    def sync(self, timeout_ms=0):
+        self._chk(lib().fz_sync(self._h, int(timeout_ms)))
+
+    def steps_done(self):
+        n = C.c_int64()
+        self._chk(lib().fz_steps_done(self._h, C.byref(n)))
+        return n.value
+
+    # -- results ---------------------------------------------------------------------------
+    def _nsamples(self):
+        return min(self.steps_done(), self._cap)
+
+    def ir(self, fp64=True):
+        n = self._nsamples()
+        if fp64:
+            out = np.zeros((self._nrec, n), np.float64)
+            self._chk(lib().fz_get_ir64(self._h, out.ctypes.data_as(C.POINTER(C.c_double)), out.size))
+        else:
+            out = np.zeros((self._nrec, n), np.float32)
+            self._chk(lib().fz_get_ir(self._h, out.ctypes.data_as(C.POINTER(C.c_float)), out.size))
+        return out
+
+    def vel(self):
+        n = self._nsamples()
+        out = np.zeros((self._nrec, n, 3), np.float32)
+        self._chk(lib().fz_get_vel(self._h, out.ctypes.data_as(C.POINTER(C.c_float)), out.size))
+        return out
+
+    def fields(self):
+        Nz, Ny, Nx = self.shape
+        out = [np.zeros((Nz, Ny, Nx), np.float64) for _ in range(4)]
+        self._chk(lib().fz_get_fields(self._h, *[_dptr(a) for a in out]))
+        return out
+
+    def energy(self):
+        e = C.c_double()
+        self._chk(lib().fz_energy(self._h, C.byref(e)))
+        return e.value
+
+    def info(self):
+        dims = (C.c_int32 * 3)()
+        nb, nu = C.c_int64(), C.c_int64()
+        self._chk(lib().fz_info(self._h, dims, C.byref(nb), C.byref(nu)))
+        return {"dims": tuple(dims), "n_band": nb.value, "n_update": nu.value}
+
+    def profile(self, on=True):
+        self._chk(lib().fz_profile_enable(self._h, 1 if on else 0))
+
+    def profile_read(self):
+        ms = (C.c_double * 8)()
+        n = (C.c_int64 * 8)()
+        self._chk(lib().fz_profile_read(self._h, ms, n, 8))
+        kinds = ["stage0", "stage1", "stage2", "band", "receivers"]
+        return {k: (ms[i], n[i]) for i, k in enumerate(kinds)}
+
+    def write_outputs(self, output_dir, src_idx=0, scene_name="scene"):
+        os.makedirs(output_dir, exist_ok=True)
+        self._chk(lib().fz_write_outputs(self._h, output_dir.encode(), int(src_idx), scene_name.encode()))
+
+    # -- whole reference project -----------------------------------------------------------
+    @classmethod
+    def from_project(cls, scene, config, src, rec, precision="fp32", device=0):
+        """Same four inputs as `fases3D <scene.obj> <config.txt> <src.txt> <rec.txt>`; returns
+        (solver, Nt)."""
+        h = C.c_void_p()
+        nt = C.c_int64()
+        rc = lib().fz_load_project(os.fsencode(scene), os.fsencode(config), os.fsencode(src), os.fsencode(rec),
+                                   _abi.FZ_FP64 if precision == "fp64" else _abi.FZ_FP32, int(device),
+                                   C.byref(h), C.byref(nt))
+        check(rc)
+        s = cls(_handle=h)
+        # receivers were set by the loader with capacity Nt
+        s._cap = nt.value
+        info = s.info()
+        s.shape = tuple(reversed(info["dims"]))
+        s._nrec = _count_rec(rec)
+        return s, nt.value
+
+
+def _count_rec(path):
+    n = 0
+    with open(path) as f:
+        for line in f:
+            if not line.strip() or line.startswith("#"):
+                continue
+            parts = line.split()
+            try:
+                [float(x) for x in parts[:3]]
+            except ValueError:
+                continue
+            if len(parts) >= 3:
+                n += 1
+    return n
+
+
+def source_waveform(src_opt, glob_f, f_cutoff, dt, Nt, h, rho):
+    """(u_s, p_ref, p_peak) of main3D.cu:963-1110, 2*Nt+1 samples at dt/2."""
+    n = 2 * int(Nt) + 1
+    us = np.zeros(n)
+    pr = np.zeros(n)
+    pk = C.c_double()
+    check(lib().fz_source_waveform(int(src_opt), float(glob_f), float(f_cutoff), float(dt), int(Nt), float(h),
+                                   float(rho), _dptr(us), _dptr(pr), C.byref(pk)))
+    return us, pr, pk.value

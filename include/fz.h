@@ -1,0 +1,183 @@
+/*
+ * fz.h -- C ABI of the B200-native FASES time-domain stepper (libfz.so).
+ *
+ * The reference solver (vitorotri/fases, F.A.S.E.S v0.9) has no library or plugin API: its
+ * boundary is the process contract of the `fases3D` executable (argv + project files + stdout),
+ * driven by `common/gui.py` through `subprocess.Popen`. This header is the function-level form
+ * of that contract. Every entry point below names the piece of `fases3D` it replaces
+ * (paths relative to the reference project root).
+ *
+ * Conventions
+ *   - Every function returns an int status: FZ_OK (0) or a negative FZ_E* code. Nothing in the
+ *     library calls exit(); the reference calls std::exit inside read_fit_file
+ *     (common/filterABC.h:24-29,44-48). The text of the last error is returned by
+ *     fz_last_error() (per handle) or fz_global_error() (for calls without a handle).
+ *   - Host arrays are owned by the caller and copied on entry; fz_get_* copy into caller buffers.
+ *     No device pointer ever escapes the library.
+ *   - Grid arrays passed across the ABI use the reference layout: cell (i,j,k) at
+ *     i + Nx*(j + Ny*k), x fastest (3D-solver/core/functions3D.cuh:48-50). The device layout is
+ *     private (rows padded and aligned to 128 bytes).
+ *   - One CUDA stream per handle. A handle is not thread-safe; distinct handles may run
+ *     concurrently on one GPU. Only fz_sync and fz_get_* wait for the device, and every wait is
+ *     a bounded poll that returns FZ_ETIMEOUT instead of hanging.
+ */
+#ifndef FZ_H
+#define FZ_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FZ_ABI_VERSION 1
+
+/* status codes */
+#define FZ_OK 0
+#define FZ_EINVAL -1       /* bad argument */
+#define FZ_ENOMEM -2       /* host or device allocation failed */
+#define FZ_ECUDA -3        /* CUDA runtime error (text in fz_last_error) */
+#define FZ_EIO -4          /* file could not be opened, read or written */
+#define FZ_EPARSE -5       /* malformed config / .fit / poles / src / rec file */
+#define FZ_ESTATE -6       /* call out of order (e.g. fz_run before geometry) */
+#define FZ_ETIMEOUT -7     /* a bounded device wait gave up */
+#define FZ_ENONFINITE -8   /* health check found NaN/Inf in the state */
+#define FZ_ENODEV -9       /* no usable CUDA device */
+
+/* precision modes */
+#define FZ_FP32 0  /* FP32 field state; FP64 ADE state, receiver samples and energy (default) */
+#define FZ_FP64 1  /* every field and state in FP64 */
+
+/* source waveform types: config.txt line 16 (3D-solver/core/main3D.cu:968) */
+#define FZ_SRC_PCS 0
+#define FZ_SRC_RICKER 1
+#define FZ_SRC_SINE 2
+
+typedef struct fz_handle fz_handle;
+
+/* Solver parameters. Replaces the scalar part of main3D.cu's setup:
+ * h = config[0] (main3D.cu:132); c, rho (454-456); dt = CFL*h/c (729-730);
+ * PML keys U D R L F B = config[6..11] (155-160); PML_CELLS (functions3D.cuh:12-14);
+ * tol = 3h (main3D.cu:224). */
+typedef struct fz_params {
+  int32_t abi_version; /* must be FZ_ABI_VERSION */
+  int32_t precision;   /* FZ_FP32 or FZ_FP64 */
+  int32_t device;      /* CUDA device ordinal */
+  int32_t pml_cells;   /* cPML thickness in cells (reference: 20) */
+  int32_t pml[6];      /* face flags in reference order U,D,R,L,F,B = z-hi,z-lo,x-hi,x-lo,y-hi,y-lo */
+  double h;            /* grid spacing [m] */
+  double c;            /* speed of sound [m/s] */
+  double rho;          /* air density [kg/m^3] */
+  double dt;           /* time step [s] */
+  double tol_cells;    /* immersed blending band in cells: tol = tol_cells*h (reference: 3) */
+} fz_params;
+
+/* Fills p with the reference defaults: FP32, device 0, 20 PML cells, no PML faces, h = 0.02,
+ * T = 20 degC -> c = sqrt(1.4*287.05*293.15), rho = 1.225, CFL 0.5, tol = 3h. */
+int fz_params_init(fz_params* p);
+
+/* Creates a solver on p->device. Replaces main3D.cu:235-293 (device probe) and the allocation
+ * block 755-843. Device memory is allocated later, by fz_load_geometry_raw. */
+int fz_create(const fz_params* p, fz_handle** out);
+void fz_destroy(fz_handle* h);
+
+/* Immersed geometry, as the reference caches it in output/S.bin (float32 signed distance, positive
+ * in air) and output/oid.bin (uint8 material id, 0xFF = none) (main3D.cu:350-364, 410-421).
+ * Nx,Ny,Nz are the padded grid (room + 3 ghost cells per side, parsing3D.h:128).
+ * Builds the cell-class bytes, the compact band list in build_boundary_map order
+ * (common/filterABC.h:95-108) with its precomputed probe geometry
+ * (functions3D.cuh:483-512), and zeroes all fields (main3D.cu:755-802). */
+int fz_load_geometry_raw(fz_handle* h, const float* S, const uint8_t* oid, int32_t Nx, int32_t Ny,
+                         int32_t Nz);
+
+/* ADE materials. Replaces read_fit_file per layer (common/filterABC.h:31-90) plus the device
+ * copies (main3D.cu:639-658). Arrays use the reference's flat(k, m, K) = m*K + k layout:
+ * Rinf[nMat], A/zeta[nMat*K], B/C/alpha/beta[nMat*L]. Material m is oid m+1. */
+int fz_set_materials(fz_handle* h, int32_t nMat, int32_t K, int32_t L, const double* Rinf,
+                     const double* A, const double* zeta, const double* B, const double* C,
+                     const double* alpha, const double* beta);
+
+/* Point sources. cell_ijk[3*n] are grid cells ((int)(x/h)+3 per axis, main3D.cu:874-876);
+ * sval[n] the scaled source strengths (main3D.cu:1071-1110); u_s[n_us] the shared waveform at
+ * dt/2 spacing (length >= 2*Nt+1, main3D.cu:963-1124); for FZ_SRC_SINE freq[n] are per-source
+ * frequencies and u_s may be NULL. Replaces kernel_inject_src_SSP (functions3D.cuh:1039-1047). */
+int fz_set_sources(fz_handle* h, int32_t n, const int32_t* cell_ijk, const double* sval,
+                   int32_t src_opt, const double* freq, const double* u_s, int64_t n_us);
+
+/* Receivers at grid cells cell_ijk[3*n] ((int)(x/h)+3, main3D.cu:938-940). Samples p and
+ * (u,v,w) after every step into a device buffer of capacity_steps samples per receiver
+ * (replaces the per-step cudaMemcpy at main3D.cu:1399-1414). */
+int fz_set_receivers(fz_handle* h, int32_t n, const int32_t* cell_ijk, int64_t capacity_steps);
+
+/* Initial fields in the reference layout (any pointer may be NULL = zero). The reference always
+ * starts quiescent (main3D.cu:1134-1135); this is the Gaussian-pulse initial condition of the
+ * synthetic benchmarks and the hook the tests use. */
+int fz_set_fields(fz_handle* h, const double* p, const double* u, const double* v, const double* w);
+
+/* Enqueues nsteps SSP-RK3 steps on the handle's stream and returns. One step is the reference
+ * time-loop body main3D.cu:1280-1319 + 1399-1414: three fused stage kernels (WENO-Z, Godunov
+ * flux, RK combination, cPML, source), each followed by the immersed ADE band update, then the
+ * receiver gather. */
+int fz_run(fz_handle* h, int64_t nsteps);
+
+/* fz_run bracketed by CUDA events on the handle's stream, followed by a bounded wait; *ms gets
+ * the device time of the nsteps steps. */
+int fz_run_timed(fz_handle* h, int64_t nsteps, double* ms);
+
+/* Bounded wait for all enqueued work (timeout_ms <= 0: 600000 ms). */
+int fz_sync(fz_handle* h, int64_t timeout_ms);
+
+/* Steps completed so far (after fz_sync). */
+int fz_steps_done(fz_handle* h, int64_t* n);
+
+/* Receiver traces [n_rec][n_steps] (float32, as IR<r>_<s>.bin, main3D.cu:1403-1404) and
+ * [n_rec][n_steps][3] velocities (as VEL<r>_<s>.bin, main3D.cu:1408-1412). cap = elements. */
+int fz_get_ir(fz_handle* h, float* out, int64_t cap);
+int fz_get_ir64(fz_handle* h, double* out, int64_t cap);
+int fz_get_vel(fz_handle* h, float* out, int64_t cap);
+
+/* Current state (the reference's U0 after the swap, main3D.cu:1312-1315), reference layout. */
+int fz_get_fields(fz_handle* h, double* p, double* u, double* v, double* w);
+
+/* FP64 acoustic energy 0.5*sum(p^2/(rho c^2) + rho |u|^2) * h^3 over the grid (the unused
+ * host diagnostic functions3D.cuh:111-129, evaluated on the device in FP64). */
+int fz_energy(fz_handle* h, double* E);
+
+/* Writes output_dir/IR<r>_<src_idx>.bin and VEL<r>_<src_idx>.bin (main3D.cu:1251-1256) and
+ * output_dir/header.txt (main3D.cu:1441-1449) from the samples taken so far. */
+int fz_write_outputs(fz_handle* h, const char* output_dir, int32_t src_idx, const char* scene_name);
+
+/* Grid and band facts: dims[3], n_band, n_update (cells the stage kernels write). */
+int fz_info(fz_handle* h, int32_t* dims, int64_t* n_band, int64_t* n_update);
+
+/* Per-kernel-kind device time. When enabled, every launch in fz_run is bracketed by CUDA events
+ * on the handle's stream; fz_profile_read returns accumulated milliseconds and launch counts for
+ * kinds 0..2 = stage kernels 0,1,2; 3 = band kernels; 4 = receiver gather. */
+int fz_profile_enable(fz_handle* h, int32_t on);
+int fz_profile_read(fz_handle* h, double* ms, int64_t* launches, int32_t nkinds);
+
+/* Whole reference project: config/config.txt, config/poles.txt, input/fit/<layer>.fit,
+ * src.txt, rec.txt (main3D.cu:66-160, 587-634, 861-959) with the geometry from the reference's
+ * scene cache output/S.bin + output/oid.bin + output/scene_cache.txt (main3D.cu:334-380).
+ * Creates the handle, loads geometry, materials, sources (with the PCS/Ricker/sine waveform and
+ * its scaling, main3D.cu:963-1124), receivers, and writes config/p_ref.bin (main3D.cu:1096-1108)
+ * and output/pre_header.txt (main3D.cu:527-532). n_steps_out receives Nt (main3D.cu:752). */
+int fz_load_project(const char* scene_path, const char* config_path, const char* src_path,
+                    const char* rec_path, int32_t precision, int32_t device, fz_handle** out,
+                    int64_t* n_steps_out);
+
+/* Source waveform exactly as main3D.cu:963-1124 computes it: u_s[0..2Nt] (double) for
+ * src_opt PCS or Ricker, and the radiated reference pulse p_ref[0..2Nt] per unit source
+ * (main3D.cu:1084-1090) with its peak. */
+int fz_source_waveform(int32_t src_opt, double glob_f, double f_cutoff, double dt, int64_t Nt,
+                       double h, double rho, double* u_s, double* p_ref, double* p_peak);
+
+int fz_last_error(fz_handle* h, char* buf, size_t cap);
+int fz_global_error(char* buf, size_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FZ_H */

@@ -1,0 +1,21 @@
+#!/usr/bin/env bash
+# Builds the reference FASES 3D solver (vitorotri/fases v0.9) from its own sources, unmodified,
+# for sm_100a, into oracle/_ref/fases3D. It is the checker the CPU restatement is pinned
+# against (tests/golden/make_golden.py runs it on a B200); it is never part of the product.
+# The source tree is read in place; nothing is copied into this repository.
+# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+set -euo pipefail
+REF="${1:-/root/reference}"
+HERE="$(cd "$(dirname "$0")" && pwd)"
+OUT="$HERE/_ref"
+mkdir -p "$OUT"
+if [ ! -f "$REF/3D-solver/core/main3D.cu" ]; then
+  echo "reference sources not found under $REF" >&2
+  exit 2
+fi
+# Same flags as 3D-solver/Makefile:1-32 with ARCH set to sm_100a.
+nvcc -std=c++17 -O3 -gencode arch=compute_100a,code=sm_100a -Xcompiler -fopenmp \
+  -I"$REF/3D-solver/include" -I"$REF/common" \
+  "$REF/3D-solver/core/main3D.cu" -o "$OUT/fases3D" 2> "$OUT/build.log" || {
+    cat "$OUT/build.log" >&2; exit 1; }
+echo "built $OUT/fases3D"

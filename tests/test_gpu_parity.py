@@ -1,0 +1,86 @@
+"""CUDA stepper vs the FP64 CPU oracle on seeded small rooms (cPML, obstacle, six ADE walls,
+PCS source, Gaussian pulse, receivers). Calls go through the C ABI (libfz.so via ctypes)."""
+import numpy as np
+import pytest
+
+from tests.helpers import rel_l2, run_gpu, run_oracle, small_room
+
+pytestmark = pytest.mark.gpu
+
+# FP64 GPU vs FP64 oracle: same scheme, only the operation order differs.
+TOL_FP64 = 1e-10
+# FP32 GPU vs FP64 oracle, receiver traces, relative L2 (the plain-path accuracy target is 1e-5).
+TOL_FP32_IR = 1e-5
+
+
+def _first_mismatch(a, b, tol):
+    d = np.abs(a - b)
+    scale = np.max(np.abs(b)) + 1e-300
+    idx = np.argwhere(d > tol * scale)
+    return None if idx.size == 0 else (tuple(idx[0]), a[tuple(idx[0])], b[tuple(idx[0])])
+
+
+@pytest.mark.parametrize("steps", [1, 3])
+def test_fields_fp64_few_steps(steps):
+    cfg = small_room(seed=1, steps=steps)
+    s = run_gpu(cfg, "fp64")
+    o = run_oracle(cfg)
+    g = s.fields()
+    r = o.fields()
+    for name, a, b in zip("puvw", g, r):
+        err = rel_l2(a, b)
+        assert err < TOL_FP64, (name, err, _first_mismatch(a, b, 1e-9))
+
+
+def test_ir_fp64_long():
+    cfg = small_room(seed=2, steps=120)
+    s = run_gpu(cfg, "fp64")
+    o = run_oracle(cfg)
+    ir_o, vel_o = o.ir()
+    ir_g = s.ir()
+    assert ir_g.shape == ir_o.shape
+    assert rel_l2(ir_g, ir_o) < TOL_FP64
+    vel_g = s.vel()
+    assert rel_l2(vel_g, vel_o) < 1e-6  # VEL is returned as float32
+
+
+def test_ir_fp32_vs_fp64_oracle():
+    cfg = small_room(seed=3, steps=120)
+    s = run_gpu(cfg, "fp32")
+    o = run_oracle(cfg)
+    ir_o, _ = o.ir()
+    ir_g = s.ir()
+    errs = [rel_l2(ir_g[r], ir_o[r]) for r in range(ir_o.shape[0])]
+    assert max(errs) < TOL_FP32_IR, errs
+
+
+def test_graph_and_direct_launches_agree():
+    cfg = small_room(seed=4, steps=25)  # 2 graphs of 10 steps + 5 direct steps
+    a = run_gpu(cfg, "fp32", graph=True)
+    b = run_gpu(cfg, "fp32", graph=False)
+    assert np.array_equal(a.ir(), b.ir())
+    for x, y in zip(a.fields(), b.fields()):
+        assert np.array_equal(x, y)
+
+
+def test_no_pml_no_source_pulse_only():
+    cfg = small_room(seed=5, pml=(0, 0, 0, 0, 0, 0), source=None, steps=40)
+    s = run_gpu(cfg, "fp64")
+    o = run_oracle(cfg)
+    for a, b in zip(s.fields(), o.fields()):
+        assert rel_l2(a, b) < TOL_FP64
+
+
+def test_all_pml_faces():
+    cfg = small_room(seed=6, room=(30, 30, 30), pml=(1, 1, 1, 1, 1, 1), pml_cells=5, obstacle=False, steps=40)
+    s = run_gpu(cfg, "fp64")
+    o = run_oracle(cfg)
+    for a, b in zip(s.fields(), o.fields()):
+        assert rel_l2(a, b) < TOL_FP64
+
+
+def test_energy_matches_oracle():
+    cfg = small_room(seed=7, steps=30)
+    s = run_gpu(cfg, "fp64")
+    o = run_oracle(cfg)
+    assert abs(s.energy() - o.energy()) <= 1e-10 * abs(o.energy())
