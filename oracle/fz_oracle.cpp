@@ -167,9 +167,9 @@ struct Oracle {
     const R sy = Bf * pref * std::pow(ym, m) + Ff * pref * std::pow(yp, m);
     const R sz = Df * pref * std::pow(zm, m) + Uf * pref * std::pow(zp, m);
     const R dx = Lf * xm + Rf * xp, dy = Bf * ym + Ff * yp, dz = Df * zm + Uf * zp;
-    const R kx = 1.0 + (kappa_max - 1.0) * std::pow(dx, m);
-    const R ky = 1.0 + (kappa_max - 1.0) * std::pow(dy, m);
-    const R kz = 1.0 + (kappa_max - 1.0) * std::pow(dz, m);
+    const R kapx = 1.0 + (kappa_max - 1.0) * std::pow(dx, m);
+    const R kapy = 1.0 + (kappa_max - 1.0) * std::pow(dy, m);
+    const R kapz = 1.0 + (kappa_max - 1.0) * std::pow(dz, m);
     const R ax = alpha_min + (alpha_max - alpha_min) * (1.0 - dx);
     const R ay = alpha_min + (alpha_max - alpha_min) * (1.0 - dy);
     const R az = alpha_min + (alpha_max - alpha_min) * (1.0 - dz);
@@ -186,23 +186,23 @@ struct Oracle {
     if (bx) {
       const int ix = (i < ng + d) ? (i - ng) : (i - (Nx - ng - d) + d);
       const size_t X = (size_t)ix + (size_t)(2 * d) * ((size_t)j + (size_t)Ny * k);
-      out.p[c] += wdt * corr(Lpx, kx, psi_px[X]);
-      out.u[c] += wdt * corr(Lux, kx, psi_ux[X]);
-      if (advance) { adv(Lpx, kx, sx, ax, psi_px[X]); adv(Lux, kx, sx, ax, psi_ux[X]); }
+      out.p[c] += wdt * corr(Lpx, kapx, psi_px[X]);
+      out.u[c] += wdt * corr(Lux, kapx, psi_ux[X]);
+      if (advance) { adv(Lpx, kapx, sx, ax, psi_px[X]); adv(Lux, kapx, sx, ax, psi_ux[X]); }
     }
     if (by) {
       const int jy = (j < ng + d) ? (j - ng) : (j - (Ny - ng - d) + d);
       const size_t Y = (size_t)i + (size_t)Nx * ((size_t)jy + (size_t)(2 * d) * k);
-      out.p[c] += wdt * corr(Lpy, ky, psi_py[Y]);
-      out.v[c] += wdt * corr(Lvy, ky, psi_vy[Y]);
-      if (advance) { adv(Lpy, ky, sy, ay, psi_py[Y]); adv(Lvy, ky, sy, ay, psi_vy[Y]); }
+      out.p[c] += wdt * corr(Lpy, kapy, psi_py[Y]);
+      out.v[c] += wdt * corr(Lvy, kapy, psi_vy[Y]);
+      if (advance) { adv(Lpy, kapy, sy, ay, psi_py[Y]); adv(Lvy, kapy, sy, ay, psi_vy[Y]); }
     }
     if (bz) {
-      const int kz = (k < ng + d) ? (k - ng) : (k - (Nz - ng - d) + d);
-      const size_t Z = (size_t)i + (size_t)Nx * ((size_t)j + (size_t)Ny * kz);
-      out.p[c] += wdt * corr(Lpz, kz, psi_pz[Z]);
-      out.w[c] += wdt * corr(Lwz, kz, psi_wz[Z]);
-      if (advance) { adv(Lpz, kz, sz, az, psi_pz[Z]); adv(Lwz, kz, sz, az, psi_wz[Z]); }
+      const int kt = (k < ng + d) ? (k - ng) : (k - (Nz - ng - d) + d);
+      const size_t Z = (size_t)i + (size_t)Nx * ((size_t)j + (size_t)Ny * kt);
+      out.p[c] += wdt * corr(Lpz, kapz, psi_pz[Z]);
+      out.w[c] += wdt * corr(Lwz, kapz, psi_wz[Z]);
+      if (advance) { adv(Lpz, kapz, sz, az, psi_pz[Z]); adv(Lwz, kapz, sz, az, psi_wz[Z]); }
     }
   }
 
