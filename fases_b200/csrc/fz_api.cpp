@@ -1,5 +1,6 @@
 // fz_api.cpp -- C ABI of the stepper (include/fz.h): handle lifetime, geometry and band setup,
 // materials, sources, receivers, the step loop with CUDA graphs, bounded waits and readback.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -92,6 +93,39 @@ void free_device(fz_handle* h) {
   dfree(h->d_rec_cell);
   dfree(h->d_ir);
   dfree(h->d_vel);
+}
+
+// cuTensorMapEncodeTiled, fetched from the driver at run time (no link-time libcuda dependency).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+
+// 3-D map over one device field (Sx x Ny x Nz elements) with PW x PH x 1 boxes; reads outside
+// the allocation fill with zeros.
+int make_field_map(fz_handle* h, CUtensorMap* map, void* base) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return set_error(h, FZ_ECUDA, "cuTensorMapEncodeTiled not available from the driver");
+  const cuuint64_t dims[3] = {(cuuint64_t)h->Sx, (cuuint64_t)h->Ny, (cuuint64_t)h->Nz};
+  const cuuint64_t strides[2] = {(cuuint64_t)h->Sx * h->rsize, (cuuint64_t)h->plane * h->rsize};
+  const cuuint32_t box[3] = {(cuuint32_t)fz::PW, (cuuint32_t)fz::PH, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = enc(map, h->fp64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base,
+                         dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_error(h, FZ_ECUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+  return FZ_OK;
 }
 
 // Per-axis cPML coefficient table, restated from functions3D.cuh:689-723 (evaluated once here in
@@ -356,6 +390,7 @@ fz::StageArgs<R> stage_args(fz_handle* h, int stage) {
   a.nn_add = (stage == 0) ? 0 : (stage == 1) ? 2 : 1;  // main3D.cu:1288, 1296, 1304
   a.half_dt = (R)(0.5 * p.dt);
   a.step = h->d_step;
+  a.err = h->d_err;
   return a;
 }
 
@@ -423,7 +458,8 @@ cudaError_t enqueue_step(fz_handle* h) {
   for (int st = 0; st < 3; st++) {
     {
       Timer t(h, st);
-      e = fz::launch_stage<R>(st, stage_args<R>(h, st), h->stage_grid, h->stream);
+      const int in_set = (st == 0) ? h->i0 : (st == 1) ? h->i1 : h->i2;
+      e = fz::launch_stage<R>(st, stage_args<R>(h, st), h->maps[in_set], h->stage_grid, h->stream);
       if (e != cudaSuccess) return e;
     }
     if (h->nB > 0) {
@@ -498,6 +534,12 @@ int load_geometry(fz_handle* h, const float* S, const uint8_t* oid, int Nx, int 
       FZ_CUDA(h, cudaMemset(h->U[s][f], 0, bytes), "cudaMemset(fields)");
     }
   // cell classes: update where the stage kernels would not return early (functions3D.cuh:1091-1097)
+  for (int s = 0; s < 3; s++) {
+    int rc = make_field_map(h, &h->maps[s].p, h->U[s][0]);
+    if (rc == FZ_OK) rc = make_field_map(h, &h->maps[s].u, h->U[s][1]);
+    if (rc == FZ_OK) rc = make_field_map(h, &h->maps[s].v, h->U[s][2]);
+    if (rc != FZ_OK) return rc;
+  }
   h->cls_host.assign((size_t)h->ncell_dev, 0);
   int64_t nup = 0;
   const float hf = (float)h->prm.h;
@@ -626,6 +668,8 @@ int fz_create(const fz_params* p, fz_handle** out) {
   if (e == cudaSuccess) e = cudaMalloc(&h->d_step, sizeof(int64_t));
   if (e == cudaSuccess) e = cudaMemset(h->d_step, 0, sizeof(int64_t));
   if (e == cudaSuccess) e = cudaMalloc(&h->d_scratch, 64);
+  if (e == cudaSuccess) e = cudaMalloc(&h->d_err, sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMemset(h->d_err, 0, sizeof(int32_t));
   if (e != cudaSuccess) {
     int rc = fzi::set_global_error(FZ_ECUDA, std::string("fz_create: ") + cudaGetErrorString(e));
     fz_destroy(h);
@@ -646,6 +690,7 @@ void fz_destroy(fz_handle* h) {
   free_device(h);
   dfree(h->d_step);
   dfree(h->d_scratch);
+  dfree(h->d_err);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -789,7 +834,15 @@ int fz_sync(fz_handle* h, int64_t timeout_ms) {
   int sleep_us = 20;
   for (;;) {
     cudaError_t e = cudaStreamQuery(h->stream);
-    if (e == cudaSuccess) return FZ_OK;
+    if (e == cudaSuccess) {
+      int32_t kerr = 0;
+      e = cudaMemcpy(&kerr, h->d_err, sizeof(kerr), cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) return cuda_fail(h, e, "error word D2H");
+      if (kerr != 0)
+        return set_error(h, FZ_ETIMEOUT, "a kernel's bounded wait gave up (code " + std::to_string(kerr) +
+                                             "); results of this run are invalid");
+      return FZ_OK;
+    }
     if (e != cudaErrorNotReady) return cuda_fail(h, e, "stream");
     const auto ms =
         std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0).count();

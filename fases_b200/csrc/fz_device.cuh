@@ -1,5 +1,6 @@
 // fz_device.cuh -- device-side types shared by the stepping kernels.
 #pragma once
+#include <cuda.h>  // CUtensorMap (type only; the driver entry point is fetched at run time)
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -20,6 +21,7 @@ constexpr int HY = 3;  // y halo
 constexpr int PW = TX + 2 * HX;  // 40 tile columns
 constexpr int PH = TY + 2 * HY;  // 22 tile rows
 constexpr int NTHREADS = TX * TY;
+constexpr int NBUF = 3;  // plane tiles in flight (TMA ring)
 
 // Cell-class bits (one byte per cell, replaces the reference's 4-byte S read per stage).
 constexpr uint8_t CLS_UPDATE = 1;  // interior cell with S >= h: written by the stage kernels
@@ -94,6 +96,15 @@ struct StageArgs {
   int32_t nn_mul, nn_add;  // nn = nn_mul * n + nn_add
   R half_dt;
   const int64_t* step;  // device step counter n
+  int32_t* err;         // set to a nonzero FZ_KERR_* code when a bounded wait gives up
+};
+
+// Kernel error codes written to the handle's device error word.
+constexpr int32_t KERR_TMA_TIMEOUT = 1;
+
+// TMA descriptors of the stage-input fields p, u, v (boxes of PW x PH x 1 cells).
+struct StageMaps {
+  CUtensorMap p, u, v;
 };
 
 // Immersed band cells (compact list in the reference's build_boundary_map order).

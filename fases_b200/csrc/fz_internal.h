@@ -79,6 +79,11 @@ struct fz_handle {
   double* d_ir = nullptr;
   double* d_vel = nullptr;
 
+  // TMA descriptors of p, u, v of each field set (stage-kernel plane tiles)
+  fz::StageMaps maps[3];
+  // device error word written by kernels whose bounded waits gave up
+  int32_t* d_err = nullptr;
+
   // step counter and bookkeeping
   int64_t* d_step = nullptr;
   double* d_scratch = nullptr;

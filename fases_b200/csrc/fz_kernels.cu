@@ -111,27 +111,111 @@ __device__ __forceinline__ typename Pair<R>::T godunov(typename Pair<R>::T vm, t
 }
 
 // ------------------------------------------------------------------------------------------
+// TMA and mbarrier primitives (PTX). Plain per-CTA tensor loads, never multicast.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred P;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, P;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: gives up after ~2^31 clock cycles (about a second) and reports failure.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (clock64() - t0 > (1ll << 31)) return false;
+  }
+  return true;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y,
+                                            int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
+          "r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Shared-memory layout of the stage kernel.
+template <class R>
+struct StageSmem {
+  typedef typename Pair<R>::T P;
+  // one field of one plane tile, padded to a multiple of 128 bytes (TMA destinations)
+  static constexpr int FIELD = ((PH * PW * (int)sizeof(R) + 127) / 128) * 128;
+  static constexpr int TILES = NBUF * 3 * FIELD;                 // [buf][p,u,v]
+  static constexpr int XC = TY * (TX + 2) * (int)sizeof(P);        // one V array of x-centres
+  static constexpr int YC = (TY + 2) * TX * (int)sizeof(P);        // one V array of y-centres
+  static constexpr int CENTRES = 2 * (2 * XC + 2 * YC);            // double buffered (m, p) x and y
+  static constexpr int BYTES = TILES + CENTRES + 64 + 128;         // + mbarriers + base alignment
+};
+
+// ------------------------------------------------------------------------------------------
 // Fused stage kernel. CTA = 32 x 16 columns marching in z over kz_chunk planes.
-//  - z: a register queue of (p, w) over five planes; the z-centre of plane k+1 is evaluated once
-//    and its two face values are used by the flux above plane k and (next iteration) below k+1.
-//  - x, y: plane k of (p,u) and (p,v) is staged in shared memory with a 3-cell halo; every
-//    x- and y-centre is evaluated once (the reference evaluates every face from both sides) and
-//    exchanged through shared memory.
+//  - x, y: plane k of p, u, v arrives by TMA into a ring of three shared-memory tiles (with a
+//    3-cell halo), issued two planes ahead, so global latency overlaps the arithmetic of the
+//    planes in between. Every x- and y-centre is evaluated once (the reference evaluates every
+//    face from both sides) and exchanged through a double-buffered shared array: one barrier
+//    per plane.
+//  - z: a register queue of (p, w) over five planes, refilled one plane ahead; the z-centre of
+//    plane k+1 is evaluated once and serves the flux above plane k and (next iteration) below
+//    plane k+1.
 // STAGE 0: U1 = U0 + dt L(U0); 1: U2 = 3/4 U0 + 1/4 (U1 + dt L(U1)); 2: U1 = (U0 + 2 (U2 + dt L(U2)))/3
 // (functions3D.cuh:1149-1152, 1230-1233, 1311-1314), cPML with weights 1, 1/4, 2/3 and the psi
 // advance in stage 2 (functions3D.cuh:1157-1162, 1237-1242, 1320-1325), then the point sources of
 // the stage (main3D.cu:1288, 1296, 1304).
 // ------------------------------------------------------------------------------------------
+template <class R>
+__device__ __forceinline__ R source_sum(const StageArgs<R>& A, int64_t g) {
+  const int64_t n = *A.step;
+  const int64_t nn = A.nn_mul * n + A.nn_add;
+  R add = R(0);
+  for (int s = 0; s < A.nsrc; ++s) {
+    if (A.src_cell[s] != g) continue;
+    R amp;
+    if (A.src_opt == 2) {
+      const double ph = 2.0 * 3.14159265358979323846 * (double)A.src_freq[s] * (double)nn * (double)A.half_dt;
+      amp = (R)sin(ph);
+    } else {
+      amp = (nn < A.n_us) ? A.u_s[nn] : R(0);
+    }
+    add += A.src_w * A.src_coef[s] * amp;
+  }
+  return add;
+}
+
 template <class R, int STAGE>
-__global__ void __launch_bounds__(NTHREADS, 1) k_stage(const StageArgs<R> A) {
+__global__ void __launch_bounds__(NTHREADS, 1)
+    k_stage(const StageArgs<R> A, const __grid_constant__ StageMaps M) {
   typedef typename Pair<R>::T P;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  P* TU = reinterpret_cast<P*>(smem_raw);  // [PH][PW] (p, u)
-  P* TV = TU + PH * PW;                    // [PH][PW] (p, v)
-  P* XCm = TV + PH * PW;                   // [TY][TX+2] V- (upper x face) of x-centres i0-1 .. i0+TX
-  P* XCp = XCm + TY * (TX + 2);            // [TY][TX+2] V+ (lower x face)
-  P* YCm = XCp + TY * (TX + 2);            // [TY+2][TX] V- of y-centres j0-1 .. j0+TY
-  P* YCp = YCm + (TY + 2) * TX;            // [TY+2][TX] V+
+  typedef StageSmem<R> L;
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  // TMA destinations must be 128-byte aligned: align the base explicitly
+  unsigned char* smem_raw = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
+  R* tiles = reinterpret_cast<R*>(smem_raw);
+  unsigned char* cbase = smem_raw + L::TILES;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + L::TILES + L::CENTRES);
 
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int lt = ty * TX + tx;
@@ -140,10 +224,32 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_stage(const StageArgs<R> A) {
   const int kb = GHOST + blockIdx.z * A.kz_chunk;
   const int ke = min(kb + A.kz_chunk, A.Nz - GHOST);
   if (kb >= ke) return;
+  const int nplanes = ke - kb;
   const int64_t Sx = A.Sx, plane = A.plane;
   const bool col_ok = (j < A.Ny) && (XOFF + i < Sx);
   const int64_t col = XOFF + i + Sx * (int64_t)j;
   const bool valid = (i < A.Nx - GHOST) && (j < A.Ny - GHOST);
+  const int tma_x = XOFF + i0 - HX, tma_y = j0 - HY;
+  constexpr uint32_t TILE_BYTES = 3u * PH * PW * sizeof(R);
+
+  auto field = [&](int buf, int f) -> R* { return tiles + (buf * 3 + f) * (L::FIELD / (int)sizeof(R)); };
+  auto issue = [&](int it) {
+    const int b = it % NBUF;
+    mbar_expect_tx(&mbar[b], TILE_BYTES);
+    tma_load_3d(field(b, 0), &M.p, &mbar[b], tma_x, tma_y, kb + it);
+    tma_load_3d(field(b, 1), &M.u, &mbar[b], tma_x, tma_y, kb + it);
+    tma_load_3d(field(b, 2), &M.v, &mbar[b], tma_x, tma_y, kb + it);
+  };
+
+  if (lt == 0) {
+    for (int b = 0; b < NBUF; ++b) mbar_init(&mbar[b], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (lt == 0) {
+    issue(0);
+    if (nplanes > 1) issue(1);
+  }
 
   const P kA = pmk(A.frc2, A.firho);
   const P kC = psplat<R>(-A.fc);
@@ -157,47 +263,71 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_stage(const StageArgs<R> A) {
   // z prologue: centres kb-1 and kb give the flux through face kb-1/2 and V-(kb+1/2).
   P z0 = ld_pw(kb - 3), z1 = ld_pw(kb - 2), z2 = ld_pw(kb - 1), z3 = ld_pw(kb), z4 = ld_pw(kb + 1);
   P z5 = ld_pw(kb + 2);
+  P qe_next = ld_pw(kb + 3);
   P zm, zp, vmB, vpB;
   weno_center<R>(z0, z1, z2, z3, z4, zm, zp);
   weno_center<R>(z1, z2, z3, z4, z5, vmB, vpB);
   P Fz_lo = godunov<R>(zm, vpB, kA, kC);
   zm = vmB;
-  // queue: planes k-1, k, k+1, k+2
-  P qa = z2, qb = z3, qc = z4, qd = z5;
+  P qa = z2, qb = z3, qc = z4, qd = z5;  // planes k-1 .. k+2
 
-  for (int k = kb; k < ke; ++k) {
+  // prefetched per-cell loads of the current plane
+  uint8_t cls_n = 0;
+  R bp_n = R(0), bu_n = R(0), bv_n = R(0), bw_n = R(0);
+  if (valid) {
+    const int64_t g = col + plane * kb;
+    cls_n = A.cls[g];
+    if (STAGE > 0 && (cls_n & CLS_UPDATE)) {
+      bp_n = A.pb[g]; bu_n = A.ub[g]; bv_n = A.vb[g]; bw_n = A.wb[g];
+    }
+  }
+
+  for (int it = 0; it < nplanes; ++it) {
+    const int k = kb + it;
+    const int buf = it % NBUF;
+    const uint32_t parity = (uint32_t)((it / NBUF) & 1);
+    P* XCm = reinterpret_cast<P*>(cbase + (it & 1) * (2 * L::XC + 2 * L::YC));
+    P* XCp = XCm + TY * (TX + 2);
+    P* YCm = XCp + TY * (TX + 2);
+    P* YCp = YCm + (TY + 2) * TX;
+
+    // ---- register loads for this plane (prefetched) and the next one
+    const P qe = qe_next;
+    if (it + 1 < nplanes) qe_next = ld_pw(k + 4);
+    const uint8_t cls = cls_n;
+    const R bp = bp_n, bu = bu_n, bv = bv_n, bw = bw_n;
+    if (valid && it + 1 < nplanes) {
+      const int64_t g = col + plane * (k + 1);
+      cls_n = A.cls[g];
+      if (STAGE > 0 && (cls_n & CLS_UPDATE)) {
+        bp_n = A.pb[g]; bu_n = A.ub[g]; bv_n = A.vb[g]; bw_n = A.wb[g];
+      }
+    }
+
     // ---- z: centre k+1 -> flux through face k+1/2
-    const P qe = ld_pw(k + 3);
     P vmC, vpC;
     weno_center<R>(qa, qb, qc, qd, qe, vmC, vpC);
     const P Fz_hi = godunov<R>(zm, vpC, kA, kC);
 
-    // ---- stage plane k of (p,u,v) into shared memory with halo
-    __syncthreads();
-    for (int e = lt; e < PH * PW; e += NTHREADS) {
-      const int r = e / PW, q = e - r * PW;
-      const int gj = j0 - HY + r, gc = XOFF + i0 - HX + q;
-      R p = R(0), u = R(0), v = R(0);
-      if (gj < A.Ny && gc < Sx) {
-        const int64_t g = gc + Sx * (int64_t)gj + plane * k;
-        p = A.pi[g];
-        u = A.ui[g];
-        v = A.vi[g];
-      }
-      TU[e] = pmk(p, u);
-      TV[e] = pmk(p, v);
+    // ---- plane k tile
+    if (!mbar_wait_bounded(&mbar[buf], parity)) {
+      atomicOr(A.err, KERR_TMA_TIMEOUT);
+      return;
     }
-    __syncthreads();
+    const R* Tp = field(buf, 0);
+    const R* Tu = field(buf, 1);
+    const R* Tv = field(buf, 2);
 
     // ---- x and y centres of this thread's cell
     P xm, xp, ym, yp;
     {
-      const P* row = TU + (ty + HY) * PW + (tx + HX);
-      weno_center<R>(row[-2], row[-1], row[0], row[1], row[2], xm, xp);
+      const int c0 = (ty + HY) * PW + (tx + HX);
+      weno_center<R>(pmk(Tp[c0 - 2], Tu[c0 - 2]), pmk(Tp[c0 - 1], Tu[c0 - 1]), pmk(Tp[c0], Tu[c0]),
+                     pmk(Tp[c0 + 1], Tu[c0 + 1]), pmk(Tp[c0 + 2], Tu[c0 + 2]), xm, xp);
       XCm[ty * (TX + 2) + tx + 1] = xm;
       XCp[ty * (TX + 2) + tx + 1] = xp;
-      const P* cl = TV + (ty + HY) * PW + (tx + HX);
-      weno_center<R>(cl[-2 * PW], cl[-PW], cl[0], cl[PW], cl[2 * PW], ym, yp);
+      weno_center<R>(pmk(Tp[c0 - 2 * PW], Tv[c0 - 2 * PW]), pmk(Tp[c0 - PW], Tv[c0 - PW]), pmk(Tp[c0], Tv[c0]),
+                     pmk(Tp[c0 + PW], Tv[c0 + PW]), pmk(Tp[c0 + 2 * PW], Tv[c0 + 2 * PW]), ym, yp);
       YCm[(ty + 1) * TX + tx] = ym;
       YCp[(ty + 1) * TX + tx] = yp;
     }
@@ -205,10 +335,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_stage(const StageArgs<R> A) {
     //      rows (j0-1, j0+TY)
     if (lt < TX) {
       const int r = lt >> 1, side = lt & 1;
-      const int c = side ? (HX + TX) : (HX - 1);
-      const P* row = TU + (r + HY) * PW + c;
+      const int c0 = (r + HY) * PW + (side ? (HX + TX) : (HX - 1));
       P em, ep;
-      weno_center<R>(row[-2], row[-1], row[0], row[1], row[2], em, ep);
+      weno_center<R>(pmk(Tp[c0 - 2], Tu[c0 - 2]), pmk(Tp[c0 - 1], Tu[c0 - 1]), pmk(Tp[c0], Tu[c0]),
+                     pmk(Tp[c0 + 1], Tu[c0 + 1]), pmk(Tp[c0 + 2], Tu[c0 + 2]), em, ep);
       const int slot = r * (TX + 2) + (side ? TX + 1 : 0);
       XCm[slot] = em;
       XCp[slot] = ep;
@@ -216,29 +346,32 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_stage(const StageArgs<R> A) {
       const int e = lt - TX;
       const int r = (e < TX) ? -1 : TY;
       const int c = e & (TX - 1);
-      const P* cl = TV + (r + HY) * PW + (c + HX);
+      const int c0 = (r + HY) * PW + (c + HX);
       P em, ep;
-      weno_center<R>(cl[-2 * PW], cl[-PW], cl[0], cl[PW], cl[2 * PW], em, ep);
+      weno_center<R>(pmk(Tp[c0 - 2 * PW], Tv[c0 - 2 * PW]), pmk(Tp[c0 - PW], Tv[c0 - PW]), pmk(Tp[c0], Tv[c0]),
+                     pmk(Tp[c0 + PW], Tv[c0 + PW]), pmk(Tp[c0 + 2 * PW], Tv[c0 + 2 * PW]), em, ep);
       YCm[(r + 1) * TX + c] = em;
       YCp[(r + 1) * TX + c] = ep;
     }
     __syncthreads();
+    // the tile ring slot of plane it-1 is free now: fetch plane it+2 into it
+    if (lt == 0 && it + 2 < nplanes) {
+      fence_proxy_async();
+      issue(it + 2);
+    }
 
-    // ---- face fluxes of this cell
-    const P Fx_lo = godunov<R>(XCm[ty * (TX + 2) + tx], xp, kA, kC);
-    const P Fx_hi = godunov<R>(xm, XCp[ty * (TX + 2) + tx + 2], kA, kC);
-    const P Fy_lo = godunov<R>(YCm[ty * TX + tx], yp, kA, kC);
-    const P Fy_hi = godunov<R>(ym, YCp[(ty + 2) * TX + tx], kA, kC);
-
-    if (valid) {
+    if (valid && (cls & (CLS_UPDATE | CLS_SOURCE))) {
       const int64_t g = col + plane * k;
-      const uint8_t cls = A.cls[g];
       if (cls & CLS_UPDATE) {
-        // flux differences (times h): .x pressure part, .y velocity part
+        // ---- face fluxes of this cell; flux differences (times h): .x pressure, .y velocity
+        const P Fx_lo = godunov<R>(XCm[ty * (TX + 2) + tx], xp, kA, kC);
+        const P Fx_hi = godunov<R>(xm, XCp[ty * (TX + 2) + tx + 2], kA, kC);
+        const P Fy_lo = godunov<R>(YCm[ty * TX + tx], yp, kA, kC);
+        const P Fy_hi = godunov<R>(ym, YCp[(ty + 2) * TX + tx], kA, kC);
         const P Lx = psub(Fx_lo, Fx_hi), Ly = psub(Fy_lo, Fy_hi), Lz = psub(Fz_lo, Fz_hi);
         const R Lp = Lx.x + Ly.x + Lz.x;
-        const R p_in = qb.x, w_in = qb.y;
-        const R u_in = TU[(ty + HY) * PW + tx + HX].y, v_in = TV[(ty + HY) * PW + tx + HX].y;
+        const int c0 = (ty + HY) * PW + (tx + HX);
+        const R p_in = qb.x, w_in = qb.y, u_in = Tu[c0], v_in = Tv[c0];
         R pn, un, vn, wn;
         if (STAGE == 0) {
           pn = p_in + A.dt_h * Lp;
@@ -246,16 +379,16 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_stage(const StageArgs<R> A) {
           vn = v_in + A.dt_h * Ly.y;
           wn = w_in + A.dt_h * Lz.y;
         } else if (STAGE == 1) {
-          pn = R(0.75) * A.pb[g] + R(0.25) * (p_in + A.dt_h * Lp);
-          un = R(0.75) * A.ub[g] + R(0.25) * (u_in + A.dt_h * Lx.y);
-          vn = R(0.75) * A.vb[g] + R(0.25) * (v_in + A.dt_h * Ly.y);
-          wn = R(0.75) * A.wb[g] + R(0.25) * (w_in + A.dt_h * Lz.y);
+          pn = R(0.75) * bp + R(0.25) * (p_in + A.dt_h * Lp);
+          un = R(0.75) * bu + R(0.25) * (u_in + A.dt_h * Lx.y);
+          vn = R(0.75) * bv + R(0.25) * (v_in + A.dt_h * Ly.y);
+          wn = R(0.75) * bw + R(0.25) * (w_in + A.dt_h * Lz.y);
         } else {
           const R third = R(1.0 / 3.0), two3 = R(2.0 / 3.0);
-          pn = third * A.pb[g] + two3 * (p_in + A.dt_h * Lp);
-          un = third * A.ub[g] + two3 * (u_in + A.dt_h * Lx.y);
-          vn = third * A.vb[g] + two3 * (v_in + A.dt_h * Ly.y);
-          wn = third * A.wb[g] + two3 * (w_in + A.dt_h * Lz.y);
+          pn = third * bp + two3 * (p_in + A.dt_h * Lp);
+          un = third * bu + two3 * (u_in + A.dt_h * Lx.y);
+          vn = third * bv + two3 * (v_in + A.dt_h * Ly.y);
+          wn = third * bw + two3 * (w_in + A.dt_h * Lz.y);
         }
         if (A.pml_on) {
           // cPML (functions3D.cuh:725-755): field += w dt ((1/kappa - 1) D + psi), psi frozen
@@ -287,45 +420,15 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_stage(const StageArgs<R> A) {
             if (STAGE == 2) A.psiz[Z] = pmk(cz.b * ps.x + cz.ca * Dp, cz.b * ps.y + cz.ca * Dw);
           }
         }
-        if (cls & CLS_SOURCE) {
-          const int64_t n = *A.step;
-          const int64_t nn = A.nn_mul * n + A.nn_add;
-          for (int s = 0; s < A.nsrc; ++s) {
-            if (A.src_cell[s] != g) continue;
-            R amp;
-            if (A.src_opt == 2) {
-              const double ph = 2.0 * 3.14159265358979323846 * (double)A.src_freq[s] * (double)nn *
-                                (double)A.half_dt;
-              amp = (R)sin(ph);
-            } else {
-              amp = (nn < A.n_us) ? (R)A.u_s[nn] : R(0);
-            }
-            pn += A.src_w * A.src_coef[s] * amp;
-          }
-        }
+        if (cls & CLS_SOURCE) pn += source_sum(A, g);
         A.po[g] = pn;
         A.uo[g] = un;
         A.vo[g] = vn;
         A.wo[g] = wn;
-      } else if (cls & CLS_SOURCE) {
+      } else {
         // A source in a cell the stage kernels skip still adds to the stale output value, as
         // kernel_inject_src_SSP does (functions3D.cuh:1046).
-        const int64_t n = *A.step;
-        const int64_t nn = A.nn_mul * n + A.nn_add;
-        R pn = A.po[g];
-        for (int s = 0; s < A.nsrc; ++s) {
-          if (A.src_cell[s] != g) continue;
-          R amp;
-          if (A.src_opt == 2) {
-            const double ph = 2.0 * 3.14159265358979323846 * (double)A.src_freq[s] * (double)nn *
-                              (double)A.half_dt;
-            amp = (R)sin(ph);
-          } else {
-            amp = (nn < A.n_us) ? (R)A.u_s[nn] : R(0);
-          }
-          pn += A.src_w * A.src_coef[s] * amp;
-        }
-        A.po[g] = pn;
+        A.po[g] = A.po[g] + source_sum(A, g);
       }
     }
 
@@ -452,8 +555,7 @@ __global__ void k_energy(const R* __restrict__ p, const R* __restrict__ u, const
 // ------------------------------------------------------------------------------------------
 template <class R>
 size_t stage_smem_bytes() {
-  typedef typename Pair<R>::T P;
-  return sizeof(P) * (2 * PH * PW + 2 * TY * (TX + 2) + 2 * (TY + 2) * TX);
+  return (size_t)StageSmem<R>::BYTES;
 }
 
 template <class R>
@@ -474,15 +576,15 @@ cudaError_t stage_occupancy(int* blocks_per_sm) {
 }
 
 template <class R>
-cudaError_t launch_stage(int stage, const StageArgs<R>& a, dim3 grid, cudaStream_t s) {
+cudaError_t launch_stage(int stage, const StageArgs<R>& a, const StageMaps& m, dim3 grid, cudaStream_t s) {
   const dim3 block(TX, TY, 1);
   const size_t smem = stage_smem_bytes<R>();
   if (stage == 0)
-    k_stage<R, 0><<<grid, block, smem, s>>>(a);
+    k_stage<R, 0><<<grid, block, smem, s>>>(a, m);
   else if (stage == 1)
-    k_stage<R, 1><<<grid, block, smem, s>>>(a);
+    k_stage<R, 1><<<grid, block, smem, s>>>(a, m);
   else
-    k_stage<R, 2><<<grid, block, smem, s>>>(a);
+    k_stage<R, 2><<<grid, block, smem, s>>>(a, m);
   return cudaGetLastError();
 }
 
@@ -513,7 +615,7 @@ cudaError_t launch_energy(const R* p, const R* u, const R* v, const R* w, int64_
   template size_t stage_smem_bytes<R>();                                                           \
   template cudaError_t stage_setup<R>();                                                           \
   template cudaError_t stage_occupancy<R>(int*);                                                   \
-  template cudaError_t launch_stage<R>(int, const StageArgs<R>&, dim3, cudaStream_t);              \
+  template cudaError_t launch_stage<R>(int, const StageArgs<R>&, const StageMaps&, dim3, cudaStream_t); \
   template cudaError_t launch_band<R>(const BandArgs<R>&, cudaStream_t);                           \
   template cudaError_t launch_receivers<R>(const R*, const R*, const R*, const R*, const int64_t*, \
                                            int, double*, double*, int64_t, int64_t*,               \
