@@ -22,17 +22,19 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and not _stale():
+def build(force: bool = False, verbose: bool = False, out: str = None, defines=()) -> str:
+    out = out or LIB
+    if not force and out == LIB and not _stale():
         return LIB
     cmd = ["nvcc", "-std=c++17", "-O3", *ARCH, "-lineinfo", "-shared",
            "-Xcompiler", "-fPIC,-ffp-contract=off", "-I", os.path.join(HERE, "..", "include")]
     if verbose:
         cmd += ["-Xptxas", "-v"]
+    cmd += ["-D" + d for d in defines]
     cmd += [os.path.join(CSRC, f) for f in SOURCES]
-    cmd += ["-o", LIB]
+    cmd += ["-o", out]
     subprocess.run(cmd, check=True)
-    return LIB
+    return out
 
 
 if __name__ == "__main__":

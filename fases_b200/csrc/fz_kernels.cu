@@ -205,8 +205,11 @@ __device__ __forceinline__ R source_sum(const StageArgs<R>& A, int64_t g) {
   return add;
 }
 
+#ifndef FZ_STAGE_MINBLOCKS_F32
+#define FZ_STAGE_MINBLOCKS_F32 2  // two 16-warp CTAs per SM in FP32 (64 registers, no spills)
+#endif
 template <class R, int STAGE>
-__global__ void __launch_bounds__(NTHREADS, 1)
+__global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_F32 : 1)
     k_stage(const StageArgs<R> A, const __grid_constant__ StageMaps M) {
   typedef typename Pair<R>::T P;
   typedef StageSmem<R> L;
