@@ -25,7 +25,11 @@ __device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a
 __device__ __forceinline__ float2 pmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 __device__ __forceinline__ float2 psub(float2 a, float2 b) {
-  return __ffma2_rn(b, make_float2(-1.f, -1.f), a);
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;"
+      : "=l"(r)
+      : "l"(*reinterpret_cast<unsigned long long*>(&a)), "l"(*reinterpret_cast<unsigned long long*>(&b)));
+  return *reinterpret_cast<float2*>(&r);
 }
 __device__ __forceinline__ float2 pabs(float2 a) { return make_float2(fabsf(a.x), fabsf(a.y)); }
 __device__ __forceinline__ float frcp(float x) {
@@ -64,16 +68,14 @@ __device__ __forceinline__ typename Pair<R>::T psplat(R x) {
 // (the 12/13 scaling is absorbed into eps).
 // ------------------------------------------------------------------------------------------
 template <class R>
-__device__ __forceinline__ void weno_center(typename Pair<R>::T qm2, typename Pair<R>::T qm1,
-                                            typename Pair<R>::T q0, typename Pair<R>::T qp1,
-                                            typename Pair<R>::T qp2, typename Pair<R>::T& vm,
-                                            typename Pair<R>::T& vp) {
+__device__ __forceinline__ void weno_core(typename Pair<R>::T a, typename Pair<R>::T b, typename Pair<R>::T c,
+                                          typename Pair<R>::T d, typename Pair<R>::T D2, typename Pair<R>::T D1,
+                                          typename Pair<R>::T D0, typename Pair<R>::T q0, typename Pair<R>::T& vm,
+                                          typename Pair<R>::T& vp) {
   typedef typename Pair<R>::T P;
-  const P a = psub(qm1, qm2), b = psub(q0, qm1), c = psub(qp1, q0), d = psub(qp2, qp1);
-  const P D2 = psub(b, a), D1 = psub(c, b), D0 = psub(d, c);  // second differences
-  const P E2 = pfma(b, psplat<R>(R(2)), D2);                  // u_{i-2} - 4u_{i-1} + 3u_i
-  const P E1 = padd(b, c);                                    // -(u_{i-1} - u_{i+1})
-  const P E0 = pfma(c, psplat<R>(R(-2)), D0);                 // 3u_i - 4u_{i+1} + u_{i+2} (sign)
+  const P E2 = pfma(b, psplat<R>(R(2)), D2);   // u_{i-2} - 4u_{i-1} + 3u_i
+  const P E1 = padd(b, c);                     // -(u_{i-1} - u_{i+1})
+  const P E0 = pfma(c, psplat<R>(R(-2)), D0);  // 3u_i - 4u_{i+1} + u_{i+2} (sign)
   const P k313 = psplat<R>(R(3.0 / 13.0));
   const P B0 = pfma(D0, D0, pmul(pmul(E0, k313), E0));
   const P B1 = pfma(D1, D1, pmul(pmul(E1, k313), E1));
@@ -98,6 +100,16 @@ __device__ __forceinline__ void weno_center(typename Pair<R>::T qm2, typename Pa
   const P Np = pfma(q2w, ep2, pfma(q1w, ep1, pmul(q0w, ep0)));
   vm = pfma(Nm, prcp(Sm), q0);
   vp = pfma(Np, prcp(Sp), q0);
+}
+
+template <class R>
+__device__ __forceinline__ void weno_center(typename Pair<R>::T qm2, typename Pair<R>::T qm1,
+                                            typename Pair<R>::T q0, typename Pair<R>::T qp1,
+                                            typename Pair<R>::T qp2, typename Pair<R>::T& vm,
+                                            typename Pair<R>::T& vp) {
+  typedef typename Pair<R>::T P;
+  const P a = psub(qm1, qm2), b = psub(q0, qm1), c = psub(qp1, q0), d = psub(qp2, qp1);
+  weno_core<R>(a, b, c, d, psub(b, a), psub(c, b), psub(d, c), q0, vm, vp);
 }
 
 // Godunov (exact Riemann) flux of linear acoustics for a (pressure, normal velocity) pair
@@ -272,7 +284,8 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
   weno_center<R>(z1, z2, z3, z4, z5, vmB, vpB);
   P Fz_lo = godunov<R>(zm, vpB, kA, kC);
   zm = vmB;
-  P qa = z2, qb = z3, qc = z4, qd = z5;  // planes k-1 .. k+2
+  // queue of plane values k-1 .. k+2 for the centre of plane k+1
+  P qa = z2, qb = z3, qc = z4, qd = z5;
 
   // prefetched per-cell loads of the current plane
   uint8_t cls_n = 0;
