@@ -1,0 +1,150 @@
+"""Reads a golden reference project (written by make_golden.py, run through the reference solver)
+into the inputs of the CPU oracle, with the reference's float32 conventions (main3D.cu:115-160,
+454-456, 729-752, 861-959, 963-1124; common/filterABC.h:31-90). Test infrastructure only; it is
+independent of the product's C++ project parser, which the GPU tests exercise on the same files.
+"""
+import os
+import re
+
+import numpy as np
+
+f32 = np.float32
+
+
+def read_config(path):
+    vals = []
+    for line in open(path):
+        line = line.split("#", 1)[0]
+        m = re.match(r"\s*([-+0-9.eE]+)", line)
+        if m:
+            try:
+                vals.append(f32(float(m.group(1))))
+            except ValueError:
+                pass
+    return vals
+
+
+def read_fit(path):
+    toks = []
+    for line in open(path):
+        s = line.strip()
+        if not s or s.startswith("#"):
+            continue
+        toks += s.split()
+    Rinf = f32(toks[0])
+    K, L = int(toks[1]), int(toks[2])
+    pos = 3
+    A, zeta = [], []
+    for _ in range(K):
+        A.append(f32(toks[pos])); zeta.append(f32(toks[pos + 1])); pos += 2
+    B, C, al, be = [], [], [], []
+    for _ in range(L):
+        B.append(f32(toks[pos])); C.append(f32(toks[pos + 1])); al.append(f32(toks[pos + 2])); be.append(f32(toks[pos + 3]))
+        pos += 4
+    return Rinf, A, zeta, B, C, al, be
+
+
+def obj_layers(path):
+    names, seen, cur, have, pending = [], set(), "unnamed", False, True
+    for raw in open(path):
+        line = raw.strip()
+        if not line or line.startswith("#"):
+            continue
+        if line.startswith("o ") or line.startswith("g "):
+            parts = line.split()[1:]
+            nm = parts[1] if len(parts) >= 2 else (parts[0] if parts else "unnamed")
+            if not have or nm != cur:
+                cur, have, pending = nm, True, True
+        elif line.startswith("f ") and len(line.split()) >= 4 and pending:
+            nm = cur if have else "unnamed"
+            if nm not in seen:
+                seen.add(nm)
+                names.append(nm)
+            pending = False
+    return names
+
+
+def load(case_dir):
+    """Returns a dict with the oracle inputs plus the reference's IR/VEL traces."""
+    cfg = read_config(os.path.join(case_dir, "config", "config.txt"))
+    h = cfg[0]
+    t_max = cfg[1]
+    f_in = cfg[2]
+    f_x = f_in
+    for oc in (63.0, 125.0, 250.0, 500.0, 1000.0, 2000.0, 4000.0, 8000.0):
+        hi = f32(oc) * f32(1.41421356)
+        if f_in <= hi:
+            f_x = hi
+            break
+    f_cutoff = f32(2.0) * f_x
+    rho = f32(1.225)
+    Temp = cfg[3] + f32(273.15)
+    c = np.sqrt(f32(1.4) * f32(287.05) * Temp, dtype=f32)
+    dt = f32(cfg[4] * h / c)
+    Nt = int(t_max / dt) + 1
+    pml = tuple(int(cfg[6 + i] != 0) for i in range(6))
+    src_opt = int(cfg[15]) if len(cfg) > 15 else 0
+    glob_f = cfg[16] if len(cfg) > 16 else (f32(25.0) if src_opt == 0 else f32(0.5) * f_cutoff)
+    lines = open(os.path.join(case_dir, "output", "scene_cache.txt")).read().split("\n")
+    Nx, Ny, Nz = [int(x) for x in lines[1].split()[:3]]
+    N = Nx * Ny * Nz
+    S = np.fromfile(os.path.join(case_dir, "output", "S.bin"), np.float32, N).reshape(Nz, Ny, Nx)
+    oid = np.fromfile(os.path.join(case_dir, "output", "oid.bin"), np.uint8, N).reshape(Nz, Ny, Nx)
+    Km, Lm = [int(x) for x in open(os.path.join(case_dir, "config", "poles.txt")).read().split()[:2]]
+    Km, Lm = max(1, Km), max(1, Lm)
+    layers = obj_layers(os.path.join(case_dir, "scene.obj"))
+    nm = len(layers)
+    mat = {"Rinf": np.zeros(nm), "A": np.zeros((nm, Km)), "zeta": np.zeros((nm, Km)), "B": np.zeros((nm, Lm)),
+           "Cc": np.zeros((nm, Lm)), "alpha": np.zeros((nm, Lm)), "beta": np.zeros((nm, Lm))}
+    for m, name in enumerate(layers):
+        if "ounding" in name or "oundary" in name:
+            continue
+        Rinf, A, zeta, B, C_, al, be = read_fit(os.path.join(case_dir, "input", "fit", name + ".fit"))
+        mat["Rinf"][m] = Rinf
+        mat["A"][m, :len(A)] = A
+        mat["zeta"][m, :len(zeta)] = zeta
+        mat["B"][m, :len(B)] = B
+        mat["Cc"][m, :len(C_)] = C_
+        mat["alpha"][m, :len(al)] = al
+        mat["beta"][m, :len(be)] = be
+    src, spress, sfreq = [], [], []
+    for line in open(os.path.join(case_dir, "src.txt")):
+        if not line.strip() or line.startswith("#"):
+            continue
+        v = [f32(x) for x in line.split()]
+        if len(v) < 4:
+            continue
+        ijk = [int(v[a] / h) + 3 for a in range(3)]
+        if all(0 <= ijk[a] < n for a, n in enumerate((Nx, Ny, Nz))):
+            src.append(ijk)
+            spress.append(f32(2e-5 * float(np.power(f32(10.0), f32(v[3] / 20.0), dtype=f32))))
+            sfreq.append(v[4] if len(v) > 4 else f32(0.5) * f_cutoff)
+    rec = []
+    for line in open(os.path.join(case_dir, "rec.txt")):
+        if not line.strip() or line.startswith("#"):
+            continue
+        v = [f32(x) for x in line.split()]
+        rec.append([int(v[a] / h) + 3 for a in range(3)])
+    from oracle.oracle import waveform
+    us, pref, pk = waveform(src_opt, float(glob_f), float(f_cutoff), float(dt), Nt, float(h), float(rho))
+    sval = np.array([f32(s / f32(pk)) for s in spress], np.float64)
+    us32 = us.astype(np.float32).astype(np.float64)
+    nrec = len(rec)
+    ir = np.stack([np.fromfile(os.path.join(case_dir, "output", f"IR{r}_0.bin"), np.float32) for r in range(nrec)])
+    vel = np.stack([np.fromfile(os.path.join(case_dir, "output", f"VEL{r}_0.bin"), np.float32).reshape(-1, 3)
+                    for r in range(nrec)])
+    return {"S": S, "oid": oid, "h": float(h), "c": float(c), "rho": float(rho), "dt": float(dt), "Nt": Nt,
+            "pml": pml, "materials": mat, "src": np.array(src, np.int32), "sval": sval, "src_opt": src_opt,
+            "src_freq": np.array(sfreq, np.float64), "u_s": us32, "rec": np.array(rec, np.int32), "ir": ir,
+            "vel": vel, "p_ref_scaled": pref * float(f32(spress[0] / f32(pk))) if spress else None,
+            "case_dir": case_dir}
+
+
+def run_oracle(fx, steps=None):
+    from oracle.oracle import Oracle
+    steps = fx["Nt"] if steps is None else steps
+    o = Oracle(fx["S"], fx["oid"], fx["h"], fx["c"], fx["rho"], fx["dt"], pml=fx["pml"], materials=fx["materials"],
+               src_cells=fx["src"], sval=fx["sval"], src_opt=fx["src_opt"], src_freq=fx["src_freq"], u_s=fx["u_s"],
+               rec_cells=fx["rec"], max_steps=steps)
+    o.run(steps)
+    return o

@@ -1,0 +1,114 @@
+"""Pins against the reference solver itself: the golden fixtures under tests/golden/ hold small
+reference projects and the outputs of the reference `fases3D` built from its own sources and run
+on a B200 (tests/golden/make_golden.py).
+
+CPU: the FP64 oracle reproduces the reference's receiver traces.
+GPU: the product, driven through the project loader of the C ABI (fz_load_project) on the same
+project files, reproduces the reference's traces and output files."""
+import os
+import shutil
+
+import numpy as np
+import pytest
+
+from tests.golden import fixture
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CASES = ["box_pcs", "box_ricker"]
+# FP64 oracle vs the reference's FP32 solver: per-receiver relative L2
+TOL_ORACLE = 5e-6
+# FP32 CUDA stepper vs the reference's FP32 solver
+TOL_GPU = 2e-5
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_oracle_matches_reference_solver(case):
+    fx = fixture.load(os.path.join(HERE, "golden", case))
+    o = fixture.run_oracle(fx)
+    ir, vel = o.ir()
+    assert ir.shape == fx["ir"].shape
+    for r in range(ir.shape[0]):
+        assert _rel(ir[r], fx["ir"][r]) < TOL_ORACLE, (case, r)
+        assert _rel(vel[r], fx["vel"][r]) < 10 * TOL_ORACLE, (case, r)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_fixture_geometry_is_consistent(case):
+    """The reference's band: oid set exactly where 0 <= S <= 3h (plus the builder's gradient
+    rule), never in the outermost cells."""
+    fx = fixture.load(os.path.join(HERE, "golden", case))
+    S, oid, h = fx["S"], fx["oid"], fx["h"]
+    band = oid != 0xFF
+    assert band.any()
+    assert np.all(S[band] >= 0) and np.all(S[band] <= 3 * h * (1 + 1e-6))
+    assert not band[0].any() and not band[-1].any()
+
+
+def _copy_project(case, tmp_path):
+    dst = tmp_path / case
+    shutil.copytree(os.path.join(HERE, "golden", case), dst)
+    return str(dst)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", CASES)
+def test_project_loader_and_stepper_match_reference(case, tmp_path):
+    from fases_b200 import Solver
+    proj = _copy_project(case, tmp_path)
+    ref_ir = fixture.load(proj)["ir"]
+    s, nt = Solver.from_project(os.path.join(proj, "scene.obj"), os.path.join(proj, "config", "config.txt"),
+                                os.path.join(proj, "src.txt"), os.path.join(proj, "rec.txt"))
+    assert nt == ref_ir.shape[1]
+    s.run(nt)
+    ir = s.ir()
+    for r in range(ir.shape[0]):
+        assert _rel(ir[r], ref_ir[r]) < TOL_GPU, (case, r, _rel(ir[r], ref_ir[r]))
+    # output files in the reference's formats
+    out = os.path.join(proj, "fz_out")
+    s.write_outputs(out, 0, os.path.join(proj, "scene.obj"))
+    for r in range(ir.shape[0]):
+        a = np.fromfile(os.path.join(out, f"IR{r}_0.bin"), np.float32)
+        b = np.fromfile(os.path.join(proj, "output", f"IR{r}_0.bin"), np.float32)
+        assert a.shape == b.shape and _rel(a, b) < TOL_GPU
+        va = np.fromfile(os.path.join(out, f"VEL{r}_0.bin"), np.float32)
+        vb = np.fromfile(os.path.join(proj, "output", f"VEL{r}_0.bin"), np.float32)
+        assert va.shape == vb.shape
+    hdr = open(os.path.join(out, "header.txt")).read().split()
+    ref_hdr = open(os.path.join(proj, "output", "header.txt")).read().split()
+    assert len(hdr) == len(ref_hdr) == 13
+    assert hdr[:4] == ref_hdr[:4]          # Nx Ny Nz Nt
+    assert hdr[9] == ref_hdr[9]            # dt, the value common/allIRs.py reads
+    assert hdr[11:] == ref_hdr[11:]        # h, tol/h
+    # p_ref.bin written by the loader (main3D.cu:1096-1108) is the reference's, bit for bit
+    pr = np.fromfile(os.path.join(proj, "config", "p_ref.bin"), np.float64)
+    pr_ref = np.fromfile(os.path.join(HERE, "golden", case, "config", "p_ref.bin"), np.float64)
+    assert pr.shape == pr_ref.shape
+    assert np.max(np.abs(pr - pr_ref)) <= 1e-12 * np.max(np.abs(pr_ref))
+    s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", CASES)
+def test_fp64_stepper_matches_oracle_on_reference_geometry(case):
+    """The FP64 CUDA path equals the FP64 oracle on the reference's own S.bin/oid.bin."""
+    from fases_b200 import Solver, params
+    fx = fixture.load(os.path.join(HERE, "golden", case))
+    steps = 60
+    prm = params(h=fx["h"], c=fx["c"], rho=fx["rho"], dt=fx["dt"], pml=fx["pml"], precision="fp64")
+    s = Solver(prm)
+    s.load_geometry(fx["S"], fx["oid"])
+    m = fx["materials"]
+    s.set_materials(m["Rinf"], m["A"], m["zeta"], m["B"], m["Cc"], m["alpha"], m["beta"])
+    s.set_sources(fx["src"], fx["sval"], fx["src_opt"], u_s=fx["u_s"], freq=fx["src_freq"])
+    s.set_receivers(fx["rec"], steps)
+    s.run(steps)
+    o = fixture.run_oracle(fx, steps)
+    ir_o, _ = o.ir()
+    assert _rel(s.ir(), ir_o) < 1e-10
+    for a, b in zip(s.fields(), o.fields()):
+        assert _rel(a, b) < 1e-10
+    s.close()
