@@ -112,20 +112,35 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
-// 3-D map over one device field (Sx x Ny x Nz elements) with PW x PH x 1 boxes; reads outside
-// the allocation fill with zeros.
-int make_field_map(fz_handle* h, CUtensorMap* map, void* base) {
+// 3-D map over one device array (Sx x Ny x Nz elements of esz bytes) with bx x by x 1 boxes;
+// reads outside the allocation fill with zeros.
+int make_map(fz_handle* h, CUtensorMap* map, void* base, size_t esz, CUtensorMapDataType type, int bx, int by) {
   EncodeTiledFn enc = encode_fn();
   if (!enc) return set_error(h, FZ_ECUDA, "cuTensorMapEncodeTiled not available from the driver");
   const cuuint64_t dims[3] = {(cuuint64_t)h->Sx, (cuuint64_t)h->Ny, (cuuint64_t)h->Nz};
-  const cuuint64_t strides[2] = {(cuuint64_t)h->Sx * h->rsize, (cuuint64_t)h->plane * h->rsize};
-  const cuuint32_t box[3] = {(cuuint32_t)fz::PW, (cuuint32_t)fz::PH, 1};
+  const cuuint64_t strides[2] = {(cuuint64_t)h->Sx * esz, (cuuint64_t)h->plane * esz};
+  const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
   const cuuint32_t estr[3] = {1, 1, 1};
-  const CUresult r = enc(map, h->fp64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base,
-                         dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  const CUresult r = enc(map, type, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return set_error(h, FZ_ECUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
   return FZ_OK;
+}
+
+int make_field_maps(fz_handle* h) {
+  const CUtensorMapDataType t = h->fp64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  for (int s = 0; s < 3; s++) {
+    for (int f = 0; f < 3; f++) {
+      int rc = make_map(h, &h->halo_map[s][f], h->U[s][f], h->rsize, t, fz::PW, fz::PH);
+      if (rc != FZ_OK) return rc;
+    }
+    for (int f = 0; f < 4; f++) {
+      int rc = make_map(h, &h->own_map[s][f], h->U[s][f], h->rsize, t, fz::TX, fz::TY);
+      if (rc != FZ_OK) return rc;
+    }
+  }
+  return make_map(h, &h->cls_map, h->d_cls, 1, CU_TENSOR_MAP_DATA_TYPE_UINT8, fz::TX, fz::TY);
 }
 
 // Per-axis cPML coefficient table, restated from functions3D.cuh:689-723 (evaluated once here in
@@ -336,10 +351,23 @@ int finalize(fz_handle* h) {
   const int nty = (h->Ny - 2 * GHOST + fz::TY - 1) / fz::TY;
   const int nzi = h->Nz - 2 * GHOST;
   const int64_t slots = (int64_t)h->nsm * occ;
-  int nkz = (int)std::max<int64_t>(1, (4 * slots + (int64_t)ntx * nty - 1) / ((int64_t)ntx * nty));
-  nkz = std::min(nkz, std::max(1, nzi / 8));
-  h->kz_chunk = (nzi + nkz - 1) / nkz;
-  nkz = (nzi + h->kz_chunk - 1) / h->kz_chunk;
+  // Pick the z-chunk count that best fills whole waves of CTA slots, charging each chunk about
+  // 1.5 planes of start-up work (two extra z centres and the TMA ring fill).
+  int best = 1;
+  double best_eff = -1.0;
+  for (int nk = 1; nk <= std::max(1, nzi / 8); nk++) {
+    const int chunk = (nzi + nk - 1) / nk;
+    const int nk_eff = (nzi + chunk - 1) / chunk;
+    const int64_t items = (int64_t)ntx * nty * nk_eff;
+    const int64_t waves = (items + slots - 1) / slots;
+    const double eff = ((double)items / (double)(waves * slots)) * ((double)chunk / (chunk + 1.5));
+    if (eff > best_eff + 1e-9) {
+      best_eff = eff;
+      best = nk;
+    }
+  }
+  h->kz_chunk = (nzi + best - 1) / best;
+  int nkz = (nzi + h->kz_chunk - 1) / h->kz_chunk;
   h->stage_grid = dim3((unsigned)ntx, (unsigned)nty, (unsigned)nkz);
   h->finalized = true;
   return FZ_OK;
@@ -459,7 +487,16 @@ cudaError_t enqueue_step(fz_handle* h) {
     {
       Timer t(h, st);
       const int in_set = (st == 0) ? h->i0 : (st == 1) ? h->i1 : h->i2;
-      e = fz::launch_stage<R>(st, stage_args<R>(h, st), h->maps[in_set], h->stage_grid, h->stream);
+      fz::StageMaps m;
+      m.p = h->halo_map[in_set][0];
+      m.u = h->halo_map[in_set][1];
+      m.v = h->halo_map[in_set][2];
+      m.bp = h->own_map[h->i0][0];
+      m.bu = h->own_map[h->i0][1];
+      m.bv = h->own_map[h->i0][2];
+      m.bw = h->own_map[h->i0][3];
+      m.cls = h->cls_map;
+      e = fz::launch_stage<R>(st, stage_args<R>(h, st), m, h->stage_grid, h->stream);
       if (e != cudaSuccess) return e;
     }
     if (h->nB > 0) {
@@ -534,12 +571,6 @@ int load_geometry(fz_handle* h, const float* S, const uint8_t* oid, int Nx, int 
       FZ_CUDA(h, cudaMemset(h->U[s][f], 0, bytes), "cudaMemset(fields)");
     }
   // cell classes: update where the stage kernels would not return early (functions3D.cuh:1091-1097)
-  for (int s = 0; s < 3; s++) {
-    int rc = make_field_map(h, &h->maps[s].p, h->U[s][0]);
-    if (rc == FZ_OK) rc = make_field_map(h, &h->maps[s].u, h->U[s][1]);
-    if (rc == FZ_OK) rc = make_field_map(h, &h->maps[s].v, h->U[s][2]);
-    if (rc != FZ_OK) return rc;
-  }
   h->cls_host.assign((size_t)h->ncell_dev, 0);
   int64_t nup = 0;
   const float hf = (float)h->prm.h;
@@ -553,6 +584,10 @@ int load_geometry(fz_handle* h, const float* S, const uint8_t* oid, int Nx, int 
   h->n_update = nup;
   FZ_CUDA(h, cudaMalloc(&h->d_cls, h->cls_host.size()), "cudaMalloc(cls)");
   FZ_CUDA(h, cudaMemcpy(h->d_cls, h->cls_host.data(), h->cls_host.size(), cudaMemcpyHostToDevice), "cls H2D");
+  {
+    int rc = make_field_maps(h);
+    if (rc != FZ_OK) return rc;
+  }
   h->pml_on = false;
   for (int f = 0; f < 6; f++) h->pml_on = h->pml_on || (h->prm.pml[f] != 0);
   int rc = upload_pml<R>(h);

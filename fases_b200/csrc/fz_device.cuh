@@ -102,9 +102,13 @@ struct StageArgs {
 // Kernel error codes written to the handle's device error word.
 constexpr int32_t KERR_TMA_TIMEOUT = 1;
 
-// TMA descriptors of the stage-input fields p, u, v (boxes of PW x PH x 1 cells).
+// TMA descriptors of one stage launch: the stage-input fields p, u, v as halo tiles
+// (PW x PH x 1), the base state U0 as own tiles (TX x TY x 1; stages 1 and 2) and the class bytes
+// as an own tile.
 struct StageMaps {
   CUtensorMap p, u, v;
+  CUtensorMap bp, bu, bv, bw;
+  CUtensorMap cls;
 };
 
 // Immersed band cells (compact list in the reference's build_boundary_map order).

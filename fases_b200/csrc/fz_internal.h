@@ -79,8 +79,11 @@ struct fz_handle {
   double* d_ir = nullptr;
   double* d_vel = nullptr;
 
-  // TMA descriptors of p, u, v of each field set (stage-kernel plane tiles)
-  fz::StageMaps maps[3];
+  // TMA descriptors: halo tiles of p, u, v and own tiles of p, u, v, w of each field set, and
+  // the class bytes
+  CUtensorMap halo_map[3][3];
+  CUtensorMap own_map[3][4];
+  CUtensorMap cls_map;
   // device error word written by kernels whose bounded waits gave up
   int32_t* d_err = nullptr;
 

@@ -175,8 +175,11 @@ template <class R>
 struct StageSmem {
   typedef typename Pair<R>::T P;
   // one field of one plane tile, padded to a multiple of 128 bytes (TMA destinations)
-  static constexpr int FIELD = ((PH * PW * (int)sizeof(R) + 127) / 128) * 128;
-  static constexpr int TILES = NBUF * 3 * FIELD;                 // [buf][p,u,v]
+  static constexpr int FIELD = ((PH * PW * (int)sizeof(R) + 127) / 128) * 128;  // halo tile
+  static constexpr int OWN = ((TX * TY * (int)sizeof(R) + 127) / 128) * 128;     // own tile
+  static constexpr int CLSB = ((TX * TY + 127) / 128) * 128;                     // class bytes
+  static constexpr int BUF = 3 * FIELD + 4 * OWN + CLSB;         // p,u,v halo | U0 own | cls
+  static constexpr int TILES = NBUF * BUF;
   static constexpr int XC = TY * (TX + 2) * (int)sizeof(P);        // one V array of x-centres
   static constexpr int YC = (TY + 2) * TX * (int)sizeof(P);        // one V array of y-centres
   static constexpr int CENTRES = 2 * (2 * XC + 2 * YC);            // double buffered (m, p) x and y
@@ -245,15 +248,29 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
   const int64_t col = XOFF + i + Sx * (int64_t)j;
   const bool valid = (i < A.Nx - GHOST) && (j < A.Ny - GHOST);
   const int tma_x = XOFF + i0 - HX, tma_y = j0 - HY;
-  constexpr uint32_t TILE_BYTES = 3u * PH * PW * sizeof(R);
+  constexpr uint32_t TILE_BYTES = 3u * PH * PW * sizeof(R) + (STAGE > 0 ? 4u * TX * TY * sizeof(R) : 0u) +
+                                  (uint32_t)(TX * TY);
 
-  auto field = [&](int buf, int f) -> R* { return tiles + (buf * 3 + f) * (L::FIELD / (int)sizeof(R)); };
+  unsigned char* const ring = reinterpret_cast<unsigned char*>(tiles);
+  auto field = [&](int buf, int f) -> R* { return reinterpret_cast<R*>(ring + buf * L::BUF + f * L::FIELD); };
+  auto own = [&](int buf, int f) -> R* {
+    return reinterpret_cast<R*>(ring + buf * L::BUF + 3 * L::FIELD + f * L::OWN);
+  };
+  auto clsb = [&](int buf) -> uint8_t* { return ring + buf * L::BUF + 3 * L::FIELD + 4 * L::OWN; };
   auto issue = [&](int it) {
     const int b = it % NBUF;
+    const int z = kb + it;
     mbar_expect_tx(&mbar[b], TILE_BYTES);
-    tma_load_3d(field(b, 0), &M.p, &mbar[b], tma_x, tma_y, kb + it);
-    tma_load_3d(field(b, 1), &M.u, &mbar[b], tma_x, tma_y, kb + it);
-    tma_load_3d(field(b, 2), &M.v, &mbar[b], tma_x, tma_y, kb + it);
+    tma_load_3d(field(b, 0), &M.p, &mbar[b], tma_x, tma_y, z);
+    tma_load_3d(field(b, 1), &M.u, &mbar[b], tma_x, tma_y, z);
+    tma_load_3d(field(b, 2), &M.v, &mbar[b], tma_x, tma_y, z);
+    if (STAGE > 0) {
+      tma_load_3d(own(b, 0), &M.bp, &mbar[b], tma_x + HX, j0, z);
+      tma_load_3d(own(b, 1), &M.bu, &mbar[b], tma_x + HX, j0, z);
+      tma_load_3d(own(b, 2), &M.bv, &mbar[b], tma_x + HX, j0, z);
+      tma_load_3d(own(b, 3), &M.bw, &mbar[b], tma_x + HX, j0, z);
+    }
+    tma_load_3d(clsb(b), &M.cls, &mbar[b], tma_x + HX, j0, z);
   };
 
   if (lt == 0) {
@@ -287,21 +304,14 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
   // queue of plane values k-1 .. k+2 for the centre of plane k+1
   P qa = z2, qb = z3, qc = z4, qd = z5;
 
-  // prefetched per-cell loads of the current plane
-  uint8_t cls_n = 0;
-  R bp_n = R(0), bu_n = R(0), bv_n = R(0), bw_n = R(0);
-  if (valid) {
-    const int64_t g = col + plane * kb;
-    cls_n = A.cls[g];
-    if (STAGE > 0 && (cls_n & CLS_UPDATE)) {
-      bp_n = A.pb[g]; bu_n = A.ub[g]; bv_n = A.vb[g]; bw_n = A.wb[g];
-    }
-  }
 
-  for (int it = 0; it < nplanes; ++it) {
+  // cPML membership of this column along x and y (fixed during the march)
+  const bool pml_xy = A.pml_on && valid && (A.pcx[i].tile >= 0 || A.pcy[j].tile >= 0);
+  int buf = 0;
+  uint32_t parity = 0;
+  int64_t gk = col + plane * kb;  // offset of (i, j, k)
+  for (int it = 0; it < nplanes; ++it, gk += plane) {
     const int k = kb + it;
-    const int buf = it % NBUF;
-    const uint32_t parity = (uint32_t)((it / NBUF) & 1);
     P* XCm = reinterpret_cast<P*>(cbase + (it & 1) * (2 * L::XC + 2 * L::YC));
     P* XCp = XCm + TY * (TX + 2);
     P* YCm = XCp + TY * (TX + 2);
@@ -310,15 +320,6 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
     // ---- register loads for this plane (prefetched) and the next one
     const P qe = qe_next;
     if (it + 1 < nplanes) qe_next = ld_pw(k + 4);
-    const uint8_t cls = cls_n;
-    const R bp = bp_n, bu = bu_n, bv = bv_n, bw = bw_n;
-    if (valid && it + 1 < nplanes) {
-      const int64_t g = col + plane * (k + 1);
-      cls_n = A.cls[g];
-      if (STAGE > 0 && (cls_n & CLS_UPDATE)) {
-        bp_n = A.pb[g]; bu_n = A.ub[g]; bv_n = A.vb[g]; bw_n = A.wb[g];
-      }
-    }
 
     // ---- z: centre k+1 -> flux through face k+1/2
     P vmC, vpC;
@@ -333,6 +334,7 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
     const R* Tp = field(buf, 0);
     const R* Tu = field(buf, 1);
     const R* Tv = field(buf, 2);
+    const uint8_t cls = clsb(buf)[lt];
 
     // ---- x and y centres of this thread's cell
     P xm, xp, ym, yp;
@@ -377,7 +379,7 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
     }
 
     if (valid && (cls & (CLS_UPDATE | CLS_SOURCE))) {
-      const int64_t g = col + plane * k;
+      const int64_t g = gk;
       if (cls & CLS_UPDATE) {
         // ---- face fluxes of this cell; flux differences (times h): .x pressure, .y velocity
         const P Fx_lo = godunov<R>(XCm[ty * (TX + 2) + tx], xp, kA, kC);
@@ -389,6 +391,13 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
         const int c0 = (ty + HY) * PW + (tx + HX);
         const R p_in = qb.x, w_in = qb.y, u_in = Tu[c0], v_in = Tv[c0];
         R pn, un, vn, wn;
+        R bp = R(0), bu = R(0), bv = R(0), bw = R(0);
+        if (STAGE > 0) {
+          bp = own(buf, 0)[lt];
+          bu = own(buf, 1)[lt];
+          bv = own(buf, 2)[lt];
+          bw = own(buf, 3)[lt];
+        }
         if (STAGE == 0) {
           pn = p_in + A.dt_h * Lp;
           un = u_in + A.dt_h * Lx.y;
@@ -406,7 +415,7 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
           vn = third * bv + two3 * (v_in + A.dt_h * Ly.y);
           wn = third * bw + two3 * (w_in + A.dt_h * Lz.y);
         }
-        if (A.pml_on) {
+        if (pml_xy || (A.pml_on && A.pcz[k].tile >= 0)) {
           // cPML (functions3D.cuh:725-755): field += w dt ((1/kappa - 1) D + psi), psi frozen
           // within the step and advanced once, in stage 2, by recursive convolution.
           const PmlCoef<R> cx = A.pcx[i], cy = A.pcy[j], cz = A.pcz[k];
@@ -448,6 +457,10 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
       }
     }
 
+    if (++buf == NBUF) {
+      buf = 0;
+      parity ^= 1u;
+    }
     Fz_lo = Fz_hi;
     zm = vmC;
     qa = qb;
