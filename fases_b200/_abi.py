@@ -25,6 +25,8 @@ FZ_FP64 = 1
 FZ_SRC_PCS = 0
 FZ_SRC_RICKER = 1
 FZ_SRC_SINE = 2
+FZ_NOALLOC_MAX_BLOCKS = 4096
+FZ_NOALLOC_MAX_CELLS = 4096 * 16384
 
 ERROR_NAMES = {
     FZ_EINVAL: "FZ_EINVAL", FZ_ENOMEM: "FZ_ENOMEM", FZ_ECUDA: "FZ_ECUDA", FZ_EIO: "FZ_EIO",
@@ -90,6 +92,7 @@ SIGNATURES = {
                                   C.POINTER(_P), _i64p]),
     "fz_source_waveform": (C.c_int, [_i32, C.c_double, C.c_double, C.c_double, _i64, C.c_double,
                                      C.c_double, _dp, _dp, _dp]),
+    "fz_energy_noalloc": (C.c_int, [_P, _P, _P, _P, _i64, C.c_double, C.c_double, _P, _P]),
     "fz_last_error": (C.c_int, [_P, C.c_char_p, C.c_size_t]),
     "fz_global_error": (C.c_int, [C.c_char_p, C.c_size_t]),
 }

@@ -176,6 +176,24 @@ int fz_source_waveform(int32_t src_opt, double glob_f, double f_cutoff, double d
 int fz_last_error(fz_handle* h, char* buf, size_t cap);
 int fz_global_error(char* buf, size_t cap);
 
+/* Allocation-free energy of caller-owned FP32 device fields. No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory (their fields live in a pool they manage, or
+ * they run where a cudaMalloc -- which may synchronise the device -- is not allowed). The caller
+ * passes device arrays p, u, v, w of n elements each and a device slot *out; the function
+ * enqueues two kernels on `stream` (a cudaStream_t, NULL = default stream) that write
+ * 0.5 * sum(p^2/(rho c^2) + rho |u|^2), accumulated in FP64, to *out, and returns without
+ * waiting. It calls no cudaMalloc/cudaFree: its scratch is a fixed device array of
+ * FZ_NOALLOC_MAX_BLOCKS doubles (32 KB) in the library, held by every GPU that loads it until
+ * the process exits. n may be at most FZ_NOALLOC_MAX_CELLS; larger n returns FZ_EINVAL.
+ * The first call on a device looks up that array's device address (with the device current);
+ * make that first call before any stream capture. All calls share the array: calls that overlap
+ * on the GPU race and give wrong results; order them (one stream, or events). */
+#define FZ_NOALLOC_MAX_BLOCKS 4096
+#define FZ_NOALLOC_MAX_CELLS (4096LL * 16384LL)
+int fz_energy_noalloc(const float* p, const float* u, const float* v, const float* w, int64_t n, double rho,
+                      double c, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
