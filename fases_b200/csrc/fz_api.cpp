@@ -78,11 +78,9 @@ void free_device(fz_handle* h) {
   dfree(h->d_cls);
   for (auto& p : h->d_pml_coef) dfree(p);
   for (auto& p : h->d_psi) dfree(p);
-  dfree(h->d_bcell);
-  dfree(h->d_bcorner);
+  dfree(h->d_brec);
   dfree(h->d_bgeo);
   dfree(h->d_bnrm);
-  dfree(h->d_bmat);
   for (auto& set : h->d_ade)
     for (auto& p : set) dfree(p);
   dfree(h->d_mat);
@@ -252,16 +250,20 @@ int build_band(fz_handle* h) {
   h->nB = (int64_t)cell.size();
   h->band_mat = mat;
   if (h->nB == 0) return FZ_OK;
-  FZ_CUDA(h, cudaMalloc(&h->d_bcell, cell.size() * 8), "cudaMalloc(band)");
-  FZ_CUDA(h, cudaMalloc(&h->d_bcorner, corner.size() * 8), "cudaMalloc(band)");
+  std::vector<int4> rec((size_t)h->nB);
+  for (size_t b = 0; b < rec.size(); b++) {
+    const uint64_t c = (uint64_t)cell[b];
+    rec[b].x = (int)(uint32_t)(c & 0xffffffffu);
+    rec[b].y = (int)(uint32_t)(c >> 32);
+    rec[b].z = (int)(corner[b] - cell[b]);  // within a few rows and planes: fits 32 bits
+    rec[b].w = mat[b];
+  }
+  FZ_CUDA(h, cudaMalloc(&h->d_brec, rec.size() * sizeof(int4)), "cudaMalloc(band)");
   FZ_CUDA(h, cudaMalloc(&h->d_bgeo, geo.size() * sizeof(R)), "cudaMalloc(band)");
   FZ_CUDA(h, cudaMalloc(&h->d_bnrm, nrm.size() * sizeof(R)), "cudaMalloc(band)");
-  FZ_CUDA(h, cudaMalloc(&h->d_bmat, mat.size() * 4), "cudaMalloc(band)");
-  FZ_CUDA(h, cudaMemcpy(h->d_bcell, cell.data(), cell.size() * 8, cudaMemcpyHostToDevice), "band H2D");
-  FZ_CUDA(h, cudaMemcpy(h->d_bcorner, corner.data(), corner.size() * 8, cudaMemcpyHostToDevice), "band H2D");
+  FZ_CUDA(h, cudaMemcpy(h->d_brec, rec.data(), rec.size() * sizeof(int4), cudaMemcpyHostToDevice), "band H2D");
   FZ_CUDA(h, cudaMemcpy(h->d_bgeo, geo.data(), geo.size() * sizeof(R), cudaMemcpyHostToDevice), "band H2D");
   FZ_CUDA(h, cudaMemcpy(h->d_bnrm, nrm.data(), nrm.size() * sizeof(R), cudaMemcpyHostToDevice), "band H2D");
-  FZ_CUDA(h, cudaMemcpy(h->d_bmat, mat.data(), mat.size() * 4, cudaMemcpyHostToDevice), "band H2D");
   return FZ_OK;
 }
 
@@ -432,16 +434,14 @@ fz::BandArgs<R> band_args(fz_handle* h, int stage) {
   R* const* in = (stage == 0) ? u0 : (stage == 1) ? u1 : u2;
   R* const* out = (stage == 1) ? u2 : u1;
   b.nB = h->nB;
-  b.cell = h->d_bcell; b.corner = h->d_bcorner;
-  b.geo = (const R*)h->d_bgeo; b.nrm = (const R*)h->d_bnrm; b.mat = h->d_bmat;
+  b.rec = h->d_brec;
+  b.geo = (const R*)h->d_bgeo; b.nrm = (const R*)h->d_bnrm;
   b.pi = in[0]; b.ui = in[1]; b.vi = in[2]; b.wi = in[3];
   b.po = out[0]; b.uo = out[1]; b.vo = out[2]; b.wo = out[3];
   b.Sx = h->Sx; b.plane = h->plane;
   b.Z0 = h->prm.rho * h->prm.c;
   b.dt = h->prm.dt;
-  // ADE stage coefficients (a, b, c) and state roles (left, middle, right), main3D.cu:1290-1306
-  static const double abc[3][3] = {{0, 1, 1}, {3, 1, 4}, {1, 2, 3}};
-  b.a_ssp = abc[stage][0]; b.b_ssp = abc[stage][1]; b.inv_c_ssp = 1.0 / abc[stage][2];
+  // ADE state roles (left, middle, right) of the stage, main3D.cu:1290-1306
   int L_, M_, R_;
   if (stage == 0) { L_ = h->ph_cur; M_ = h->ph_old; R_ = h->ph_old; }
   else if (stage == 1) { L_ = h->ph_nu; M_ = h->ph_old; R_ = h->ph_cur; }
@@ -501,7 +501,7 @@ cudaError_t enqueue_step(fz_handle* h) {
     }
     if (h->nB > 0) {
       Timer t(h, 3);
-      e = fz::launch_band<R>(band_args<R>(h, st), h->stream);
+      e = fz::launch_band<R>(st, band_args<R>(h, st), h->stream);
       if (e != cudaSuccess) return e;
     }
   }

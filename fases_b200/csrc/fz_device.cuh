@@ -115,11 +115,9 @@ struct StageMaps {
 template <class R>
 struct BandArgs {
   int64_t nB;
-  const int64_t* cell;    // device index of the band cell
-  const int64_t* corner;  // device index of the trilinear base corner
-  const R* geo;           // [4*nB]: sx, sy, sz, chi
-  const R* nrm;           // [4*nB]: nx, ny, nz, unused
-  const int32_t* mat;     // material id (oid - 1)
+  const int4* rec;  // per band cell: device index (lo, hi 32 bits), corner - cell, material (oid - 1)
+  const R* geo;     // [4*nB]: sx, sy, sz, chi
+  const R* nrm;     // [4*nB]: nx, ny, nz, unused
   const R* pi;            // stage input (probe source)
   const R* ui;
   const R* vi;
@@ -130,7 +128,6 @@ struct BandArgs {
   R* wo;
   int64_t Sx, plane;
   double Z0, dt;
-  double a_ssp, b_ssp, inv_c_ssp;
   int32_t K, L;
   const double* Rinf;
   const double* A;

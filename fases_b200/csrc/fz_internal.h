@@ -46,11 +46,9 @@ struct fz_handle {
   int64_t nB = 0;
   std::vector<int64_t> band_cell_ref;  // reference-layout cell index (for the material check)
   std::vector<int32_t> band_mat;
-  int64_t* d_bcell = nullptr;
-  int64_t* d_bcorner = nullptr;
+  int4* d_brec = nullptr;  // cell index (lo, hi), corner - cell, material
   void* d_bgeo = nullptr;
   void* d_bnrm = nullptr;
-  int32_t* d_bmat = nullptr;
   double* d_ade[3][3] = {{nullptr}};  // [set][phi, psi1, psi2]
   int ph_old = 0, ph_cur = 1, ph_nu = 2;
 

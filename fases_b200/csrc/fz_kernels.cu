@@ -76,26 +76,32 @@ __device__ __forceinline__ void weno_core(typename Pair<R>::T a, typename Pair<R
   const P E2 = pfma(b, psplat<R>(R(2)), D2);   // u_{i-2} - 4u_{i-1} + 3u_i
   const P E1 = padd(b, c);                     // -(u_{i-1} - u_{i+1})
   const P E0 = pfma(c, psplat<R>(R(-2)), D0);  // 3u_i - 4u_{i+1} + u_{i+2} (sign)
+  // 12/13 (beta_r + eps) = D_r^2 + 3/13 E_r^2 + 12/13 eps
   const P k313 = psplat<R>(R(3.0 / 13.0));
-  const P B0 = pfma(D0, D0, pmul(pmul(E0, k313), E0));
-  const P B1 = pfma(D1, D1, pmul(pmul(E1, k313), E1));
-  const P B2 = pfma(D2, D2, pmul(pmul(E2, k313), E2));
   const P eps = psplat<R>(R(1e-10 * 12.0 / 13.0));
+  const P B0 = pfma(D0, D0, pfma(pmul(E0, k313), E0, eps));
+  const P B1 = pfma(D1, D1, pfma(pmul(E1, k313), E1, eps));
+  const P B2 = pfma(D2, D2, pfma(pmul(E2, k313), E2, eps));
   const P tau = pabs(psub(B0, B2));
   const P one = psplat<R>(R(1));
-  const P q0w = pfma(tau, prcp(padd(B0, eps)), one);
-  const P q1w = pfma(tau, prcp(padd(B1, eps)), one);
-  const P q2w = pfma(tau, prcp(padd(B2, eps)), one);
+  const P q0w = pfma(tau, prcp(B0), one);
+  const P q1w = pfma(tau, prcp(B1), one);
+  const P q2w = pfma(tau, prcp(B2), one);
   // normalisers: V- uses d = (3/10, 3/5, 1/10), V+ the mirrored (1/10, 3/5, 3/10)
-  const P Sm = pfma(q2w, psplat<R>(R(0.1)), pfma(q1w, psplat<R>(R(0.6)), pmul(q0w, psplat<R>(R(0.3)))));
-  const P Sp = pfma(q2w, psplat<R>(R(0.3)), pfma(q1w, psplat<R>(R(0.6)), pmul(q0w, psplat<R>(R(0.1)))));
-  // d_r * delta_r for both faces
-  const P em0 = pfma(c, psplat<R>(R(0.2)), pmul(d, psplat<R>(R(-0.05))));
-  const P em1 = pfma(b, psplat<R>(R(0.1)), pmul(c, psplat<R>(R(0.2))));
-  const P em2 = pfma(a, psplat<R>(R(-1.0 / 30.0)), pmul(b, psplat<R>(R(1.0 / 12.0))));
-  const P ep0 = pfma(c, psplat<R>(R(-1.0 / 12.0)), pmul(d, psplat<R>(R(1.0 / 30.0))));
-  const P ep1 = pfma(b, psplat<R>(R(-0.2)), pmul(c, psplat<R>(R(-0.1))));
-  const P ep2 = pfma(a, psplat<R>(R(0.05)), pmul(b, psplat<R>(R(-0.2))));
+  const P t1 = pmul(q1w, psplat<R>(R(0.6)));
+  const P Sm = pfma(q0w, psplat<R>(R(0.3)), pfma(q2w, psplat<R>(R(0.1)), t1));
+  const P Sp = pfma(q0w, psplat<R>(R(0.1)), pfma(q2w, psplat<R>(R(0.3)), t1));
+  // d_r * delta_r for both faces, written on the first and second differences:
+  //   em0 = 0.15 c - 0.05 D0      ep0 = -0.05 c + D0/30
+  //   em1 = 0.15 E1 + 0.05 D1     ep1 = -0.15 E1 + 0.05 D1
+  //   em2 = 0.05 b + D2/30        ep2 = -0.15 b - 0.05 D2
+  const P h1 = pmul(D1, psplat<R>(R(0.05)));
+  const P em0 = pfma(c, psplat<R>(R(0.15)), pmul(D0, psplat<R>(R(-0.05))));
+  const P ep0 = pfma(c, psplat<R>(R(-0.05)), pmul(D0, psplat<R>(R(1.0 / 30.0))));
+  const P em1 = pfma(E1, psplat<R>(R(0.15)), h1);
+  const P ep1 = pfma(E1, psplat<R>(R(-0.15)), h1);
+  const P em2 = pfma(b, psplat<R>(R(0.05)), pmul(D2, psplat<R>(R(1.0 / 30.0))));
+  const P ep2 = pfma(b, psplat<R>(R(-0.15)), pmul(D2, psplat<R>(R(-0.05))));
   const P Nm = pfma(q2w, em2, pfma(q1w, em1, pmul(q0w, em0)));
   const P Np = pfma(q2w, ep2, pfma(q1w, ep1, pmul(q0w, ep0)));
   vm = pfma(Nm, prcp(Sm), q0);
@@ -479,21 +485,40 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
 template <class R>
 __device__ __forceinline__ R trilin(const R* __restrict__ f, int64_t q, int64_t Sx, int64_t plane, R sx,
                                     R sy, R sz) {
-  const R c00 = f[q] * (R(1) - sx) + f[q + 1] * sx;
-  const R c10 = f[q + Sx] * (R(1) - sx) + f[q + Sx + 1] * sx;
-  const R c01 = f[q + plane] * (R(1) - sx) + f[q + plane + 1] * sx;
-  const R c11 = f[q + plane + Sx] * (R(1) - sx) + f[q + plane + Sx + 1] * sx;
+  const R c00 = __ldg(f + q) * (R(1) - sx) + __ldg(f + q + 1) * sx;
+  const R c10 = __ldg(f + q + Sx) * (R(1) - sx) + __ldg(f + q + Sx + 1) * sx;
+  const R c01 = __ldg(f + q + plane) * (R(1) - sx) + __ldg(f + q + plane + 1) * sx;
+  const R c11 = __ldg(f + q + plane + Sx) * (R(1) - sx) + __ldg(f + q + plane + Sx + 1) * sx;
   const R c0 = c00 * (R(1) - sy) + c10 * sy, c1 = c01 * (R(1) - sy) + c11 * sy;
   return c0 * (R(1) - sz) + c1 * sz;
 }
 
 template <class R>
-__global__ void __launch_bounds__(256) k_band(const BandArgs<R> B) {
+struct Vec4;
+template <>
+struct Vec4<float> {
+  typedef float4 T;
+};
+template <>
+struct Vec4<double> {
+  typedef double4 T;
+};
+
+// STAGE selects the ADE stage coefficients (a, b, c) = (0,1,1), (3,1,4), (1,2,3)
+// (main3D.cu:1290, 1298, 1306): left = (a middle + b (right + dt L(right))) / c.
+template <class R, int STAGE>
+__global__ void __launch_bounds__(256, 4) k_band(const BandArgs<R> B) {
+  typedef typename Vec4<R>::T V4;
   const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= B.nB) return;
-  const int64_t cell = B.cell[b], q = B.corner[b];
-  const R sx = B.geo[4 * b + 0], sy = B.geo[4 * b + 1], sz = B.geo[4 * b + 2], chi = B.geo[4 * b + 3];
-  const R nx = B.nrm[4 * b + 0], ny = B.nrm[4 * b + 1], nz = B.nrm[4 * b + 2];
+  const int4 rc = B.rec[b];
+  const int64_t cell = (int64_t)(((uint64_t)(uint32_t)rc.y << 32) | (uint32_t)rc.x);
+  const int64_t q = cell + rc.z;
+  const int m = rc.w;
+  const V4 g4 = reinterpret_cast<const V4*>(B.geo)[b];
+  const V4 n4 = reinterpret_cast<const V4*>(B.nrm)[b];
+  const R sx = g4.x, sy = g4.y, sz = g4.z, chi = g4.w;
+  const R nx = n4.x, ny = n4.y, nz = n4.z;
   const R pD = trilin<R>(B.pi, q, B.Sx, B.plane, sx, sy, sz);
   const R uD = trilin<R>(B.ui, q, B.Sx, B.plane, sx, sy, sz);
   const R vD = trilin<R>(B.vi, q, B.Sx, B.plane, sx, sy, sz);
@@ -501,7 +526,9 @@ __global__ void __launch_bounds__(256) k_band(const BandArgs<R> B) {
   const R un = uD * nx + vD * ny + wD * nz;
   const R utx = uD - un * nx, uty = vD - un * ny, utz = wD - un * nz;
   const double wout = (double)pD + B.Z0 * (double)un;  // outgoing characteristic
-  const int m = B.mat[b];
+  constexpr double a_ssp = (STAGE == 0) ? 0.0 : (STAGE == 1) ? 3.0 : 1.0;
+  constexpr double b_ssp = (STAGE == 2) ? 2.0 : 1.0;
+  constexpr double inv_c = (STAGE == 0) ? 1.0 : (STAGE == 1) ? 0.25 : 1.0 / 3.0;
   const int64_t nB = B.nB;
   double sumA = 0.0, sumBC = 0.0;
   for (int k = 0; k < B.K; ++k) {
@@ -509,7 +536,9 @@ __global__ void __launch_bounds__(256) k_band(const BandArgs<R> B) {
     const int64_t si = (int64_t)k * nB + b;
     const double r = B.phR[si];
     const double Lphi = wout - B.zeta[mi] * r;
-    const double v = (B.a_ssp * B.phM[si] + B.b_ssp * (r + B.dt * Lphi)) * B.inv_c_ssp;
+    double v = b_ssp * (r + B.dt * Lphi);
+    if (STAGE > 0) v += a_ssp * B.phM[si];
+    v *= inv_c;
     B.phL[si] = v;
     sumA += B.A[mi] * v;
   }
@@ -519,8 +548,14 @@ __global__ void __launch_bounds__(256) k_band(const BandArgs<R> B) {
     const double r1 = B.s1R[si], r2 = B.s2R[si];
     const double L1 = wout - (B.alpha[mi] * r1 + B.beta[mi] * r2);
     const double L2 = B.beta[mi] * r1 - B.alpha[mi] * r2;
-    const double n1 = (B.a_ssp * B.s1M[si] + B.b_ssp * (r1 + B.dt * L1)) * B.inv_c_ssp;
-    const double n2 = (B.a_ssp * B.s2M[si] + B.b_ssp * (r2 + B.dt * L2)) * B.inv_c_ssp;
+    double n1 = b_ssp * (r1 + B.dt * L1);
+    double n2 = b_ssp * (r2 + B.dt * L2);
+    if (STAGE > 0) {
+      n1 += a_ssp * B.s1M[si];
+      n2 += a_ssp * B.s2M[si];
+    }
+    n1 *= inv_c;
+    n2 *= inv_c;
     B.s1L[si] = n1;
     B.s2L[si] = n2;
     sumBC += B.B[mi] * n1 + B.C[mi] * n2;
@@ -618,11 +653,16 @@ cudaError_t launch_stage(int stage, const StageArgs<R>& a, const StageMaps& m, d
 }
 
 template <class R>
-cudaError_t launch_band(const BandArgs<R>& a, cudaStream_t s) {
+cudaError_t launch_band(int stage, const BandArgs<R>& a, cudaStream_t s) {
   if (a.nB <= 0) return cudaSuccess;
   const int bs = 256;
   const int64_t nb = (a.nB + bs - 1) / bs;
-  k_band<R><<<(unsigned)nb, bs, 0, s>>>(a);
+  if (stage == 0)
+    k_band<R, 0><<<(unsigned)nb, bs, 0, s>>>(a);
+  else if (stage == 1)
+    k_band<R, 1><<<(unsigned)nb, bs, 0, s>>>(a);
+  else
+    k_band<R, 2><<<(unsigned)nb, bs, 0, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -645,7 +685,7 @@ cudaError_t launch_energy(const R* p, const R* u, const R* v, const R* w, int64_
   template cudaError_t stage_setup<R>();                                                           \
   template cudaError_t stage_occupancy<R>(int*);                                                   \
   template cudaError_t launch_stage<R>(int, const StageArgs<R>&, const StageMaps&, dim3, cudaStream_t); \
-  template cudaError_t launch_band<R>(const BandArgs<R>&, cudaStream_t);                           \
+  template cudaError_t launch_band<R>(int, const BandArgs<R>&, cudaStream_t);                      \
   template cudaError_t launch_receivers<R>(const R*, const R*, const R*, const R*, const int64_t*, \
                                            int, double*, double*, int64_t, int64_t*,               \
                                            cudaStream_t);                                          \

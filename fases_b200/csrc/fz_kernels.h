@@ -16,7 +16,7 @@ cudaError_t stage_occupancy(int* blocks_per_sm);
 template <class R>
 cudaError_t launch_stage(int stage, const StageArgs<R>& a, const StageMaps& m, dim3 grid, cudaStream_t s);
 template <class R>
-cudaError_t launch_band(const BandArgs<R>& a, cudaStream_t s);
+cudaError_t launch_band(int stage, const BandArgs<R>& a, cudaStream_t s);
 template <class R>
 cudaError_t launch_receivers(const R* p, const R* u, const R* v, const R* w, const int64_t* rcell,
                              int nrec, double* ir, double* vel, int64_t cap, int64_t* step,
