@@ -47,6 +47,8 @@ class FzParams(C.Structure):
         ("rho", C.c_double),
         ("dt", C.c_double),
         ("tol_cells", C.c_double),
+        ("two_d", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 

@@ -496,7 +496,7 @@ cudaError_t enqueue_step(fz_handle* h) {
       m.bv = h->own_map[h->i0][2];
       m.bw = h->own_map[h->i0][3];
       m.cls = h->cls_map;
-      e = fz::launch_stage<R>(st, stage_args<R>(h, st), m, h->stage_grid, h->stream);
+      e = fz::launch_stage<R>(st, h->prm.two_d != 0, stage_args<R>(h, st), m, h->stage_grid, h->stream);
       if (e != cudaSuccess) return e;
     }
     if (h->nB > 0) {
@@ -681,6 +681,8 @@ int fz_create(const fz_params* p, fz_handle** out) {
   *out = nullptr;
   if (p->abi_version != FZ_ABI_VERSION)
     return fzi::set_global_error(FZ_EINVAL, "fz_create: abi_version mismatch");
+  if (p->two_d && (p->pml[0] || p->pml[1]))
+    return fzi::set_global_error(FZ_EINVAL, "fz_create: a planar (two_d) solve has no z faces: U_PML and D_PML must be 0");
   if (!(p->h > 0) || !(p->c > 0) || !(p->rho > 0) || !(p->dt > 0) || p->pml_cells < 1 ||
       (p->precision != FZ_FP32 && p->precision != FZ_FP64) || !(p->tol_cells > 1.0))
     return fzi::set_global_error(FZ_EINVAL, "fz_create: invalid parameter (h, c, rho, dt > 0; pml_cells >= 1; "
@@ -737,6 +739,8 @@ int fz_load_geometry_raw(fz_handle* h, const float* S, const uint8_t* oid, int32
   const int minn = 2 * GHOST + 1;
   if (Nx < minn || Ny < minn || Nz < minn)
     return set_error(h, FZ_EINVAL, "fz_load_geometry_raw: grid must be at least 7 cells per axis");
+  if (h->prm.two_d && Nz != minn)
+    return set_error(h, FZ_EINVAL, "fz_load_geometry_raw: a planar (two_d) grid has Nz = 7 (one plane plus ghosts)");
   if (h->prm.pml_cells * 2 + 2 * GHOST > std::min(Nx, std::min(Ny, Nz)) &&
       (h->prm.pml[0] || h->prm.pml[1] || h->prm.pml[2] || h->prm.pml[3] || h->prm.pml[4] || h->prm.pml[5]))
     ;  // narrow domains with overlapping PML bands follow the reference's index rule

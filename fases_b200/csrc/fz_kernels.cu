@@ -229,7 +229,8 @@ __device__ __forceinline__ R source_sum(const StageArgs<R>& A, int64_t g) {
 #ifndef FZ_STAGE_MINBLOCKS_F32
 #define FZ_STAGE_MINBLOCKS_F32 2  // two 16-warp CTAs per SM in FP32 (64 registers, no spills)
 #endif
-template <class R, int STAGE>
+// DIM2: planar solve (one updated z-plane, no z fluxes): the 3D scheme restricted to 2D.
+template <class R, int STAGE, bool DIM2>
 __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_F32 : 1)
     k_stage(const StageArgs<R> A, const __grid_constant__ StageMaps M) {
   typedef typename Pair<R>::T P;
@@ -299,16 +300,20 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
   };
 
   // z prologue: centres kb-1 and kb give the flux through face kb-1/2 and V-(kb+1/2).
-  P z0 = ld_pw(kb - 3), z1 = ld_pw(kb - 2), z2 = ld_pw(kb - 1), z3 = ld_pw(kb), z4 = ld_pw(kb + 1);
-  P z5 = ld_pw(kb + 2);
-  P qe_next = ld_pw(kb + 3);
-  P zm, zp, vmB, vpB;
-  weno_center<R>(z0, z1, z2, z3, z4, zm, zp);
-  weno_center<R>(z1, z2, z3, z4, z5, vmB, vpB);
-  P Fz_lo = godunov<R>(zm, vpB, kA, kC);
-  zm = vmB;
-  // queue of plane values k-1 .. k+2 for the centre of plane k+1
-  P qa = z2, qb = z3, qc = z4, qd = z5;
+  const P zero = psplat<R>(R(0));
+  P qa = zero, qb = zero, qc = zero, qd = zero, qe_next = zero, zm = zero, Fz_lo = zero;
+  if (!DIM2) {
+    const P z0 = ld_pw(kb - 3), z1 = ld_pw(kb - 2), z2 = ld_pw(kb - 1), z3 = ld_pw(kb), z4 = ld_pw(kb + 1);
+    const P z5 = ld_pw(kb + 2);
+    qe_next = ld_pw(kb + 3);
+    P m0, p0, m1, p1;
+    weno_center<R>(z0, z1, z2, z3, z4, m0, p0);
+    weno_center<R>(z1, z2, z3, z4, z5, m1, p1);
+    Fz_lo = godunov<R>(m0, p1, kA, kC);
+    zm = m1;
+    // queue of plane values k-1 .. k+2 for the centre of plane k+1
+    qa = z2; qb = z3; qc = z4; qd = z5;
+  }
 
 
   // cPML membership of this column along x and y (fixed during the march)
@@ -325,12 +330,14 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
 
     // ---- register loads for this plane (prefetched) and the next one
     const P qe = qe_next;
-    if (it + 1 < nplanes) qe_next = ld_pw(k + 4);
-
-    // ---- z: centre k+1 -> flux through face k+1/2
-    P vmC, vpC;
-    weno_center<R>(qa, qb, qc, qd, qe, vmC, vpC);
-    const P Fz_hi = godunov<R>(zm, vpC, kA, kC);
+    P vmC = zero, Fz_hi = zero;
+    if (!DIM2) {
+      if (it + 1 < nplanes) qe_next = ld_pw(k + 4);
+      // ---- z: centre k+1 -> flux through face k+1/2
+      P vpC;
+      weno_center<R>(qa, qb, qc, qd, qe, vmC, vpC);
+      Fz_hi = godunov<R>(zm, vpC, kA, kC);
+    }
 
     // ---- plane k tile
     if (!mbar_wait_bounded(&mbar[buf], parity)) {
@@ -395,7 +402,8 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
         const P Lx = psub(Fx_lo, Fx_hi), Ly = psub(Fy_lo, Fy_hi), Lz = psub(Fz_lo, Fz_hi);
         const R Lp = Lx.x + Ly.x + Lz.x;
         const int c0 = (ty + HY) * PW + (tx + HX);
-        const R p_in = qb.x, w_in = qb.y, u_in = Tu[c0], v_in = Tv[c0];
+        const R p_in = DIM2 ? Tp[c0] : qb.x, w_in = DIM2 ? A.wi[g] : qb.y;
+        const R u_in = Tu[c0], v_in = Tv[c0];
         R pn, un, vn, wn;
         R bp = R(0), bu = R(0), bv = R(0), bw = R(0);
         if (STAGE > 0) {
@@ -625,30 +633,42 @@ size_t stage_smem_bytes() {
 template <class R>
 cudaError_t stage_setup() {
   const int bytes = (int)stage_smem_bytes<R>();
-  cudaError_t e;
-  e = cudaFuncSetAttribute(k_stage<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_stage<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_stage<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  const void* fns[6] = {(const void*)k_stage<R, 0, false>, (const void*)k_stage<R, 1, false>,
+                        (const void*)k_stage<R, 2, false>, (const void*)k_stage<R, 0, true>,
+                        (const void*)k_stage<R, 1, true>,  (const void*)k_stage<R, 2, true>};
+  for (const void* f : fns) {
+    const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 template <class R>
 cudaError_t stage_occupancy(int* blocks_per_sm) {
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_stage<R, 0>, NTHREADS,
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_stage<R, 0, false>, NTHREADS,
                                                         stage_smem_bytes<R>());
 }
 
 template <class R>
-cudaError_t launch_stage(int stage, const StageArgs<R>& a, const StageMaps& m, dim3 grid, cudaStream_t s) {
+cudaError_t launch_stage(int stage, bool two_d, const StageArgs<R>& a, const StageMaps& m, dim3 grid,
+                         cudaStream_t s) {
   const dim3 block(TX, TY, 1);
   const size_t smem = stage_smem_bytes<R>();
-  if (stage == 0)
-    k_stage<R, 0><<<grid, block, smem, s>>>(a, m);
-  else if (stage == 1)
-    k_stage<R, 1><<<grid, block, smem, s>>>(a, m);
-  else
-    k_stage<R, 2><<<grid, block, smem, s>>>(a, m);
+  if (!two_d) {
+    if (stage == 0)
+      k_stage<R, 0, false><<<grid, block, smem, s>>>(a, m);
+    else if (stage == 1)
+      k_stage<R, 1, false><<<grid, block, smem, s>>>(a, m);
+    else
+      k_stage<R, 2, false><<<grid, block, smem, s>>>(a, m);
+  } else {
+    if (stage == 0)
+      k_stage<R, 0, true><<<grid, block, smem, s>>>(a, m);
+    else if (stage == 1)
+      k_stage<R, 1, true><<<grid, block, smem, s>>>(a, m);
+    else
+      k_stage<R, 2, true><<<grid, block, smem, s>>>(a, m);
+  }
   return cudaGetLastError();
 }
 
@@ -684,7 +704,7 @@ cudaError_t launch_energy(const R* p, const R* u, const R* v, const R* w, int64_
   template size_t stage_smem_bytes<R>();                                                           \
   template cudaError_t stage_setup<R>();                                                           \
   template cudaError_t stage_occupancy<R>(int*);                                                   \
-  template cudaError_t launch_stage<R>(int, const StageArgs<R>&, const StageMaps&, dim3, cudaStream_t); \
+  template cudaError_t launch_stage<R>(int, bool, const StageArgs<R>&, const StageMaps&, dim3, cudaStream_t); \
   template cudaError_t launch_band<R>(int, const BandArgs<R>&, cudaStream_t);                      \
   template cudaError_t launch_receivers<R>(const R*, const R*, const R*, const R*, const int64_t*, \
                                            int, double*, double*, int64_t, int64_t*,               \

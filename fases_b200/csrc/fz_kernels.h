@@ -14,7 +14,8 @@ cudaError_t stage_setup();
 template <class R>
 cudaError_t stage_occupancy(int* blocks_per_sm);
 template <class R>
-cudaError_t launch_stage(int stage, const StageArgs<R>& a, const StageMaps& m, dim3 grid, cudaStream_t s);
+cudaError_t launch_stage(int stage, bool two_d, const StageArgs<R>& a, const StageMaps& m, dim3 grid,
+                         cudaStream_t s);
 template <class R>
 cudaError_t launch_band(int stage, const BandArgs<R>& a, cudaStream_t s);
 template <class R>

@@ -171,3 +171,76 @@ def benchmark_room(room_cells=(500, 400, 200), h=0.02, seed=0, n_obstacles=5, op
         "scene": scene, "materials": wall_mats + obst_mats, "pml": tuple(pml), "c": c, "rho": rho, "dt": dt,
         "h": h, "source_cell": src, "receivers": recs, "p0": p0, "seed": seed, "f_cutoff": f_cutoff,
     }
+
+
+def box_room_2d(room_cells, h, obstacles_cells=(), tol_cells=3.0, band_cells=8.0):
+    """Planar room for the two_d solve: the 2D signed distance of an (nx, ny) rectangle with box
+    obstacles [((i0, j0), (i1, j1)), ...], replicated over the 7 planes of a planar grid (one
+    updated plane between 3 ghost planes on each side). Layers: x_lo, x_hi, y_lo, y_hi, then
+    obstacles."""
+    nx, ny = room_cells
+    Nx, Ny, Nz = nx + 2 * GHOST, ny + 2 * GHOST, 2 * GHOST + 1
+    f32 = np.float32
+    X = ((np.arange(Nx) + 0.5) * h).astype(f32)[None, :]
+    Y = ((np.arange(Ny) + 0.5) * h).astype(f32)[:, None]
+    lo = np.array([GHOST * h] * 2, f32)
+    hi = (lo + np.array([nx, ny]) * h).astype(f32)
+    walls = [X - lo[0], hi[0] - X, Y - lo[1], hi[1] - Y]
+    shape = (Ny, Nx)
+    S = np.full(shape, np.inf, f32)
+    layer = np.zeros(shape, np.int16)
+    for wi, d in enumerate(walls):
+        d = np.broadcast_to(d, shape)
+        m = d < S
+        S = np.where(m, d, S)
+        layer = np.where(m, np.int16(wi), layer)
+    ox = np.maximum(np.maximum(lo[0] - X, X - hi[0]), 0)
+    oy = np.maximum(np.maximum(lo[1] - Y, Y - hi[1]), 0)
+    S = np.where(S > 0, S, -np.sqrt(ox * ox + oy * oy)).astype(f32)
+    for q, (c0, c1) in enumerate(obstacles_cells):
+        b0 = (lo + np.array(c0, float) * h).astype(f32)
+        b1 = (lo + np.array(c1, float) * h).astype(f32)
+        qx = np.maximum(b0[0] - X, X - b1[0])
+        qy = np.maximum(b0[1] - Y, Y - b1[1])
+        d = (np.sqrt(np.maximum(qx, 0) ** 2 + np.maximum(qy, 0) ** 2) + np.minimum(np.maximum(qx, qy), 0)).astype(f32)
+        layer = np.where(d < S, np.int16(4 + q), layer)
+        S = np.minimum(S, d)
+    S = np.clip(S, -f32(band_cells * h), f32(band_cells * h)).astype(f32)
+    oid2 = np.full(shape, 0xFF, np.uint8)
+    sel = (S >= 0) & (S <= f32(tol_cells * h))
+    sel[0, :] = sel[-1, :] = False
+    sel[:, 0] = sel[:, -1] = False
+    oid2[sel] = (layer[sel] + 1).astype(np.uint8)
+    S3 = np.ascontiguousarray(np.broadcast_to(S, (Nz,) + shape))
+    oid3 = np.ascontiguousarray(np.broadcast_to(oid2, (Nz,) + shape)).copy()
+    oid3[0] = oid3[-1] = 0xFF  # outermost planes carry no material (parsing3D.h:985-987)
+    names = ["x_lo", "x_hi", "y_lo", "y_hi"] + [f"obstacle{q}" for q in range(len(obstacles_cells))]
+    return Scene(S3, oid3, h, (nx, ny, 1), names, [])
+
+
+def benchmark_2d(room_cells=(256, 256), h=0.02, seed=0, c=343.0, rho=1.2, cfl=0.5, pml_cells=16, n_receivers=4,
+                 pulse_sigma_cells=3.0):
+    """The plain 2D benchmark (FP64): 256 x 256 cells at h = 0.02 m, a 16-cell cPML on the x-hi
+    side (whose wall is a matched layer), rigid walls (R = 0.99) on x-lo and y-hi, one ADE wall on
+    y-lo with 2 seeded real poles in [1e2, 1e4] 1/s and passive residues, a Gaussian pressure
+    pulse (sigma = 3 cells) at a seeded interior point, and seeded receivers."""
+    rng = np.random.default_rng(seed)
+    scene = box_room_2d(room_cells, h)
+    dt = cfl * h / c
+    f_cutoff = c / (4 * h)
+    ade = mats.random_passive(rng, dt, f_cutoff, K=2, L=0)
+    wall_mats = [mats.rigid(0.99), mats.matched(), ade, mats.rigid(0.99)]
+    pml = (0, 0, 1, 0, 0, 0)  # R = x-hi
+    nx, ny = room_cells
+    pts = []
+    while len(pts) < n_receivers + 1:
+        i = int(rng.integers(pml_cells + 12, nx - pml_cells - 12)) + GHOST
+        j = int(rng.integers(12, ny - 12)) + GHOST
+        pts.append((i, j, GHOST))
+    src = np.array(pts[0], np.int32)
+    recs = np.array(pts[1:], np.int32)
+    p0 = gaussian_pulse(scene.shape, h, src, pulse_sigma_cells)
+    p0[:GHOST] = 0.0
+    p0[GHOST + 1:] = 0.0
+    return {"scene": scene, "materials": wall_mats, "pml": pml, "pml_cells": pml_cells, "c": c, "rho": rho,
+            "dt": dt, "h": h, "source_cell": src, "receivers": recs, "p0": p0, "seed": seed}

@@ -19,7 +19,7 @@ def _dptr(a):
 
 
 def params(h=0.02, c=None, rho=None, dt=None, cfl=0.5, pml=(0, 0, 0, 0, 0, 0), pml_cells=20,
-           precision="fp32", device=0, tol_cells=3.0):
+           precision="fp32", device=0, tol_cells=3.0, two_d=False):
     """Solver parameters. c/rho default to the reference's 20 degC air (main3D.cu:450-456);
     dt = cfl*h/c (main3D.cu:729-730). pml = (U, D, R, L, F, B) face keys (main3D.cu:155-160)."""
     p = FzParams()
@@ -36,6 +36,7 @@ def params(h=0.02, c=None, rho=None, dt=None, cfl=0.5, pml=(0, 0, 0, 0, 0, 0), p
         p.rho = float(rho)
     p.dt = float(dt) if dt is not None else float(cfl) * p.h / p.c
     p.tol_cells = float(tol_cells)
+    p.two_d = 1 if two_d else 0
     return p
 
 

@@ -71,6 +71,10 @@ typedef struct fz_params {
   double rho;          /* air density [kg/m^3] */
   double dt;           /* time step [s] */
   double tol_cells;    /* immersed blending band in cells: tol = tol_cells*h (reference: 3) */
+  int32_t two_d;       /* 1: planar solve -- the grid has exactly one updated z-plane (Nz = 7 with
+                          the ghost cells), no z fluxes and no z cPML; the 3D scheme restricted to
+                          2D (config 1 of the benchmarks). 0: 3D. */
+  int32_t reserved;
 } fz_params;
 
 /* Fills p with the reference defaults: FP32, device 0, 20 PML cells, no PML faces, h = 0.02,

@@ -121,6 +121,7 @@ typedef struct orc_setup {
   int32_t nrec;
   const int64_t* rec_cell;
   int64_t max_steps;
+  int32_t two_d;  // 1: one updated z-plane, no z fluxes (the 3D scheme restricted to 2D)
 } orc_setup;
 
 }  // extern "C"
@@ -220,6 +221,10 @@ struct Oracle {
           const R* vel[3] = {in.u.data(), in.v.data(), in.w.data()};
           const ptrdiff_t st3[3] = {sx, sy, sz};
           for (int a = 0; a < 3; a++) {
+            if (a == 2 && cfg.two_d) {
+              fl[2][0] = fl[2][1] = fl[2][2] = fl[2][3] = 0.0;
+              continue;
+            }
             const R* pp = in.p.data() + ci;
             const R* qq = vel[a] + ci;
             const ptrdiff_t s = st3[a];

@@ -26,6 +26,7 @@ class OrcSetup(C.Structure):
         ("n_us", C.c_int64),
         ("nrec", C.c_int32), ("rec_cell", C.POINTER(C.c_int64)),
         ("max_steps", C.c_int64),
+        ("two_d", C.c_int32),
     ]
 
 
@@ -72,7 +73,8 @@ class Oracle:
     """FP64 CPU restatement of the reference solver on one scene (reference array layout)."""
 
     def __init__(self, S, oid, h, c, rho, dt, pml=(0,) * 6, pml_cells=20, tol_cells=3.0, materials=None,
-                 src_cells=None, sval=None, src_opt=0, src_freq=None, u_s=None, rec_cells=None, max_steps=0):
+                 src_cells=None, sval=None, src_opt=0, src_freq=None, u_s=None, rec_cells=None, max_steps=0,
+                 two_d=False):
         L = lib()
         self._keep = []
         S = np.ascontiguousarray(S, np.float32)
@@ -125,6 +127,7 @@ class Oracle:
             st.rec_cell = rc.ctypes.data_as(C.POINTER(C.c_int64))
         self.nrec = st.nrec
         st.max_steps = max_steps
+        st.two_d = 1 if two_d else 0
         self.max_steps = max_steps
         self._h = L.orc_create(C.byref(st))
         if not self._h:
