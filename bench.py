@@ -42,6 +42,9 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=12000, help="length of the end-to-end job")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--config", default="plain3d", choices=["plain3d", "plain2d", "precision"],
+                    help="plain3d: the headline room (default); plain2d: the 2D FP64 room; "
+                         "precision: FP32 bulk vs all-FP64 on a 256^3 room")
     return ap.parse_args()
 
 
@@ -134,10 +137,10 @@ def workload(room):
     return b
 
 
-def make_solver(b, precision, capacity):
+def make_solver(b, precision, capacity, device=0):
     from fases_b200 import Solver, params
     prm = params(h=b["h"], c=b["c"], rho=b["rho"], dt=b["dt"], pml=b["pml"], pml_cells=20, precision=precision,
-                 device=0)
+                 device=device)
     s = Solver(prm)
     sc = b["scene"]
     s.load_geometry(sc.S, sc.oid)
@@ -203,19 +206,109 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def rel_l2(a, b):
+    a = np.asarray(a, float)
+    b = np.asarray(b, float)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def run_plain2d(args):
+    """Config 1: 256 x 256 planar room, FP64, 2000 steps (--steps overrides), 4 receivers; the IR
+    error against the FP64 oracle on the whole run, and the oracle's own speed."""
+    from fases_b200 import Solver, params
+    from fases_b200 import materials as mats
+    from fases_b200 import scenes
+    from oracle.oracle import Oracle
+    b = scenes.benchmark_2d()
+    steps = args.steps if args.steps != 300 else 2000
+    sc = b["scene"]
+    m = mats.pack(b["materials"])
+    prm = params(h=b["h"], c=b["c"], rho=b["rho"], dt=b["dt"], pml=b["pml"], pml_cells=b["pml_cells"],
+                 precision="fp64", two_d=True)
+    s = Solver(prm)
+    s.load_geometry(sc.S, sc.oid)
+    s.set_materials(m["Rinf"], m["A"], m["zeta"], m["B"], m["Cc"], m["alpha"], m["beta"])
+    s.set_receivers(b["receivers"], steps)
+    s.set_fields(p=b["p0"])
+    ms = s.run_timed(steps)
+    ir = s.ir()
+    s.close()
+    cells = 256 * 256
+    threads = os.cpu_count()
+    o = Oracle(sc.S, sc.oid, b["h"], b["c"], b["rho"], b["dt"], pml=b["pml"], pml_cells=b["pml_cells"], materials=m,
+               rec_cells=b["receivers"], max_steps=steps, two_d=True)
+    o.set_fields(p=b["p0"])
+    t = time.perf_counter()
+    o.run(steps, threads=threads)
+    t_cpu = time.perf_counter() - t
+    ir_o, _ = o.ir()
+    errs = [rel_l2(ir[r], ir_o[r]) for r in range(ir.shape[0])]
+    print(json.dumps({
+        "metric": "Gcell-updates/s, 2D FP64 (config 1)", "value": cells * steps / (ms / 1e3) / 1e9, "unit": UNIT,
+        "n_gpus": 1, "steps": steps, "ms_per_step": ms / steps, "higher_is_better": True, "dtype": "f64",
+        "data": "synthetic (seeded)",
+        "config": {"workload": "planar 256x256 room, h=0.02, 16-cell cPML on x-hi, rigid x-lo/y-hi, ADE y-lo "
+                               "(2 real poles), Gaussian pulse sigma=3, 4 receivers", "room_cells": cells},
+        "ir_rel_l2_vs_fp64_oracle": errs,
+        "cpu_baseline": {"value": cells * steps / t_cpu / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"the full {steps}-step run, FP64, {t_cpu:.1f} s"}}), flush=True)
+
+
+def run_precision(args):
+    """Config 3: 256^3 room with the config-2 material model; FP32 field state (FP64 ADE state,
+    FP64 receiver samples) against all-FP64, per-receiver IR rel-L2 and energy drift."""
+    from fases_b200 import materials as mats
+    from fases_b200 import scenes
+    steps = args.steps if args.steps != 300 else 30000
+    b = scenes.benchmark_room(room_cells=(256, 256, 256), n_obstacles=5, n_receivers=8)
+    b["packed"] = mats.pack(b["materials"])
+    chunks = 10
+    out = {}
+    for prec in ("fp32", "fp64"):
+        s = make_solver(b, prec, steps)
+        E = [s.energy()]
+        t_ms = 0.0
+        for q in range(chunks):
+            n = steps // chunks + (1 if q < steps % chunks else 0)
+            t_ms += s.run_timed(n)
+            E.append(s.energy())
+        out[prec] = {"ir": s.ir(), "E": np.array(E), "ms": t_ms}
+        s.close()
+    ir32, ir64 = out["fp32"]["ir"], out["fp64"]["ir"]
+    errs = [rel_l2(ir32[r], ir64[r]) for r in range(ir64.shape[0])]
+    E32, E64 = out["fp32"]["E"], out["fp64"]["E"]
+    drift = np.abs(E32 - E64) / np.maximum(E64, 1e-300)
+    cells = 256 ** 3
+    print(json.dumps({
+        "metric": "precision study (config 3): FP32 bulk vs all-FP64", "steps": steps,
+        "value": cells * steps / (out["fp32"]["ms"] / 1e3) / 1e9, "unit": UNIT,
+        "fp64_gcell_s": cells * steps / (out["fp64"]["ms"] / 1e3) / 1e9,
+        "ir_rel_l2_fp32_vs_fp64": errs, "ir_rel_l2_max": max(errs),
+        "energy_fp64": E64.tolist(), "energy_rel_diff_fp32_vs_fp64": drift.tolist(),
+        "energy_rel_change_fp64": float(E64[-1] / E64[0] - 1.0),
+        "config": {"workload": "256^3 shoebox, 5 rigid obstacles, 6 ADE walls (2 real + 2 complex poles), "
+                               "20-cell cPML on one face, Gaussian pulse, 8 receivers"}}), flush=True)
+
+
 def main():
     args = parse()
     rank, world, local, pg = dist_setup(args.gpus)
     if args.impl == "reference":
         run_reference(args, rank)
         return
-    if world > 1:
-        os.environ["CUDA_VISIBLE_DEVICES"] = os.environ.get("CUDA_VISIBLE_DEVICES", str(local))
+    if args.config == "plain2d":
+        if rank == 0:
+            run_plain2d(args)
+        return
+    if args.config == "precision":
+        if rank == 0:
+            run_precision(args)
+        return
     room = args.room
     b = workload(room)
     room_cells = int(room[0]) * int(room[1]) * int(room[2])
     nsteps_total = args.warmup + args.steps
-    s = make_solver(b, args.precision, nsteps_total + 1)
+    s = make_solver(b, args.precision, nsteps_total + 1, device=local)
     info = s.info()
     s.run(args.warmup)
     barrier(pg)
@@ -258,7 +351,8 @@ def main():
     m = b["packed"]
     ne = args.e2e_steps
     t0 = time.perf_counter()
-    prm = params(h=b["h"], c=b["c"], rho=b["rho"], dt=b["dt"], pml=b["pml"], pml_cells=20, precision=args.precision)
+    prm = params(h=b["h"], c=b["c"], rho=b["rho"], dt=b["dt"], pml=b["pml"], pml_cells=20, precision=args.precision,
+                 device=local)
     e = Solver(prm)
     e.load_geometry(sc.S, sc.oid)
     e.set_materials(m["Rinf"], m["A"], m["zeta"], m["B"], m["Cc"], m["alpha"], m["beta"])
