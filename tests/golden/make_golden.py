@@ -75,8 +75,9 @@ CASES = {
 }
 
 
-def make_project(case, dest):
-    c = CASES[case]
+def make_project(case, dest, spec=None):
+    """Writes the reference project of CASES[case] (or of the given spec) into dest."""
+    c = spec if spec is not None else CASES[case]
     os.makedirs(os.path.join(dest, "config"), exist_ok=True)
     os.makedirs(os.path.join(dest, "input", "fit"), exist_ok=True)
     os.makedirs(os.path.join(dest, "output"), exist_ok=True)
@@ -104,7 +105,7 @@ def make_project(case, dest):
         f.write("2 2\n")
     x0, y0, z0 = [0.5 * L for L in c["room"]]
     cfg = [c["h"], c["t_max"], c["f_in"], c["temp"], c["cfl"], 8, *c["pml"], 0, 0, 0, c["src_opt"], c["glob_f"], 0,
-           x0, y0, z0, 60]
+           x0, y0, z0, c.get("frames", 60)]
     names = ["h", "t_max", "wave band", "temperature", "CFL", "ADE poles", "U_PML", "D_PML", "R_PML", "L_PML",
              "F_PML", "B_PML", "ISM order", "altitude", "rays", "source type", "source frequency", "source index",
              "slice x0", "slice y0", "slice z0", "frames"]
@@ -123,15 +124,41 @@ def make_project(case, dest):
         json.dump({"case": case, **{k: v for k, v in c.items()}}, f, indent=1)
 
 
-def run_reference(dest):
-    exe = os.path.join(ROOT, "oracle", "_ref", "fases3D")
-    if not os.path.exists(exe):
+REF_EXE = os.path.join(ROOT, "oracle", "_ref", "fases3D")
+
+
+def run_reference(dest, timeout=600):
+    if not os.path.exists(REF_EXE):
         raise SystemExit("reference solver not built: run oracle/build_ref.sh")
-    cmd = [exe, os.path.join(dest, "scene.obj"), os.path.join(dest, "config", "config.txt"),
+    cmd = [REF_EXE, os.path.join(dest, "scene.obj"), os.path.join(dest, "config", "config.txt"),
            os.path.join(dest, "src.txt"), os.path.join(dest, "rec.txt")]
     with open(os.path.join(dest, "reference_stdout.txt"), "w") as log:
-        r = subprocess.run(cmd, cwd=dest, stdout=log, stderr=subprocess.STDOUT, timeout=600)
+        r = subprocess.run(cmd, cwd=dest, stdout=log, stderr=subprocess.STDOUT, timeout=timeout)
     return r.returncode
+
+
+def run_reference_timed(dest, timeout=1800):
+    """Runs the reference solver on dest, stamping each stdout line (the solver line-buffers its
+    stdout) with time.perf_counter(); returns (returncode, [(t, line), ...]). The stamps of
+    "Will now start" and "Simulation time" bracket its time loop on the wall clock."""
+    import time
+    if not os.path.exists(REF_EXE):
+        raise SystemExit("reference solver not built: run oracle/build_ref.sh")
+    cmd = [REF_EXE, os.path.join(dest, "scene.obj"), os.path.join(dest, "config", "config.txt"),
+           os.path.join(dest, "src.txt"), os.path.join(dest, "rec.txt")]
+    stamped = []
+    t_end = time.perf_counter() + timeout
+    with subprocess.Popen(cmd, cwd=dest, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True,
+                          bufsize=1) as proc:
+        for line in proc.stdout:
+            stamped.append((time.perf_counter(), line))
+            if time.perf_counter() > t_end:
+                proc.kill()
+                break
+        rc = proc.wait(timeout=60)
+    with open(os.path.join(dest, "reference_stdout.txt"), "w") as log:
+        log.writelines(line for _, line in stamped)
+    return rc, stamped
 
 
 def prune(dest):
