@@ -42,9 +42,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=12000, help="length of the end-to-end job")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    ap.add_argument("--config", default="plain3d", choices=["plain3d", "plain2d", "precision"],
+    ap.add_argument("--config", default="plain3d", choices=["plain3d", "plain2d", "precision", "batched"],
                     help="plain3d: the headline room (default); plain2d: the 2D FP64 room; "
-                         "precision: FP32 bulk vs all-FP64 on a 256^3 room")
+                         "precision: FP32 bulk vs all-FP64 on a 256^3 room; batched: 64 sources in one "
+                         "192^3 room and 32 rooms in one graph")
     return ap.parse_args()
 
 
@@ -290,6 +291,97 @@ def run_precision(args):
                                "20-cell cPML on one face, Gaussian pulse, 8 receivers"}}), flush=True)
 
 
+def _batched_solver(b, precision, capacity, cells, u_s, sval, batch=1, members=None):
+    from fases_b200 import Solver, params
+    s = Solver(params(h=b["h"], c=b["c"], rho=b["rho"], dt=b["dt"], pml=b["pml"], pml_cells=20,
+                      precision=precision, batch=batch))
+    sc = b["scene"]
+    s.load_geometry(sc.S, sc.oid)
+    m = b["packed"]
+    s.set_materials(m["Rinf"], m["A"], m["zeta"], m["B"], m["Cc"], m["alpha"], m["beta"])
+    s.set_sources(cells, np.full(len(cells), sval), 0, u_s=u_s)
+    if members is not None:
+        s.set_source_members(members)
+    s.set_receivers(b["receivers"], capacity)
+    return s
+
+
+def run_batched(args):
+    """Config 4. (a) 64 seeded PCS source positions in one 192^3 room (6 ADE walls, 5 obstacles,
+    cPML face): one batched solver (64 field sets stepped by the same launches) against one
+    single-source solve of the same room, per-source throughput. (b) 32 rooms with edges drawn
+    from [64, 160] cells per axis (seeded), advanced as one group (one CUDA graph per 10 steps)
+    against the same rooms solved one after another."""
+    from fases_b200 import Group, source_waveform
+    from fases_b200 import materials as mats
+    from fases_b200 import scenes
+    steps_a = args.steps if args.steps != 300 else 200
+    nsrc = 64
+    b = scenes.benchmark_room(room_cells=(192, 192, 192), seed=4, n_obstacles=5, n_receivers=8)
+    b["packed"] = mats.pack(b["materials"])
+    rng = np.random.default_rng(44)
+    cand = scenes.free_cells(b["scene"], scenes.seeded_cells(rng, (192, 192, 192), 4 * nsrc, margin_cells=24), 6.0)
+    cells = np.asarray(cand[:nsrc], np.int32)
+    us, _, pk = source_waveform(0, 0.25 * b["f_cutoff"], b["f_cutoff"], b["dt"], steps_a + 40, b["h"], b["rho"])
+    room = 192 ** 3
+    single = _batched_solver(b, "fp32", steps_a + 20, cells[:1], us, 1.0 / pk)
+    single.run(20)
+    ms_single = single.run_timed(steps_a)
+    ir_single = single.ir()
+    single.close()
+    bat = _batched_solver(b, "fp32", steps_a + 20, cells, us, 1.0 / pk, batch=nsrc, members=np.arange(nsrc))
+    bat.run(20)
+    ms_batch = bat.run_timed(steps_a)
+    ir_batch = bat.ir()
+    bat.close()
+    per_src_single = room * steps_a / (ms_single / 1e3) / 1e9
+    per_src_batch = nsrc * room * steps_a / (ms_batch / 1e3) / 1e9
+    a_line = {
+        "metric": "batched sources (config 4a): Gcell-updates/s per source, summed over sources",
+        "value": per_src_batch, "unit": UNIT, "single_source_value": per_src_single,
+        "per_source_speedup": per_src_batch / per_src_single, "steps": steps_a,
+        "ms_per_step_batch": ms_batch / steps_a, "ms_per_step_single": ms_single / steps_a,
+        "member0_bitwise_equal_single": bool(np.array_equal(ir_batch[0], ir_single)),
+        "config": {"workload": "192^3 shoebox, 5 rigid obstacles, 6 ADE walls (2 real + 2 complex poles), "
+                               "20-cell cPML on one face, 64 seeded PCS source positions, 8 receivers, FP32",
+                   "sources": nsrc, "room_cells": room}}
+    print(json.dumps(a_line), flush=True)
+
+    steps_b = args.steps if args.steps != 300 else 5000
+    nroom = 32
+    rng = np.random.default_rng(45)
+    rooms = [tuple(int(x) for x in rng.integers(64, 161, size=3)) for _ in range(nroom)]
+    solvers, cells_b = [], 0
+    for q, r in enumerate(rooms):
+        bq = scenes.benchmark_room(room_cells=r, seed=100 + q, n_obstacles=2, n_receivers=4)
+        bq["packed"] = mats.pack(bq["materials"])
+        usq, _, pkq = source_waveform(0, 0.25 * bq["f_cutoff"], bq["f_cutoff"], bq["dt"], steps_b + 10, bq["h"],
+                                      bq["rho"])
+        src = np.asarray([bq["source_cell"]], np.int32)
+        solvers.append((_batched_solver(bq, "fp32", steps_b, src, usq, 1.0 / pkq),
+                        _batched_solver(bq, "fp32", steps_b, src, usq, 1.0 / pkq)))
+        cells_b += r[0] * r[1] * r[2]
+    ms_seq = 0.0
+    for solo, _ in solvers:
+        ms_seq += solo.run_timed(steps_b)
+    grp = Group([g for _, g in solvers])
+    ms_grp = grp.run_timed(steps_b)
+    same = all(np.array_equal(solo.ir(), g.ir()) for solo, g in solvers)
+    grp.close()
+    for solo, g in solvers:
+        solo.close()
+        g.close()
+    b_line = {
+        "metric": "grouped rooms (config 4b): Gcell-updates/s over all rooms",
+        "value": cells_b * steps_b / (ms_grp / 1e3) / 1e9, "unit": UNIT,
+        "sequential_value": cells_b * steps_b / (ms_seq / 1e3) / 1e9, "per_room_speedup": ms_seq / ms_grp,
+        "steps": steps_b, "ms_group": ms_grp, "ms_sequential": ms_seq, "members_bitwise_equal_solo": same,
+        "config": {"workload": "32 shoeboxes, edges uniform in [64, 160] cells (seed 45), 2 rigid obstacles, "
+                               "6 ADE walls, cPML face, PCS source, 4 receivers each, FP32",
+                   "rooms": rooms, "room_cells_total": cells_b}}
+    print(json.dumps(b_line), flush=True)
+
+
 def main():
     args = parse()
     rank, world, local, pg = dist_setup(args.gpus)
@@ -303,6 +395,10 @@ def main():
     if args.config == "precision":
         if rank == 0:
             run_precision(args)
+        return
+    if args.config == "batched":
+        if rank == 0:
+            run_batched(args)
         return
     room = args.room
     b = workload(room)

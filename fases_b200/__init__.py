@@ -6,6 +6,6 @@ SSP-RK3 stages, CFS-cPML and ADE pole-residue impedance boundaries on the immers
 hand-written CUDA behind the C ABI of include/fz.h (libfz.so).
 """
 from ._abi import FzError, lib  # noqa: F401
-from .solver import Solver, params, source_waveform  # noqa: F401
+from .solver import Group, Solver, params, source_waveform  # noqa: F401
 
-__all__ = ["Solver", "params", "source_waveform", "FzError", "lib"]
+__all__ = ["Solver", "Group", "params", "source_waveform", "FzError", "lib"]

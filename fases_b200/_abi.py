@@ -48,7 +48,7 @@ class FzParams(C.Structure):
         ("dt", C.c_double),
         ("tol_cells", C.c_double),
         ("two_d", C.c_int32),
-        ("reserved", C.c_int32),
+        ("batch", C.c_int32),
     ]
 
 
@@ -75,12 +75,18 @@ SIGNATURES = {
     "fz_load_geometry_raw": (C.c_int, [_P, _fp, _u8p, _i32, _i32, _i32]),
     "fz_set_materials": (C.c_int, [_P, _i32, _i32, _i32, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
     "fz_set_sources": (C.c_int, [_P, _i32, _ip, _dp, _i32, _dp, _dp, _i64]),
+    "fz_set_source_members": (C.c_int, [_P, _i32, _ip]),
     "fz_set_receivers": (C.c_int, [_P, _i32, _ip, _i64]),
     "fz_set_fields": (C.c_int, [_P, _dp, _dp, _dp, _dp]),
     "fz_run": (C.c_int, [_P, _i64]),
     "fz_run_timed": (C.c_int, [_P, _i64, _dp]),
     "fz_sync": (C.c_int, [_P, _i64]),
     "fz_steps_done": (C.c_int, [_P, _i64p]),
+    "fz_group_create": (C.c_int, [C.POINTER(_P), _i32, C.POINTER(_P)]),
+    "fz_group_run": (C.c_int, [_P, _i64]),
+    "fz_group_run_timed": (C.c_int, [_P, _i64, _dp]),
+    "fz_group_sync": (C.c_int, [_P, _i64]),
+    "fz_group_destroy": (None, [_P]),
     "fz_get_ir": (C.c_int, [_P, _fp, _i64]),
     "fz_get_ir64": (C.c_int, [_P, _dp, _i64]),
     "fz_get_vel": (C.c_int, [_P, _fp, _i64]),

@@ -110,12 +110,12 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
-// 3-D map over one device array (Sx x Ny x Nz elements of esz bytes) with bx x by x 1 boxes;
+// 3-D map over one device array (Sx x Ny x Nz*nb elements of esz bytes) with bx x by x 1 boxes;
 // reads outside the allocation fill with zeros.
 int make_map(fz_handle* h, CUtensorMap* map, void* base, size_t esz, CUtensorMapDataType type, int bx, int by) {
   EncodeTiledFn enc = encode_fn();
   if (!enc) return set_error(h, FZ_ECUDA, "cuTensorMapEncodeTiled not available from the driver");
-  const cuuint64_t dims[3] = {(cuuint64_t)h->Sx, (cuuint64_t)h->Ny, (cuuint64_t)h->Nz};
+  const cuuint64_t dims[3] = {(cuuint64_t)h->Sx, (cuuint64_t)h->Ny, (cuuint64_t)h->Nz * h->nb};
   const cuuint64_t strides[2] = {(cuuint64_t)h->Sx * esz, (cuuint64_t)h->plane * esz};
   const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
   const cuuint32_t estr[3] = {1, 1, 1};
@@ -178,9 +178,22 @@ int upload_pml(fz_handle* h) {
   const int n[3] = {h->Nx, h->Ny, h->Nz};
   typedef typename fz::Pair<R>::T P;
   const int64_t d2 = 2 * (int64_t)p.pml_cells;
-  const int64_t tile_n[3] = {d2 * h->Ny * h->Nz, (int64_t)h->Nx * d2 * h->Nz, (int64_t)h->Nx * h->Ny * d2};
+  const int64_t nb = h->nb;
+  const int64_t tile_n[3] = {d2 * h->Ny * h->Nz * nb, (int64_t)h->Nx * d2 * h->Nz * nb,
+                             (int64_t)h->Nx * h->Ny * d2 * nb};
   for (int a = 0; a < 3; a++) {
     auto t = pml_table<R>(n[a], lo[a], hi[a], p);
+    if (a == 2 && nb > 1) {
+      // batch members stack along z: one z table per member, its psi tiles offset by the member
+      const size_t n1 = t.size();
+      t.resize(n1 * (size_t)nb);
+      for (int64_t m = 1; m < nb; m++)
+        for (size_t q = 0; q < n1; q++) {
+          fz::PmlCoef<R> c = t[q];
+          if (c.tile >= 0) c.tile += (int32_t)(m * d2);
+          t[(size_t)m * n1 + q] = c;
+        }
+    }
     FZ_CUDA(h, cudaMalloc(&h->d_pml_coef[a], t.size() * sizeof(t[0])), "cudaMalloc(pml table)");
     FZ_CUDA(h, cudaMemcpy(h->d_pml_coef[a], t.data(), t.size() * sizeof(t[0]), cudaMemcpyHostToDevice),
             "cudaMemcpy(pml table)");
@@ -247,9 +260,21 @@ int build_band(fz_handle* h) {
         mat.push_back((int32_t)o - 1);
         h->band_cell_ref.push_back(rc);
       }
-  h->nB = (int64_t)cell.size();
+  h->nB1 = (int64_t)cell.size();
+  h->nB = h->nB1 * h->nb;
   h->band_mat = mat;
   if (h->nB == 0) return FZ_OK;
+  // batch members: the same band cells in every member's field set (and their own ADE states)
+  for (int m = 1; m < h->nb; m++)
+    for (int64_t b = 0; b < h->nB1; b++) {
+      cell.push_back(cell[(size_t)b] + (int64_t)m * h->ncell_dev);
+      corner.push_back(corner[(size_t)b] + (int64_t)m * h->ncell_dev);
+      for (int q = 0; q < 4; q++) {
+        geo.push_back(geo[(size_t)(4 * b + q)]);
+        nrm.push_back(nrm[(size_t)(4 * b + q)]);
+      }
+      mat.push_back(mat[(size_t)b]);
+    }
   std::vector<int4> rec((size_t)h->nB);
   for (size_t b = 0; b < rec.size(); b++) {
     const uint64_t c = (uint64_t)cell[b];
@@ -305,19 +330,25 @@ int finalize(fz_handle* h) {
     }
   }
   // sources
+  h->nsrc_dev = 0;
   if (h->nsrc > 0) {
     std::vector<int64_t> cells;
     std::vector<R> coef, freq;
     const double As = 6.0 * h->prm.h * h->prm.h;
     for (int s = 0; s < h->nsrc; s++) {
       const int i = h->src_ijk[3 * s], j = h->src_ijk[3 * s + 1], k = h->src_ijk[3 * s + 2];
-      const int64_t g = dev_index(h, i, j, k);
-      cells.push_back(g);
-      coef.push_back((R)(h->prm.dt * h->prm.c * h->prm.c * h->src_val[s] * h->prm.rho * As /
-                         (h->prm.h * h->prm.h * h->prm.h)));
-      freq.push_back((R)(h->src_freq.empty() ? 0.0 : h->src_freq[s]));
-      h->cls_host[g] |= fz::CLS_SOURCE;
+      const int mem = h->src_member.empty() ? -1 : h->src_member[s];
+      for (int m = 0; m < h->nb; m++) {
+        if (mem >= 0 && mem != m) continue;
+        const int64_t g = dev_index(h, i, j, k) + (int64_t)m * h->ncell_dev;
+        cells.push_back(g);
+        coef.push_back((R)(h->prm.dt * h->prm.c * h->prm.c * h->src_val[s] * h->prm.rho * As /
+                           (h->prm.h * h->prm.h * h->prm.h)));
+        freq.push_back((R)(h->src_freq.empty() ? 0.0 : h->src_freq[s]));
+        h->cls_host[g] |= fz::CLS_SOURCE;
+      }
     }
+    h->nsrc_dev = (int)cells.size();
     FZ_CUDA(h, cudaMalloc(&h->d_src_cell, cells.size() * 8), "cudaMalloc(src)");
     FZ_CUDA(h, cudaMalloc(&h->d_src_coef, coef.size() * sizeof(R)), "cudaMalloc(src)");
     FZ_CUDA(h, cudaMalloc(&h->d_src_freq, freq.size() * sizeof(R)), "cudaMalloc(src)");
@@ -335,11 +366,13 @@ int finalize(fz_handle* h) {
   // receivers
   if (h->nrec > 0) {
     std::vector<int64_t> cells;
-    for (int r = 0; r < h->nrec; r++)
-      cells.push_back(dev_index(h, h->rec_ijk[3 * r], h->rec_ijk[3 * r + 1], h->rec_ijk[3 * r + 2]));
+    for (int m = 0; m < h->nb; m++)  // traces [member][receiver][step]
+      for (int r = 0; r < h->nrec; r++)
+        cells.push_back(dev_index(h, h->rec_ijk[3 * r], h->rec_ijk[3 * r + 1], h->rec_ijk[3 * r + 2]) +
+                        (int64_t)m * h->ncell_dev);
     FZ_CUDA(h, cudaMalloc(&h->d_rec_cell, cells.size() * 8), "cudaMalloc(rec)");
     FZ_CUDA(h, cudaMemcpy(h->d_rec_cell, cells.data(), cells.size() * 8, cudaMemcpyHostToDevice), "rec H2D");
-    const size_t n = (size_t)h->nrec * (size_t)std::max<int64_t>(1, h->rec_cap);
+    const size_t n = (size_t)h->nrec * h->nb * (size_t)std::max<int64_t>(1, h->rec_cap);
     FZ_CUDA(h, cudaMalloc(&h->d_ir, n * 8), "cudaMalloc(ir)");
     FZ_CUDA(h, cudaMalloc(&h->d_vel, n * 3 * 8), "cudaMalloc(vel)");
     FZ_CUDA(h, cudaMemset(h->d_ir, 0, n * 8), "cudaMemset(ir)");
@@ -360,7 +393,7 @@ int finalize(fz_handle* h) {
   for (int nk = 1; nk <= std::max(1, nzi / 8); nk++) {
     const int chunk = (nzi + nk - 1) / nk;
     const int nk_eff = (nzi + chunk - 1) / chunk;
-    const int64_t items = (int64_t)ntx * nty * nk_eff;
+    const int64_t items = (int64_t)ntx * nty * nk_eff * h->nb;
     const int64_t waves = (items + slots - 1) / slots;
     const double eff = ((double)items / (double)(waves * slots)) * ((double)chunk / (chunk + 1.5));
     if (eff > best_eff + 1e-9) {
@@ -370,7 +403,8 @@ int finalize(fz_handle* h) {
   }
   h->kz_chunk = (nzi + best - 1) / best;
   int nkz = (nzi + h->kz_chunk - 1) / h->kz_chunk;
-  h->stage_grid = dim3((unsigned)ntx, (unsigned)nty, (unsigned)nkz);
+  h->zchunks = nkz;
+  h->stage_grid = dim3((unsigned)ntx, (unsigned)nty, (unsigned)(nkz * h->nb));
   h->finalized = true;
   return FZ_OK;
 }
@@ -392,6 +426,7 @@ fz::StageArgs<R> stage_args(fz_handle* h, int stage) {
   a.Nx = h->Nx; a.Ny = h->Ny; a.Nz = h->Nz;
   a.Sx = h->Sx; a.plane = h->plane;
   a.kz_chunk = h->kz_chunk;
+  a.zchunks = h->zchunks;
   const fz_params& p = h->prm;
   a.dt_h = (R)(p.dt / p.h);
   a.frc2 = (R)(0.5 * p.rho * p.c * p.c);
@@ -408,7 +443,7 @@ fz::StageArgs<R> stage_args(fz_handle* h, int stage) {
   a.psix = (P*)h->d_psi[0];
   a.psiy = (P*)h->d_psi[1];
   a.psiz = (P*)h->d_psi[2];
-  a.nsrc = h->nsrc;
+  a.nsrc = h->nsrc_dev;
   a.src_cell = h->d_src_cell;
   a.src_coef = (const R*)h->d_src_coef;
   a.src_freq = (const R*)h->d_src_freq;
@@ -508,7 +543,7 @@ cudaError_t enqueue_step(fz_handle* h) {
   {
     Timer t(h, 4);
     R* const* u1 = (R* const*)h->U[h->i1];
-    e = fz::launch_receivers<R>(u1[0], u1[1], u1[2], u1[3], h->d_rec_cell, h->nrec, h->d_ir, h->d_vel,
+    e = fz::launch_receivers<R>(u1[0], u1[1], u1[2], u1[3], h->d_rec_cell, h->nrec * h->nb, h->d_ir, h->d_vel,
                                 h->rec_cap, h->d_step, h->stream);
     if (e != cudaSuccess) return e;
   }
@@ -560,11 +595,12 @@ int load_geometry(fz_handle* h, const float* S, const uint8_t* oid, int Nx, int 
   h->Sx = ((int64_t)Nx + XOFF + 31) / 32 * 32;
   h->plane = h->Sx * Ny;
   h->ncell_dev = h->plane * Nz;
+  h->nb = std::max(1, h->prm.batch);
   if (h->Lx == 0) { h->Lx = Nx * h->prm.h; h->Ly = Ny * h->prm.h; h->Lz = Nz * h->prm.h; }
   const size_t N = (size_t)Nx * Ny * Nz;
   h->S_host.assign(S, S + N);
   h->oid_host.assign(oid, oid + N);
-  const size_t bytes = (size_t)h->ncell_dev * sizeof(R);
+  const size_t bytes = (size_t)h->ncell_dev * h->nb * sizeof(R);
   for (int s = 0; s < 3; s++)
     for (int f = 0; f < 4; f++) {
       FZ_CUDA(h, cudaMalloc(&h->U[s][f], bytes), "cudaMalloc(fields)");
@@ -582,6 +618,10 @@ int load_geometry(fz_handle* h, const float* S, const uint8_t* oid, int Nx, int 
           nup++;
         }
   h->n_update = nup;
+  // one copy of the class bytes per batch member, so that the stage kernels index them like the fields
+  h->cls_host.resize((size_t)h->ncell_dev * h->nb);
+  for (int m = 1; m < h->nb; m++)
+    std::copy(h->cls_host.begin(), h->cls_host.begin() + h->ncell_dev, h->cls_host.begin() + m * h->ncell_dev);
   FZ_CUDA(h, cudaMalloc(&h->d_cls, h->cls_host.size()), "cudaMalloc(cls)");
   FZ_CUDA(h, cudaMemcpy(h->d_cls, h->cls_host.data(), h->cls_host.size(), cudaMemcpyHostToDevice), "cls H2D");
   {
@@ -610,10 +650,13 @@ int get_fields(fz_handle* h, double* p, double* u, double* v, double* w) {
   double* outs[4] = {p, u, v, w};
   for (int f = 0; f < 4; f++) {
     if (!outs[f]) continue;
-    const R* src = (const R*)h->U[h->i0][f] + XOFF;
-    FZ_CUDA(h, cudaMemcpy2D(tmp.data(), rowb, src, (size_t)h->Sx * sizeof(R), rowb,
-                            (size_t)h->Ny * h->Nz, cudaMemcpyDeviceToHost), "fields D2H");
-    for (size_t c = 0; c < N; c++) outs[f][c] = (double)tmp[c];
+    for (int m = 0; m < h->nb; m++) {
+      const R* src = (const R*)h->U[h->i0][f] + XOFF + (size_t)m * h->ncell_dev;
+      FZ_CUDA(h, cudaMemcpy2D(tmp.data(), rowb, src, (size_t)h->Sx * sizeof(R), rowb,
+                              (size_t)h->Ny * h->Nz, cudaMemcpyDeviceToHost), "fields D2H");
+      double* o = outs[f] + (size_t)m * N;
+      for (size_t c = 0; c < N; c++) o[c] = (double)tmp[c];
+    }
   }
   return FZ_OK;
 }
@@ -625,14 +668,17 @@ int set_fields(fz_handle* h, const double* p, const double* u, const double* v, 
   std::vector<R> tmp(N);
   const double* ins[4] = {p, u, v, w};
   for (int f = 0; f < 4; f++) {
-    R* dst = (R*)h->U[h->i0][f] + XOFF;
     if (!ins[f]) {
-      FZ_CUDA(h, cudaMemset(h->U[h->i0][f], 0, (size_t)h->ncell_dev * sizeof(R)), "fields zero");
+      FZ_CUDA(h, cudaMemset(h->U[h->i0][f], 0, (size_t)h->ncell_dev * h->nb * sizeof(R)), "fields zero");
       continue;
     }
-    for (size_t c = 0; c < N; c++) tmp[c] = (R)ins[f][c];
-    FZ_CUDA(h, cudaMemcpy2D(dst, (size_t)h->Sx * sizeof(R), tmp.data(), rowb, rowb,
-                            (size_t)h->Ny * h->Nz, cudaMemcpyHostToDevice), "fields H2D");
+    for (int m = 0; m < h->nb; m++) {
+      R* dst = (R*)h->U[h->i0][f] + XOFF + (size_t)m * h->ncell_dev;
+      const double* in = ins[f] + (size_t)m * N;
+      for (size_t c = 0; c < N; c++) tmp[c] = (R)in[c];
+      FZ_CUDA(h, cudaMemcpy2D(dst, (size_t)h->Sx * sizeof(R), tmp.data(), rowb, rowb,
+                              (size_t)h->Ny * h->Nz, cudaMemcpyHostToDevice), "fields H2D");
+    }
   }
   return FZ_OK;
 }
@@ -642,7 +688,7 @@ int energy(fz_handle* h, double* E) {
   FZ_CUDA(h, cudaMemsetAsync(h->d_scratch, 0, sizeof(double), h->stream), "energy reset");
   R* const* u0 = (R* const*)h->U[h->i0];
   const double rc2 = h->prm.rho * h->prm.c * h->prm.c;
-  FZ_CUDA(h, fz::launch_energy<R>(u0[0], u0[1], u0[2], u0[3], h->ncell_dev, 1.0 / rc2, h->prm.rho,
+  FZ_CUDA(h, fz::launch_energy<R>(u0[0], u0[1], u0[2], u0[3], h->ncell_dev * h->nb, 1.0 / rc2, h->prm.rho,
                                   h->d_scratch, h->nsm, h->stream), "energy launch");
   int rc = fz_sync(h, 0);
   if (rc != FZ_OK) return rc;
@@ -653,6 +699,14 @@ int energy(fz_handle* h, double* E) {
 bool check_handle(fz_handle* h) { return h != nullptr; }
 
 }  // namespace
+
+namespace fzi {
+int prepare(fz_handle* h) {
+  cudaSetDevice(h->device);
+  return h->fp64 ? finalize<double>(h) : finalize<float>(h);
+}
+cudaError_t enqueue(fz_handle* h) { return h->fp64 ? enqueue_step<double>(h) : enqueue_step<float>(h); }
+}  // namespace fzi
 
 // ==========================================================================================
 // C ABI
@@ -681,6 +735,8 @@ int fz_create(const fz_params* p, fz_handle** out) {
   *out = nullptr;
   if (p->abi_version != FZ_ABI_VERSION)
     return fzi::set_global_error(FZ_EINVAL, "fz_create: abi_version mismatch");
+  if (p->batch < 0 || p->batch > 4096)
+    return fzi::set_global_error(FZ_EINVAL, "fz_create: batch must be in [0, 4096]");
   if (p->two_d && (p->pml[0] || p->pml[1]))
     return fzi::set_global_error(FZ_EINVAL, "fz_create: a planar (two_d) solve has no z faces: U_PML and D_PML must be 0");
   if (!(p->h > 0) || !(p->c > 0) || !(p->rho > 0) || !(p->dt > 0) || p->pml_cells < 1 ||
@@ -801,8 +857,22 @@ int fz_set_sources(fz_handle* h, int32_t n, const int32_t* cell_ijk, const doubl
   h->src_freq.assign((size_t)n, 0.0);
   if (freq) h->src_freq.assign(freq, freq + n);
   h->src_opt = src_opt;
+  h->src_member.clear();  // every source in every batch member until fz_set_source_members
   h->u_s.clear();
   if (u_s && n_us > 0) h->u_s.assign(u_s, u_s + n_us);
+  return FZ_OK;
+}
+
+int fz_set_source_members(fz_handle* h, int32_t n, const int32_t* member) {
+  if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  if (h->finalized) return set_error(h, FZ_ESTATE, "fz_set_source_members after the first fz_run");
+  if (n != h->nsrc || (n > 0 && !member))
+    return set_error(h, FZ_EINVAL, "fz_set_source_members: need one member index per source of fz_set_sources");
+  const int nb = std::max(1, h->prm.batch);
+  for (int s = 0; s < n; s++)
+    if (member[s] < -1 || member[s] >= nb)
+      return set_error(h, FZ_EINVAL, "fz_set_source_members: member index outside [-1, batch)");
+  h->src_member.assign(member, member + n);
   return FZ_OK;
 }
 
@@ -907,12 +977,13 @@ static int get_samples(fz_handle* h, double* out64, float* out32, int64_t cap, b
   FZ_CUDA(h, cudaMemcpy(&n, h->d_step, sizeof(int64_t), cudaMemcpyDeviceToHost), "step D2H");
   n = std::min(n, h->rec_cap);
   const int comp = vel ? 3 : 1;
-  const int64_t need = (int64_t)h->nrec * n * comp;
+  const int rows = h->nrec * h->nb;  // [member][receiver]
+  const int64_t need = (int64_t)rows * n * comp;
   if (cap < need) return set_error(h, FZ_EINVAL, "output buffer too small: need " + std::to_string(need));
   if (need == 0) return FZ_OK;
-  std::vector<double> tmp((size_t)h->nrec * h->rec_cap * comp);
+  std::vector<double> tmp((size_t)rows * h->rec_cap * comp);
   FZ_CUDA(h, cudaMemcpy(tmp.data(), vel ? h->d_vel : h->d_ir, tmp.size() * 8, cudaMemcpyDeviceToHost), "IR D2H");
-  for (int r = 0; r < h->nrec; r++)
+  for (int r = 0; r < rows; r++)
     for (int64_t t = 0; t < n * comp; t++) {
       const double x = tmp[(size_t)r * h->rec_cap * comp + t];
       const size_t o = (size_t)r * n * comp + t;
@@ -944,7 +1015,7 @@ int fz_energy(fz_handle* h, double* E) {
 int fz_info(fz_handle* h, int32_t* dims, int64_t* n_band, int64_t* n_update) {
   if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
   if (dims) { dims[0] = h->Nx; dims[1] = h->Ny; dims[2] = h->Nz; }
-  if (n_band) *n_band = h->nB;
+  if (n_band) *n_band = h->nB1;  // band cells of one batch member
   if (n_update) *n_update = h->n_update;
   return FZ_OK;
 }

@@ -69,6 +69,7 @@ struct StageArgs {
   int64_t Sx;     // row pitch (elements)
   int64_t plane;  // Sx * Ny
   int32_t kz_chunk;
+  int32_t zchunks;  // z chunks per batch member: blockIdx.z = member * zchunks + chunk
   R dt_h;   // dt / h
   R frc2;   // 0.5 * rho * c^2
   R firho;  // 0.5 / rho

@@ -30,6 +30,8 @@ struct fz_handle {
   std::vector<float> S_host;
   std::vector<uint8_t> oid_host;
   int64_t n_update = 0;
+  // batch members: independent field sets stacked along z, member m at offset m * ncell_dev
+  int nb = 1;
 
   // device fields: U[set][field], set 0..2, field p,u,v,w
   void* U[3][4] = {{nullptr}};
@@ -43,7 +45,8 @@ struct fz_handle {
   void* d_psi[3] = {nullptr, nullptr, nullptr};
 
   // immersed band
-  int64_t nB = 0;
+  int64_t nB = 0;   // band records of all members (nB1 * nb)
+  int64_t nB1 = 0;  // band cells of one member
   std::vector<int64_t> band_cell_ref;  // reference-layout cell index (for the material check)
   std::vector<int32_t> band_mat;
   int4* d_brec = nullptr;  // cell index (lo, hi), corner - cell, material
@@ -63,6 +66,8 @@ struct fz_handle {
   std::vector<int32_t> src_ijk;
   std::vector<double> src_val, src_freq, u_s;
   int src_opt = 0;
+  std::vector<int32_t> src_member;  // per source: member index, -1 = every member
+  int nsrc_dev = 0;                 // device source records (sources x their members)
   int64_t* d_src_cell = nullptr;
   void* d_src_coef = nullptr;
   void* d_src_freq = nullptr;
@@ -91,6 +96,7 @@ struct fz_handle {
   int64_t steps_enqueued = 0;
   bool finalized = false;
   int kz_chunk = 0;
+  int zchunks = 1;  // z chunks per member
   dim3 stage_grid;
 
   // graphs, keyed by buffer parity
@@ -111,4 +117,8 @@ namespace fzi {
 int set_error(fz_handle* h, int code, const std::string& msg);
 int set_global_error(int code, const std::string& msg);
 int cuda_fail(fz_handle* h, cudaError_t e, const char* what);
+// finalises the handle's setup (materials, sources, receivers, launch geometry); idempotent
+int prepare(fz_handle* h);
+// enqueues one time step on the handle's stream (or into the capture the stream takes part in)
+cudaError_t enqueue(fz_handle* h);
 }  // namespace fzi

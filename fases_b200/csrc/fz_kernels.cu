@@ -246,8 +246,11 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
   const int lt = ty * TX + tx;
   const int i0 = GHOST + blockIdx.x * TX, j0 = GHOST + blockIdx.y * TY;
   const int i = i0 + tx, j = j0 + ty;
-  const int kb = GHOST + blockIdx.z * A.kz_chunk;
-  const int ke = min(kb + A.kz_chunk, A.Nz - GHOST);
+  // batch members are stacked along z (member m owns planes [m Nz, (m+1) Nz)); the cPML z table,
+  // the psi tiles and the class bytes are laid out per member the same way
+  const int member = blockIdx.z / A.zchunks;
+  const int kb = GHOST + (blockIdx.z - member * A.zchunks) * A.kz_chunk + member * A.Nz;
+  const int ke = min(kb + A.kz_chunk, (member + 1) * A.Nz - GHOST);
   if (kb >= ke) return;
   const int nplanes = ke - kb;
   const int64_t Sx = A.Sx, plane = A.plane;

@@ -215,8 +215,10 @@ int fz_write_outputs(fz_handle* h, const char* output_dir, int32_t src_idx, cons
   if (rc != FZ_OK) return rc;
   n = std::min(n, h->rec_cap);
   const std::string dir(output_dir);
-  std::vector<float> ir((size_t)h->nrec * n), vel((size_t)h->nrec * n * 3);
-  if (h->nrec > 0 && n > 0) {
+  // batch member m writes the traces of source index src_idx + m
+  const int rows = h->nrec * h->nb;
+  std::vector<float> ir((size_t)rows * n), vel((size_t)rows * n * 3);
+  if (rows > 0 && n > 0) {
     rc = fz_get_ir(h, ir.data(), (int64_t)ir.size());
     if (rc != FZ_OK) return rc;
     rc = fz_get_vel(h, vel.data(), (int64_t)vel.size());
@@ -224,9 +226,10 @@ int fz_write_outputs(fz_handle* h, const char* output_dir, int32_t src_idx, cons
   }
   // IR<rec>_<src>.bin: float32 p per step; VEL<rec>_<src>.bin: float32 (u,v,w) per step
   // (main3D.cu:1251-1256, 1403-1412)
-  for (int r = 0; r < h->nrec; r++) {
-    const std::string f1 = dir + "/IR" + std::to_string(r) + "_" + std::to_string(src_idx) + ".bin";
-    const std::string f2 = dir + "/VEL" + std::to_string(r) + "_" + std::to_string(src_idx) + ".bin";
+  for (int r = 0; r < rows; r++) {
+    const std::string tag = std::to_string(r % h->nrec) + "_" + std::to_string(src_idx + r / h->nrec) + ".bin";
+    const std::string f1 = dir + "/IR" + tag;
+    const std::string f2 = dir + "/VEL" + tag;
     FILE* a = std::fopen(f1.c_str(), "wb");
     FILE* b = std::fopen(f2.c_str(), "wb");
     if (!a || !b) {

@@ -19,9 +19,11 @@ def _dptr(a):
 
 
 def params(h=0.02, c=None, rho=None, dt=None, cfl=0.5, pml=(0, 0, 0, 0, 0, 0), pml_cells=20,
-           precision="fp32", device=0, tol_cells=3.0, two_d=False):
+           precision="fp32", device=0, tol_cells=3.0, two_d=False, batch=1):
     """Solver parameters. c/rho default to the reference's 20 degC air (main3D.cu:450-456);
-    dt = cfl*h/c (main3D.cu:729-730). pml = (U, D, R, L, F, B) face keys (main3D.cu:155-160)."""
+    dt = cfl*h/c (main3D.cu:729-730). pml = (U, D, R, L, F, B) face keys (main3D.cu:155-160).
+    batch > 1 steps that many independent field sets (one per source position) over the same
+    room in the same launches."""
     p = FzParams()
     check(lib().fz_params_init(C.byref(p)))
     p.precision = _abi.FZ_FP64 if precision == "fp64" else _abi.FZ_FP32
@@ -37,6 +39,7 @@ def params(h=0.02, c=None, rho=None, dt=None, cfl=0.5, pml=(0, 0, 0, 0, 0, 0), p
     p.dt = float(dt) if dt is not None else float(cfl) * p.h / p.c
     p.tol_cells = float(tol_cells)
     p.two_d = 1 if two_d else 0
+    p.batch = int(batch)
     return p
 
 
@@ -52,6 +55,7 @@ class Solver:
             h = C.c_void_p()
             check(lib().fz_create(C.byref(prm), C.byref(h)))
             self._h = h
+        self.batch = max(1, int(prm.batch)) if prm is not None else 1
         self._nrec = 0
         self._cap = 0
 
@@ -112,6 +116,12 @@ class Solver:
                                        _dptr(sval), int(src_opt), _dptr(fr), _dptr(us),
                                        0 if us is None else us.size))
 
+    def set_source_members(self, member):
+        """Batched solves: the batch member (0 .. batch-1, or -1 for all) of each source of the last
+        set_sources call."""
+        member = np.ascontiguousarray(member, dtype=np.int32).reshape(-1)
+        self._chk(lib().fz_set_source_members(self._h, member.size, member.ctypes.data_as(C.POINTER(C.c_int32))))
+
     def set_receivers(self, cells, capacity_steps):
         cells = np.ascontiguousarray(cells, dtype=np.int32).reshape(-1, 3)
         self._chk(lib().fz_set_receivers(self._h, cells.shape[0], cells.ctypes.data_as(C.POINTER(C.c_int32)),
@@ -120,6 +130,12 @@ class Solver:
         self._cap = int(capacity_steps)
 
     def set_fields(self, p=None, u=None, v=None, w=None):
+        """Arrays of shape [Nz, Ny, Nx] (or [batch, Nz, Ny, Nx] for batched solves)."""
+        if self.batch > 1:
+            n = self.batch * int(np.prod(self.shape))
+            for a in (p, u, v, w):
+                if a is not None and np.size(a) != n:
+                    raise ValueError("batched set_fields needs arrays of shape [batch, Nz, Ny, Nx]")
         arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (p, u, v, w)]
         self._chk(lib().fz_set_fields(self._h, *[_dptr(a) for a in arrs]))
 
@@ -147,25 +163,30 @@ class Solver:
     def _nsamples(self):
         return min(self.steps_done(), self._cap)
 
+    def _lead(self):
+        return (self.batch,) if self.batch > 1 else ()
+
     def ir(self, fp64=True):
+        """Receiver traces [n_rec, n_steps] ([batch, n_rec, n_steps] for batched solves)."""
         n = self._nsamples()
+        shape = self._lead() + (self._nrec, n)
         if fp64:
-            out = np.zeros((self._nrec, n), np.float64)
+            out = np.zeros(shape, np.float64)
             self._chk(lib().fz_get_ir64(self._h, out.ctypes.data_as(C.POINTER(C.c_double)), out.size))
         else:
-            out = np.zeros((self._nrec, n), np.float32)
+            out = np.zeros(shape, np.float32)
             self._chk(lib().fz_get_ir(self._h, out.ctypes.data_as(C.POINTER(C.c_float)), out.size))
         return out
 
     def vel(self):
         n = self._nsamples()
-        out = np.zeros((self._nrec, n, 3), np.float32)
+        out = np.zeros(self._lead() + (self._nrec, n, 3), np.float32)
         self._chk(lib().fz_get_vel(self._h, out.ctypes.data_as(C.POINTER(C.c_float)), out.size))
         return out
 
     def fields(self):
-        Nz, Ny, Nx = self.shape
-        out = [np.zeros((Nz, Ny, Nx), np.float64) for _ in range(4)]
+        """(p, u, v, w), each [Nz, Ny, Nx] ([batch, Nz, Ny, Nx] for batched solves)."""
+        out = [np.zeros(self._lead() + tuple(self.shape), np.float64) for _ in range(4)]
         self._chk(lib().fz_get_fields(self._h, *[_dptr(a) for a in out]))
         return out
 
@@ -212,6 +233,50 @@ class Solver:
         s.shape = tuple(reversed(info["dims"]))
         s._nrec = _count_rec(rec)
         return s, nt.value
+
+
+class Group:
+    """Several solvers (rooms) on one device advanced together: every run of 10 steps is one CUDA
+    graph whose parallel branches are the members. The members stay usable alone and must outlive
+    the group."""
+
+    def __init__(self, solvers):
+        self.solvers = list(solvers)
+        arr = (C.c_void_p * len(self.solvers))(*[s._h.value if isinstance(s._h, C.c_void_p) else s._h
+                                                 for s in self.solvers])
+        g = C.c_void_p()
+        check(lib().fz_group_create(arr, len(self.solvers), C.byref(g)))
+        self._g = g
+
+    def run(self, nsteps, sync=True, timeout_ms=0):
+        check(lib().fz_group_run(self._g, int(nsteps)))
+        if sync:
+            self.sync(timeout_ms)
+
+    def run_timed(self, nsteps):
+        ms = C.c_double()
+        check(lib().fz_group_run_timed(self._g, int(nsteps), C.byref(ms)))
+        return ms.value
+
+    def sync(self, timeout_ms=0):
+        check(lib().fz_group_sync(self._g, int(timeout_ms)))
+
+    def close(self):
+        if self._g:
+            lib().fz_group_destroy(self._g)
+            self._g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 def _count_rec(path):

@@ -74,7 +74,13 @@ typedef struct fz_params {
   int32_t two_d;       /* 1: planar solve -- the grid has exactly one updated z-plane (Nz = 7 with
                           the ghost cells), no z fluxes and no z cPML; the 3D scheme restricted to
                           2D (config 1 of the benchmarks). 0: 3D. */
-  int32_t reserved;
+  int32_t batch;       /* independent field sets stepped together (0 or 1: one). Members share the
+                          geometry, materials, cPML faces and receiver cells; each has its own
+                          fields, ADE and cPML states and its own sources (fz_set_source_members).
+                          Replaces the one-process-per-source runs of the auralization mode
+                          (main3D.cu:1278, driven per source by common/gui.py). Host-side arrays of
+                          fz_set_fields / fz_get_fields hold batch grids one after another; receiver
+                          traces are [batch][n_rec][n_steps]. */
 } fz_params;
 
 /* Fills p with the reference defaults: FP32, device 0, 20 PML cells, no PML faces, h = 0.02,
@@ -109,6 +115,11 @@ int fz_set_materials(fz_handle* h, int32_t nMat, int32_t K, int32_t L, const dou
 int fz_set_sources(fz_handle* h, int32_t n, const int32_t* cell_ijk, const double* sval,
                    int32_t src_opt, const double* freq, const double* u_s, int64_t n_us);
 
+/* Batched solves (fz_params.batch > 1): member[n] assigns each source of the last fz_set_sources
+ * call to one member (0 .. batch-1), or to every member (-1, the default). No counterpart in the
+ * reference, which runs one process per source position. */
+int fz_set_source_members(fz_handle* h, int32_t n, const int32_t* member);
+
 /* Receivers at grid cells cell_ijk[3*n] ((int)(x/h)+3, main3D.cu:938-940). Samples p and
  * (u,v,w) after every step into a device buffer of capacity_steps samples per receiver
  * (replaces the per-step cudaMemcpy at main3D.cu:1399-1414). */
@@ -134,6 +145,20 @@ int fz_sync(fz_handle* h, int64_t timeout_ms);
 
 /* Steps completed so far (after fz_sync). */
 int fz_steps_done(fz_handle* h, int64_t* n);
+
+/* Groups: several handles (rooms) on one device advanced together. fz_group_run enqueues nsteps
+ * steps of every member; each run of 10 steps is one CUDA graph whose parallel branches are the
+ * members, so small rooms run side by side instead of one after another. Members keep their own
+ * state and stay usable alone (fz_get_ir, fz_sync, fz_run); they must all be on one device, must
+ * outlive the group, and are finalised (materials, sources, receivers fixed) by fz_group_create.
+ * No counterpart in the reference (one process per room). */
+typedef struct fz_group fz_group;
+int fz_group_create(fz_handle* const* members, int32_t n, fz_group** out);
+int fz_group_run(fz_group* g, int64_t nsteps);
+/* fz_group_run bracketed by CUDA events on the group's stream, then a bounded wait. */
+int fz_group_run_timed(fz_group* g, int64_t nsteps, double* ms);
+int fz_group_sync(fz_group* g, int64_t timeout_ms);
+void fz_group_destroy(fz_group* g);
 
 /* Receiver traces [n_rec][n_steps] (float32, as IR<r>_<s>.bin, main3D.cu:1403-1404) and
  * [n_rec][n_steps][3] velocities (as VEL<r>_<s>.bin, main3D.cu:1408-1412). cap = elements. */

@@ -1,0 +1,106 @@
+"""Batched solves (several source positions over one room in the same launches) and groups of
+rooms advanced as one CUDA graph: every member must reproduce, bit for bit, the solve it stands
+for when run alone, and the FP64 members must match the oracle run with their own source."""
+import numpy as np
+import pytest
+
+from tests.helpers import rel_l2, run_oracle, small_room
+
+SOURCES = np.array([[6, 6, 12], [18, 14, 5], [12, 17, 9]], np.int32)
+
+
+def _solver(cfg, precision, batch=1, src_rows=None, members=None, steps=None, p0=None):
+    from fases_b200 import Solver, params
+    steps = cfg["steps"] if steps is None else steps
+    s = Solver(params(h=cfg["h"], c=cfg["c"], rho=cfg["rho"], dt=cfg["dt"], pml=cfg["pml"],
+                      pml_cells=cfg["pml_cells"], precision=precision, batch=batch))
+    s.load_geometry(cfg["scene"].S, cfg["scene"].oid)
+    m = cfg["materials"]
+    s.set_materials(m["Rinf"], m["A"], m["zeta"], m["B"], m["Cc"], m["alpha"], m["beta"])
+    rows = SOURCES if src_rows is None else src_rows
+    s.set_sources(rows, np.full(len(rows), cfg["sval"][0]), cfg["src_opt"], u_s=cfg["u_s"])
+    if members is not None:
+        s.set_source_members(members)
+    s.set_receivers(cfg["recs"], steps)
+    if p0 is not None:
+        s.set_fields(p=p0)
+    return s
+
+
+def test_batch_parameter_is_validated():
+    import ctypes
+
+    from fases_b200 import _abi, params
+    p = params(batch=-2)
+    h = ctypes.c_void_p()
+    assert _abi.lib().fz_create(ctypes.byref(p), ctypes.byref(h)) == _abi.FZ_EINVAL
+    assert "batch" in _abi.last_error()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_batched_members_equal_single_source_runs(precision):
+    cfg = small_room(seed=11, pml=(1, 0, 1, 0, 0, 1), steps=37, pulse=False)
+    nb = len(SOURCES)
+    b = _solver(cfg, precision, batch=nb, members=np.arange(nb))
+    b.run(cfg["steps"])
+    ir_b = b.ir()
+    f_b = b.fields()
+    assert ir_b.shape == (nb, len(cfg["recs"]), cfg["steps"])
+    for m in range(nb):
+        s = _solver(cfg, precision, src_rows=SOURCES[m:m + 1])
+        s.run(cfg["steps"])
+        assert np.array_equal(s.ir(), ir_b[m]), (precision, m)
+        for a, fb in zip(s.fields(), f_b):
+            assert np.array_equal(a, fb[m]), (precision, m)
+        s.close()
+    if precision == "fp64":
+        for m in range(nb):
+            c = dict(cfg, src=SOURCES[m:m + 1])
+            ir_o, _ = run_oracle(c).ir()
+            for r in range(ir_o.shape[0]):
+                assert rel_l2(ir_b[m, r], ir_o[r]) < 1e-10, (m, r)
+    b.close()
+
+
+@pytest.mark.gpu
+def test_batched_shared_source_and_initial_fields():
+    """Sources with member -1 act in every member; initial fields are set per member."""
+    cfg = small_room(seed=12, steps=24)
+    nb = 2
+    rng = np.random.default_rng(3)
+    p0 = np.stack([cfg["p0"], cfg["p0"] * rng.uniform(0.5, 1.5)])
+    b = _solver(cfg, "fp32", batch=nb, src_rows=SOURCES[:1], p0=p0)
+    b.run(cfg["steps"])
+    ir_b = b.ir()
+    for m in range(nb):
+        s = _solver(cfg, "fp32", src_rows=SOURCES[:1], p0=p0[m])
+        s.run(cfg["steps"])
+        assert np.array_equal(s.ir(), ir_b[m]), m
+        s.close()
+    b.close()
+
+
+@pytest.mark.gpu
+def test_group_members_equal_solo_runs():
+    from fases_b200 import Group
+    rooms = [(26, 22, 18), (30, 20, 16), (20, 24, 22)]
+    steps = 23  # two graphs of 10 steps plus 3 single steps
+    cfgs = [small_room(seed=20 + q, room=r, steps=steps) for q, r in enumerate(rooms)]
+    solos = []
+    for c in cfgs:
+        s = _solver(c, "fp32", src_rows=SOURCES[:1], p0=c["p0"])
+        s.run(steps)
+        solos.append(s.ir())
+        s.close()
+    members = [_solver(c, "fp32", src_rows=SOURCES[:1], p0=c["p0"]) for c in cfgs]
+    with Group(members) as g:
+        g.run(steps)
+        for s, ref in zip(members, solos):
+            assert s.steps_done() == steps
+            assert np.array_equal(s.ir(), ref)
+        # a member stays usable alone after group runs
+        members[1].run(3)
+        assert members[1].steps_done() == steps + 3
+    for s in members:
+        s.close()
