@@ -52,6 +52,10 @@ class FzParams(C.Structure):
     ]
 
 
+# int (*fz_progress_fn)(int64_t done, int64_t total, void* user)
+PROGRESS_FN = C.CFUNCTYPE(C.c_int, C.c_int64, C.c_int64, C.c_void_p)
+
+
 class FzError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"{ERROR_NAMES.get(code, code)}: {msg}")
@@ -80,6 +84,7 @@ SIGNATURES = {
     "fz_set_fields": (C.c_int, [_P, _dp, _dp, _dp, _dp]),
     "fz_run": (C.c_int, [_P, _i64]),
     "fz_run_timed": (C.c_int, [_P, _i64, _dp]),
+    "fz_run_progress": (C.c_int, [_P, _i64, _i32, C.c_void_p, C.c_void_p]),
     "fz_sync": (C.c_int, [_P, _i64]),
     "fz_steps_done": (C.c_int, [_P, _i64p]),
     "fz_group_create": (C.c_int, [C.POINTER(_P), _i32, C.POINTER(_P)]),

@@ -910,6 +910,23 @@ int fz_run(fz_handle* h, int64_t nsteps) {
   return h->fp64 ? run_steps<double>(h, nsteps) : run_steps<float>(h, nsteps);
 }
 
+int fz_run_progress(fz_handle* h, int64_t nsteps, int32_t every_percent, fz_progress_fn cb, void* user) {
+  if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  if (nsteps < 0 || every_percent < 1 || every_percent > 100)
+    return set_error(h, FZ_EINVAL, "fz_run_progress: nsteps >= 0 and every_percent in [1, 100]");
+  const int64_t slice = std::max<int64_t>(1, nsteps * every_percent / 100);
+  int64_t done = 0;
+  while (done < nsteps) {
+    const int64_t n = std::min(slice, nsteps - done);
+    int rc = fz_run(h, n);
+    if (rc == FZ_OK) rc = fz_sync(h, 0);
+    if (rc != FZ_OK) return rc;
+    done += n;
+    if (cb && cb(done, nsteps, user) != 0) break;
+  }
+  return FZ_OK;
+}
+
 int fz_run_timed(fz_handle* h, int64_t nsteps, double* ms) {
   if (!check_handle(h) || !ms) return fzi::set_global_error(FZ_EINVAL, "NULL argument");
   cudaSetDevice(h->device);

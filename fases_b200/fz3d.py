@@ -47,13 +47,7 @@ def main(argv=None):
     s, nt = Solver.from_project(scene, config, src, rec, precision=precision)
     print(f"[OK] Will now start {nt} iterations", flush=True)
     t0 = time.perf_counter()
-    step = max(1, nt // 20)
-    done = 0
-    while done < nt:
-        n = min(step, nt - done)
-        s.run(n)
-        done += n
-        print("%d%%" % int(100.0 * done / nt + 0.5), flush=True)
+    s.run_progress(nt, lambda done, total: print("%d%%" % int(100.0 * done / total + 0.5), flush=True), 5)
     print("[OK] Simulation time: %f min" % ((time.perf_counter() - t0) / 60.0), flush=True)
     out = _project_output_dir(config)
     s.write_outputs(out, _src_index(config), os.path.abspath(scene))

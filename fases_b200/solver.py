@@ -145,6 +145,14 @@ class Solver:
         if sync:
             self.sync(timeout_ms)
 
+    def run_progress(self, nsteps, callback, every_percent=5):
+        """Runs nsteps in slices of every_percent %, calling callback(done, total) after each slice
+        (the reference's "NN%" protocol); a truthy return value stops the run."""
+        def _cb(done, total, _user):
+            return 1 if callback(done, total) else 0
+        fn = _abi.PROGRESS_FN(_cb)
+        self._chk(lib().fz_run_progress(self._h, int(nsteps), int(every_percent), C.cast(fn, C.c_void_p), None))
+
     def run_timed(self, nsteps):
         """Runs nsteps and returns their device time in ms (CUDA events on the solver's stream)."""
         ms = C.c_double()

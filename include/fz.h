@@ -140,6 +140,13 @@ int fz_run(fz_handle* h, int64_t nsteps);
  * the device time of the nsteps steps. */
 int fz_run_timed(fz_handle* h, int64_t nsteps, double* ms);
 
+/* Progress protocol: fz_run in slices of every_percent % of nsteps (the reference prints "NN%"
+ * every 5 %, functions3D.cuh:1431-1439, parsed by common/gui.py:6713), a bounded wait after each
+ * slice, then cb(steps_done_in_this_call, nsteps, user) on the calling thread (cb may be NULL).
+ * A nonzero return from cb stops the run after that slice (returns FZ_OK). */
+typedef int (*fz_progress_fn)(int64_t done, int64_t total, void* user);
+int fz_run_progress(fz_handle* h, int64_t nsteps, int32_t every_percent, fz_progress_fn cb, void* user);
+
 /* Bounded wait for all enqueued work (timeout_ms <= 0: 600000 ms). */
 int fz_sync(fz_handle* h, int64_t timeout_ms);
 

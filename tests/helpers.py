@@ -40,7 +40,7 @@ def small_room(seed=0, room=(26, 22, 18), pml=(0, 0, 1, 0, 0, 0), pml_cells=6, o
     return out
 
 
-def run_gpu(cfg, precision, steps=None, graph=True):
+def run_gpu(cfg, precision, steps=None, graph=True, run=True):
     from fases_b200 import Solver, params
     steps = cfg["steps"] if steps is None else steps
     prm = params(h=cfg["h"], c=cfg["c"], rho=cfg["rho"], dt=cfg["dt"], pml=cfg["pml"],
@@ -56,7 +56,8 @@ def run_gpu(cfg, precision, steps=None, graph=True):
         s.set_fields(p=cfg["p0"])
     if not graph:
         s.profile(True)
-    s.run(steps)
+    if run:
+        s.run(steps)
     return s
 
 
