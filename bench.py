@@ -42,10 +42,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=12000, help="length of the end-to-end job")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    ap.add_argument("--config", default="plain3d", choices=["plain3d", "plain2d", "precision", "batched"],
+    ap.add_argument("--config", default="plain3d", choices=["plain3d", "plain2d", "precision", "batched", "adjoint"],
                     help="plain3d: the headline room (default); plain2d: the 2D FP64 room; "
                          "precision: FP32 bulk vs all-FP64 on a 256^3 room; batched: 64 sources in one "
-                         "192^3 room and 32 rooms in one graph")
+                         "192^3 room and 32 rooms in one graph; adjoint: misfit gradient on a 256^3 room")
     return ap.parse_args()
 
 
@@ -382,6 +382,45 @@ def run_batched(args):
     print(json.dumps(b_line), flush=True)
 
 
+def run_adjoint(args):
+    """Config 5: 256^3 room with the config-2 material model; misfit J = sum_r ||IR_r(theta) -
+    IR_r(theta_true)||^2 over 8 receivers after 8000 FP32 steps (--steps overrides); gradient with
+    respect to every ADE coefficient by the discrete adjoint with checkpoints every 100 steps.
+    Reports the backward / forward device-time ratio."""
+    from fases_b200 import materials as mats
+    from fases_b200 import scenes
+    steps = args.steps if args.steps != 300 else 8000
+    seg = 100
+    b = scenes.benchmark_room(room_cells=(256, 256, 256), n_obstacles=5, n_receivers=8)
+    b["packed"] = mats.pack(b["materials"])
+    rng = np.random.default_rng(9)
+    true = {k: np.array(v, dtype=np.float64, copy=True) for k, v in b["packed"].items()}
+    for k in ("A", "B", "Cc"):
+        true[k] = true[k] * (1.0 + 0.1 * rng.standard_normal(true[k].shape))
+    bt = dict(b, packed=true)
+    s = make_solver(bt, "fp32", steps)
+    s.run(steps)
+    target = s.ir()
+    s.close()
+    s = make_solver(b, "fp32", steps)
+    g = s.misfit_gradient(target, nsteps=steps, segment_steps=seg)
+    s.close()
+    s = make_solver(b, "fp32", steps)
+    s.run(20)
+    ms_plain = s.run_timed(steps) if steps <= 2000 else s.run_timed(2000) * steps / 2000.0
+    s.close()
+    cells = 256 ** 3
+    print(json.dumps({
+        "metric": "adjoint (config 5): backward / forward device time", "value": g["backward_ms"] / g["forward_ms"],
+        "unit": "ratio", "higher_is_better": False, "steps": steps, "segment_steps": seg,
+        "forward_ms": g["forward_ms"], "backward_ms": g["backward_ms"], "plain_forward_ms": ms_plain,
+        "forward_gcell_s": cells * steps / (g["forward_ms"] / 1e3) / 1e9, "J": g["J"],
+        "grad_norm": float(np.linalg.norm(g["raw"])), "n_parameters": int(g["raw"].size),
+        "config": {"workload": "256^3 shoebox, 5 rigid obstacles, 6 ADE walls (2 real + 2 complex poles), "
+                               "20-cell cPML on one face, Gaussian pulse, 8 receivers, FP32; target from "
+                               "A, B, C perturbed by 10 % (seed 9)"}}), flush=True)
+
+
 def main():
     args = parse()
     rank, world, local, pg = dist_setup(args.gpus)
@@ -399,6 +438,10 @@ def main():
     if args.config == "batched":
         if rank == 0:
             run_batched(args)
+        return
+    if args.config == "adjoint":
+        if rank == 0:
+            run_adjoint(args)
         return
     room = args.room
     b = workload(room)

@@ -1,0 +1,371 @@
+// fz_adjoint.cpp -- gradient of a receiver misfit with respect to the ADE material coefficients by
+// the discrete adjoint of the stepping scheme (kernels in fz_adjoint.cu). No counterpart in the
+// reference: its material fit (common/fminconFIT.py:239-348) matches octave absorption in the
+// frequency domain and never differentiates the time-domain solver.
+//
+// Schedule: one forward pass that saves the state (U0, the ADE "old" set, the cPML psi tiles)
+// every `seg` steps; then, last segment first, restore the segment's checkpoint, recompute its
+// steps while storing every stage input and ADE set, and sweep the segment backwards, three
+// reversed stages per step (band adjoint, WENO-Z centre adjoint, gather).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fz_adjoint.h"
+#include "fz_internal.h"
+
+using fz::GHOST;
+using fz::XOFF;
+
+namespace {
+
+#define FZ_ACUDA(h, call, what)                                         \
+  do {                                                                  \
+    cudaError_t e__ = (call);                                           \
+    if (e__ != cudaSuccess) return fzi::cuda_fail(h, e__, what);       \
+  } while (0)
+
+struct Arena {
+  char* base = nullptr;
+  size_t used = 0, cap = 0;
+  void* take(size_t bytes) {
+    const size_t a = (used + 255) & ~(size_t)255;
+    if (a + bytes > cap) return nullptr;
+    used = a + bytes;
+    return base + a;
+  }
+};
+
+size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// One saved state: fields U0, ADE "old" set, psi tiles.
+struct State {
+  void* f[4] = {nullptr, nullptr, nullptr, nullptr};
+  double* ade[3] = {nullptr, nullptr, nullptr};
+  void* psi[3] = {nullptr, nullptr, nullptr};
+};
+
+template <class R>
+int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target, int64_t tsteps, double* J,
+                    double* grad, int64_t grad_cap, double* ms) {
+  typedef typename fz::Pair<R>::T P;
+  cudaStream_t s = h->stream;
+  const int64_t N = h->ncell_dev;
+  const size_t fb = (size_t)N * sizeof(R);
+  const int64_t nB = h->nB;
+  const int K = h->K, L = h->L;
+  const int nMat = std::max(1, h->nMat);
+  const int Pn = 1 + 2 * K + 4 * L;
+  if (grad_cap < (int64_t)nMat * Pn)
+    return fzi::set_error(h, FZ_EINVAL, "fz_misfit_gradient: grad needs nMat*(1+2K+4L) = " +
+                                            std::to_string((int64_t)nMat * Pn) + " elements");
+  const size_t ade_b[3] = {(size_t)K * nB * 8, (size_t)L * nB * 8, (size_t)L * nB * 8};
+  const int64_t d2 = 2 * (int64_t)h->prm.pml_cells;
+  const int64_t tile_n[3] = {d2 * h->Ny * h->Nz, (int64_t)h->Nx * d2 * h->Nz, (int64_t)h->Nx * h->Ny * d2};
+  size_t psi_b[3];
+  for (int a = 0; a < 3; a++) psi_b[a] = h->d_psi[a] ? (size_t)tile_n[a] * sizeof(P) : 0;
+  size_t ade_sum = 0, psi_sum = 0;
+  for (int a = 0; a < 3; a++) {
+    ade_sum += round256(ade_b[a]);
+    psi_sum += round256(psi_b[a]);
+  }
+  const int64_t nseg = (nsteps + seg - 1) / seg;
+  const size_t state_b = 4 * round256(fb) + ade_sum + psi_sum;
+  const size_t seg_b = (size_t)seg * (3 * 4 * round256(fb) + 4 * ade_sum);
+  const size_t adj_b = 4 * 4 * round256(fb) + 30 * round256(fb) + 4 * ade_sum + psi_sum +
+                       round256((size_t)nMat * Pn * 8) + round256((size_t)h->nrec * tsteps * 8);
+  const size_t total = (size_t)(nseg + 1) * state_b + seg_b + adj_b + 4096;
+  size_t free_b = 0, tot_b = 0;
+  FZ_ACUDA(h, cudaMemGetInfo(&free_b, &tot_b), "cudaMemGetInfo");
+  if (total + ((size_t)256 << 20) > free_b)
+    return fzi::set_error(h, FZ_ENOMEM, "fz_misfit_gradient: needs " + std::to_string(total >> 20) + " MiB, " +
+                                            std::to_string(free_b >> 20) + " MiB free (shorten segment_steps)");
+  Arena ar;
+  ar.cap = total;
+  FZ_ACUDA(h, cudaMalloc((void**)&ar.base, total), "cudaMalloc(adjoint)");
+  struct Guard {
+    char* p;
+    ~Guard() { cudaFree(p); }
+  } guard{ar.base};
+
+  auto take_state = [&](State& st) {
+    for (int f = 0; f < 4; f++) st.f[f] = ar.take(fb);
+    for (int a = 0; a < 3; a++) st.ade[a] = (double*)ar.take(ade_b[a]);
+    for (int a = 0; a < 3; a++) st.psi[a] = psi_b[a] ? ar.take(psi_b[a]) : nullptr;
+  };
+  std::vector<State> ck((size_t)nseg + 1);
+  for (auto& st : ck) take_state(st);
+  // per-step storage of one segment: stage inputs U0, U1, U2 and ADE sets phi^n, phi^(1), phi^(2),
+  // phi^{n+1}
+  std::vector<void*> S[3];
+  std::vector<double*> Ad[4][3];
+  for (int t = 0; t < seg; t++) {
+    for (int q = 0; q < 3; q++)
+      for (int f = 0; f < 4; f++) S[q].push_back(ar.take(fb));
+    for (int q = 0; q < 4; q++)
+      for (int a = 0; a < 3; a++) Ad[q][a].push_back((double*)ar.take(ade_b[a]));
+  }
+  R* lam[4][4];  // adjoint field sets A (carried), B, C, D
+  for (int q = 0; q < 4; q++)
+    for (int f = 0; f < 4; f++) lam[q][f] = (R*)ar.take(fb);
+  R* contrib = (R*)ar.take(30 * round256(fb));
+  double* lade[4][3];  // ADE adjoint sets: next, old, 1, 2
+  for (int q = 0; q < 4; q++)
+    for (int a = 0; a < 3; a++) lade[q][a] = (double*)ar.take(ade_b[a]);
+  P* lpsi[3];
+  for (int a = 0; a < 3; a++) lpsi[a] = psi_b[a] ? (P*)ar.take(psi_b[a]) : nullptr;
+  double* d_grad = (double*)ar.take((size_t)nMat * Pn * 8);
+  double* d_target = (double*)ar.take((size_t)h->nrec * tsteps * 8);
+  if (!d_target) return fzi::set_error(h, FZ_ENOMEM, "fz_misfit_gradient: arena layout overflow");
+
+  auto save = [&](const State& st) -> cudaError_t {
+    cudaError_t e = cudaSuccess;
+    for (int f = 0; f < 4 && e == cudaSuccess; f++)
+      e = cudaMemcpyAsync(st.f[f], h->U[h->i0][f], fb, cudaMemcpyDeviceToDevice, s);
+    for (int a = 0; a < 3 && e == cudaSuccess; a++)
+      if (ade_b[a]) e = cudaMemcpyAsync(st.ade[a], h->d_ade[h->ph_old][a], ade_b[a], cudaMemcpyDeviceToDevice, s);
+    for (int a = 0; a < 3 && e == cudaSuccess; a++)
+      if (psi_b[a]) e = cudaMemcpyAsync(st.psi[a], h->d_psi[a], psi_b[a], cudaMemcpyDeviceToDevice, s);
+    return e;
+  };
+  auto restore = [&](const State& st, int64_t step) -> cudaError_t {
+    cudaError_t e = cudaSuccess;
+    for (int f = 0; f < 4 && e == cudaSuccess; f++)
+      e = cudaMemcpyAsync(h->U[h->i0][f], st.f[f], fb, cudaMemcpyDeviceToDevice, s);
+    for (int a = 0; a < 3 && e == cudaSuccess; a++)
+      if (ade_b[a]) e = cudaMemcpyAsync(h->d_ade[h->ph_old][a], st.ade[a], ade_b[a], cudaMemcpyDeviceToDevice, s);
+    for (int a = 0; a < 3 && e == cudaSuccess; a++)
+      if (psi_b[a]) e = cudaMemcpyAsync(h->d_psi[a], st.psi[a], psi_b[a], cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_step, &step, sizeof(step), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // the step value lives on this stack frame
+    return e;
+  };
+
+  // cells no kernel writes stay constant through a run: make them zero in every field set, so
+  // that a checkpoint of U0 alone reproduces the whole state
+  for (int q = 0; q < 3; q++)
+    for (int f = 0; f < 4; f++)
+      FZ_ACUDA(h, fz::launch_clear_inactive<R>((R*)h->U[q][f], h->d_cls, N, s), "clear inactive");
+
+  cudaEvent_t ev[4];
+  for (auto& e : ev) FZ_ACUDA(h, cudaEventCreate(&e), "event");
+  struct EvGuard {
+    cudaEvent_t* e;
+    ~EvGuard() {
+      for (int i = 0; i < 4; i++) cudaEventDestroy(e[i]);
+    }
+  } evg{ev};
+
+  // ---- forward with checkpoints
+  FZ_ACUDA(h, cudaEventRecord(ev[0], s), "event record");
+  for (int64_t q = 0; q < nseg; q++) {
+    FZ_ACUDA(h, save(ck[(size_t)q]), "checkpoint");
+    const int rc = fz_run(h, std::min<int64_t>(seg, nsteps - q * seg));
+    if (rc != FZ_OK) return rc;
+  }
+  FZ_ACUDA(h, save(ck[(size_t)nseg]), "checkpoint");
+  FZ_ACUDA(h, cudaEventRecord(ev[1], s), "event record");
+  int rc = fz_sync(h, 0);
+  if (rc != FZ_OK) return rc;
+
+  // ---- misfit
+  std::vector<double> ir((size_t)h->nrec * h->rec_cap);
+  FZ_ACUDA(h, cudaMemcpy(ir.data(), h->d_ir, ir.size() * 8, cudaMemcpyDeviceToHost), "IR D2H");
+  double Jv = 0.0;
+  for (int r = 0; r < h->nrec; r++)
+    for (int64_t n = 0; n < nsteps; n++) {
+      const double d = ir[(size_t)r * h->rec_cap + n] - target[(size_t)r * tsteps + n];
+      Jv += d * d;
+    }
+  if (J) *J = Jv;
+  FZ_ACUDA(h, cudaMemcpy(d_target, target, (size_t)h->nrec * tsteps * 8, cudaMemcpyHostToDevice), "target H2D");
+
+  // ---- backward
+  for (int f = 0; f < 4; f++) FZ_ACUDA(h, cudaMemsetAsync(lam[0][f], 0, fb, s), "memset");
+  for (int a = 0; a < 3; a++)
+    if (ade_b[a]) FZ_ACUDA(h, cudaMemsetAsync(lade[0][a], 0, ade_b[a], s), "memset");
+  for (int a = 0; a < 3; a++)
+    if (psi_b[a]) FZ_ACUDA(h, cudaMemsetAsync(lpsi[a], 0, psi_b[a], s), "memset");
+  FZ_ACUDA(h, cudaMemsetAsync(d_grad, 0, (size_t)nMat * Pn * 8, s), "memset");
+
+  const fz_params& p = h->prm;
+  fz::AdjStageArgs<R> sa;
+  std::memset(&sa, 0, sizeof(sa));
+  sa.contrib = contrib;
+  sa.cls = h->d_cls;
+  sa.Nx = h->Nx; sa.Ny = h->Ny; sa.Nz = h->Nz;
+  sa.Sx = h->Sx; sa.plane = h->plane;
+  sa.ncell = (int64_t)(round256(fb) / sizeof(R));
+  sa.inv_h = (R)(1.0 / p.h);
+  sa.fc = (R)(0.5 * p.c);
+  sa.frc2 = (R)(0.5 * p.rho * p.c * p.c);
+  sa.firho = (R)(0.5 / p.rho);
+  sa.pml_on = h->pml_on ? 1 : 0;
+  sa.pml_d2 = (int)d2;
+  sa.pcx = (const fz::PmlCoef<R>*)h->d_pml_coef[0];
+  sa.pcy = (const fz::PmlCoef<R>*)h->d_pml_coef[1];
+  sa.pcz = (const fz::PmlCoef<R>*)h->d_pml_coef[2];
+  sa.lpsix = lpsi[0]; sa.lpsiy = lpsi[1]; sa.lpsiz = lpsi[2];
+
+  fz::AdjBandArgs<R> ba;
+  std::memset(&ba, 0, sizeof(ba));
+  ba.nB = nB;
+  ba.rec = h->d_brec;
+  ba.geo = (const R*)h->d_bgeo;
+  ba.nrm = (const R*)h->d_bnrm;
+  ba.Sx = h->Sx; ba.plane = h->plane;
+  ba.Z0 = p.rho * p.c;
+  ba.dt = p.dt;
+  ba.K = K; ba.L = L; ba.nMat = nMat;
+  {
+    const double* m = h->d_mat;
+    ba.Rinf = m; m += nMat;
+    ba.A = m; m += (size_t)nMat * K;
+    ba.zeta = m; m += (size_t)nMat * K;
+    ba.B = m; m += (size_t)nMat * L;
+    ba.C = m; m += (size_t)nMat * L;
+    ba.alpha = m; m += (size_t)nMat * L;
+    ba.beta = m;
+  }
+  ba.grad = d_grad;
+
+  // buffer roles: A = adjoint of the step's output, B/D = of the stage-2/stage-1 inputs, C = of U0
+  int iA = 0, iB = 1, iC = 2, iD = 3;
+  int jN = 0, jO = 1, j1 = 2, j2 = 3;  // ADE adjoint sets: next, old, after stage 0, after stage 1
+  auto set_in = [&](auto& x, const void* const* f) {
+    x.pi = (const R*)f[0]; x.ui = (const R*)f[1]; x.vi = (const R*)f[2]; x.wi = (const R*)f[3];
+  };
+
+  FZ_ACUDA(h, cudaEventRecord(ev[2], s), "event record");
+  for (int64_t q = nseg - 1; q >= 0; q--) {
+    const int len = (int)std::min<int64_t>(seg, nsteps - q * seg);
+    FZ_ACUDA(h, restore(ck[(size_t)q], q * seg), "restore");
+    // recompute the segment, storing stage inputs and ADE sets
+    for (int t = 0; t < len; t++) {
+      cudaError_t e = cudaSuccess;
+      for (int f = 0; f < 4 && e == cudaSuccess; f++)
+        e = cudaMemcpyAsync(S[0][(size_t)t * 4 + f], h->U[h->i0][f], fb, cudaMemcpyDeviceToDevice, s);
+      for (int a = 0; a < 3 && e == cudaSuccess; a++)
+        if (ade_b[a]) e = cudaMemcpyAsync(Ad[0][a][(size_t)t], h->d_ade[h->ph_old][a], ade_b[a], cudaMemcpyDeviceToDevice, s);
+      if (e == cudaSuccess) e = fzi::enqueue_stage(h, 0);
+      for (int f = 0; f < 4 && e == cudaSuccess; f++)
+        e = cudaMemcpyAsync(S[1][(size_t)t * 4 + f], h->U[h->i1][f], fb, cudaMemcpyDeviceToDevice, s);
+      for (int a = 0; a < 3 && e == cudaSuccess; a++)
+        if (ade_b[a]) e = cudaMemcpyAsync(Ad[1][a][(size_t)t], h->d_ade[h->ph_cur][a], ade_b[a], cudaMemcpyDeviceToDevice, s);
+      if (e == cudaSuccess) e = fzi::enqueue_stage(h, 1);
+      for (int f = 0; f < 4 && e == cudaSuccess; f++)
+        e = cudaMemcpyAsync(S[2][(size_t)t * 4 + f], h->U[h->i2][f], fb, cudaMemcpyDeviceToDevice, s);
+      for (int a = 0; a < 3 && e == cudaSuccess; a++)
+        if (ade_b[a]) e = cudaMemcpyAsync(Ad[2][a][(size_t)t], h->d_ade[h->ph_nu][a], ade_b[a], cudaMemcpyDeviceToDevice, s);
+      if (e == cudaSuccess) e = fzi::enqueue_stage(h, 2);
+      for (int a = 0; a < 3 && e == cudaSuccess; a++)
+        if (ade_b[a]) e = cudaMemcpyAsync(Ad[3][a][(size_t)t], h->d_ade[h->ph_cur][a], ade_b[a], cudaMemcpyDeviceToDevice, s);
+      if (e == cudaSuccess) e = fzi::enqueue_finish(h);
+      if (e != cudaSuccess) return fzi::cuda_fail(h, e, "adjoint recompute");
+    }
+    // reverse sweep
+    for (int t = len - 1; t >= 0; t--) {
+      const int64_t n = q * seg + t;
+      for (int qq : {iB, iC, iD})
+        for (int f = 0; f < 4; f++) FZ_ACUDA(h, cudaMemsetAsync(lam[qq][f], 0, fb, s), "memset");
+      for (int qq : {jO, j1, j2})
+        for (int a = 0; a < 3; a++)
+          if (ade_b[a]) FZ_ACUDA(h, cudaMemsetAsync(lade[qq][a], 0, ade_b[a], s), "memset");
+      FZ_ACUDA(h, fz::launch_adj_receivers<R>(lam[iA][0], h->d_rec_cell, h->nrec, h->d_ir, h->rec_cap, d_target,
+                                               tsteps, n, s), "adjoint receivers");
+      const void* const* in_st[3] = {&S[0][(size_t)t * 4], &S[1][(size_t)t * 4], &S[2][(size_t)t * 4]};
+      for (int st = 2; st >= 0; st--) {
+        // adjoint of the stage output (out), of its input (inb) and of U0 (base)
+        const int out = (st == 2) ? iA : (st == 1) ? iB : iD;
+        const int inb = (st == 2) ? iB : (st == 1) ? iD : iC;
+        // ADE value sets (left, middle, right) and their adjoints, as band_args assigns them
+        const int vL = (st == 0) ? 1 : (st == 1) ? 2 : 3, vM = 0, vR = (st == 0) ? 0 : (st == 1) ? 1 : 2;
+        const int gL = (st == 0) ? j1 : (st == 1) ? j2 : jN;
+        const int gR = (st == 0) ? jO : (st == 1) ? j1 : j2;
+        if (nB > 0) {
+          set_in(ba, in_st[st]);
+          ba.lp = lam[out][0]; ba.lu = lam[out][1]; ba.lv = lam[out][2]; ba.lw = lam[out][3];
+          ba.ip = lam[inb][0]; ba.iu = lam[inb][1]; ba.iv = lam[inb][2]; ba.iw = lam[inb][3];
+          ba.phL = Ad[vL][0][(size_t)t]; ba.phM = Ad[vM][0][(size_t)t]; ba.phR = Ad[vR][0][(size_t)t];
+          ba.s1L = Ad[vL][1][(size_t)t]; ba.s1M = Ad[vM][1][(size_t)t]; ba.s1R = Ad[vR][1][(size_t)t];
+          ba.s2L = Ad[vL][2][(size_t)t]; ba.s2M = Ad[vM][2][(size_t)t]; ba.s2R = Ad[vR][2][(size_t)t];
+          ba.gphL = lade[gL][0]; ba.gphM = lade[jO][0]; ba.gphR = lade[gR][0];
+          ba.gs1L = lade[gL][1]; ba.gs1M = lade[jO][1]; ba.gs1R = lade[gR][1];
+          ba.gs2L = lade[gL][2]; ba.gs2M = lade[jO][2]; ba.gs2R = lade[gR][2];
+          FZ_ACUDA(h, fz::launch_adj_band<R>(st, ba, s), "adjoint band");
+        }
+        set_in(sa, in_st[st]);
+        sa.lp = lam[out][0]; sa.lu = lam[out][1]; sa.lv = lam[out][2]; sa.lw = lam[out][3];
+        sa.ip = lam[inb][0]; sa.iu = lam[inb][1]; sa.iv = lam[inb][2]; sa.iw = lam[inb][3];
+        sa.bp = lam[iC][0]; sa.bu = lam[iC][1]; sa.bv = lam[iC][2]; sa.bw = lam[iC][3];
+        const double w = (st == 0) ? 1.0 : (st == 1) ? 0.25 : 2.0 / 3.0;
+        sa.stage = st;
+        sa.b_in = (R)w;
+        sa.a_base = (R)((st == 0) ? 0.0 : (st == 1) ? 0.75 : 1.0 / 3.0);
+        sa.cb = (R)(w * p.dt / p.h);
+        sa.wdt = (R)(w * p.dt);
+        FZ_ACUDA(h, fz::launch_adj_centres<R>(sa, s), "adjoint centres");
+        FZ_ACUDA(h, fz::launch_adj_gather<R>(sa, s), "adjoint gather");
+      }
+      std::swap(iA, iC);  // the adjoint of U0^n is the next (earlier) step's output adjoint
+      std::swap(jN, jO);
+    }
+  }
+  FZ_ACUDA(h, cudaEventRecord(ev[3], s), "event record");
+  FZ_ACUDA(h, cudaStreamSynchronize(s), "adjoint sync");
+  FZ_ACUDA(h, cudaMemcpy(grad, d_grad, (size_t)nMat * Pn * 8, cudaMemcpyDeviceToHost), "grad D2H");
+  if (ms) {
+    float a = 0.f, b = 0.f;
+    FZ_ACUDA(h, cudaEventElapsedTime(&a, ev[0], ev[1]), "event elapsed");
+    FZ_ACUDA(h, cudaEventElapsedTime(&b, ev[2], ev[3]), "event elapsed");
+    ms[0] = a;
+    ms[1] = b;
+  }
+  // leave the handle at the end of the forward run
+  FZ_ACUDA(h, restore(ck[(size_t)nseg], nsteps), "restore final state");
+  return fz_sync(h, 0);
+}
+
+}  // namespace
+
+extern "C" {
+
+int fz_material_layout(fz_handle* h, int32_t* nMat, int32_t* K, int32_t* L) {
+  if (!h) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  const int rc = fzi::prepare(h);
+  if (rc != FZ_OK) return rc;
+  if (nMat) *nMat = std::max(1, h->nMat);
+  if (K) *K = h->K;
+  if (L) *L = h->L;
+  return FZ_OK;
+}
+
+int fz_misfit_gradient(fz_handle* h, int64_t nsteps, int32_t segment_steps, const double* target,
+                       int64_t target_steps, double* J, double* grad, int64_t grad_cap, double* ms) {
+  if (!h) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  if (nsteps < 1 || segment_steps < 1 || !target || !grad || target_steps < nsteps)
+    return fzi::set_error(h, FZ_EINVAL, "fz_misfit_gradient: nsteps >= 1, segment_steps >= 1, target of "
+                                        "[n_rec][target_steps >= nsteps], grad required");
+  if (h->prm.two_d || h->nb != 1)
+    return fzi::set_error(h, FZ_EINVAL, "fz_misfit_gradient: 3D single-member solves only");
+  int rc = fzi::prepare(h);
+  if (rc != FZ_OK) return rc;
+  if (h->nrec < 1 || h->rec_cap < nsteps)
+    return fzi::set_error(h, FZ_EINVAL, "fz_misfit_gradient: receivers with capacity >= nsteps required");
+  if (h->steps_enqueued != 0)
+    return fzi::set_error(h, FZ_ESTATE, "fz_misfit_gradient: the handle must be at step 0 (set fields, then call)");
+  for (int q = 0; q < h->nsrc; q++) {
+    const int64_t c = (int64_t)XOFF + h->src_ijk[3 * q] +
+                      h->Sx * ((int64_t)h->src_ijk[3 * q + 1] + (int64_t)h->Ny * h->src_ijk[3 * q + 2]);
+    if (!(h->cls_host[(size_t)c] & fz::CLS_UPDATE))
+      return fzi::set_error(h, FZ_EINVAL, "fz_misfit_gradient: a source sits in a cell the stage kernels skip");
+  }
+  cudaSetDevice(h->device);
+  return h->fp64 ? misfit_gradient<double>(h, nsteps, segment_steps, target, target_steps, J, grad, grad_cap, ms)
+                 : misfit_gradient<float>(h, nsteps, segment_steps, target, target_steps, J, grad, grad_cap, ms);
+}
+
+}  // extern "C"

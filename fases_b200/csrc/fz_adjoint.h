@@ -1,0 +1,123 @@
+// fz_adjoint.h -- kernels of the discrete adjoint of one SSP-RK3 step (fz_adjoint.cu) and the
+// arguments they take. The adjoint is of the scheme the stepping kernels compute
+// (3D-solver/core/functions3D.cuh:56-78, 426-565, 661-1001, 1086-1327); the reference has no
+// adjoint or gradient of any kind.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fz_device.cuh"
+
+namespace fz {
+
+// Adjoint of the stage kernel of one stage: the stage output is
+//   out = a U0 + b (in + dt/h sum_d dF_d(in)) + w dt sum_d [pml_d] ((1/kappa_d - 1) dF_d/h + psi_d)
+// on update cells (dF_d = flux difference along axis d), and psi^{n+1} = b_d psi^n + ca_d dF_d/h
+// in stage 2.
+template <class R>
+struct AdjStageArgs {
+  typedef typename Pair<R>::T P;
+  const R* pi;  // stage input (stored forward state)
+  const R* ui;
+  const R* vi;
+  const R* wi;
+  const R* lp;  // adjoint of the stage output (after the band adjoint scaled band cells)
+  const R* lu;
+  const R* lv;
+  const R* lw;
+  R* ip;  // adjoint of the stage input (accumulated)
+  R* iu;
+  R* iv;
+  R* iw;
+  R* bp;  // adjoint of U0 (accumulated; stages 1 and 2)
+  R* bu;
+  R* bv;
+  R* bw;
+  R* contrib;  // [30][ncell]: per axis d, stencil offset k - 2, component (p, normal velocity)
+  const uint8_t* cls;
+  int32_t Nx, Ny, Nz;
+  int64_t Sx, plane, ncell;
+  R cb;      // b dt / h
+  R a_base;  // a
+  R b_in;    // b
+  R wdt;     // w dt
+  R inv_h;
+  R fc, frc2, firho;  // Godunov: c/2, rho c^2 / 2, 1 / (2 rho)
+  int32_t stage;
+  int32_t pml_on, pml_d2;
+  const PmlCoef<R>* pcx;
+  const PmlCoef<R>* pcy;
+  const PmlCoef<R>* pcz;
+  P* lpsix;  // adjoint of the cPML psi tiles (stage 2: of psi^{n+1} on entry, of psi^n on exit)
+  P* lpsiy;
+  P* lpsiz;
+};
+
+// Adjoint of the immersed band of one stage (functions3D.cuh:426-565), with the gradient of the
+// misfit with respect to the ADE coefficients accumulated per material.
+template <class R>
+struct AdjBandArgs {
+  int64_t nB;
+  const int4* rec;
+  const R* geo;
+  const R* nrm;
+  const R* pi;  // stage input (probe source)
+  const R* ui;
+  const R* vi;
+  const R* wi;
+  R* lp;  // adjoint of the stage output: read, then scaled by (1 - chi) at band cells
+  R* lu;
+  R* lv;
+  R* lw;
+  R* ip;  // adjoint of the stage input: probe contributions scattered with atomics
+  R* iu;
+  R* iv;
+  R* iw;
+  int64_t Sx, plane;
+  double Z0, dt;
+  int32_t K, L, nMat;
+  const double* Rinf;
+  const double* A;
+  const double* zeta;
+  const double* B;
+  const double* C;
+  const double* alpha;
+  const double* beta;
+  // ADE state values of the stage (left = written, middle, right), [q*nB + b]
+  const double* phL;
+  const double* phM;
+  const double* phR;
+  const double* s1L;
+  const double* s1M;
+  const double* s1R;
+  const double* s2L;
+  const double* s2M;
+  const double* s2R;
+  // their adjoints: left read, middle and right accumulated
+  const double* gphL;
+  double* gphM;
+  double* gphR;
+  const double* gs1L;
+  double* gs1M;
+  double* gs1R;
+  const double* gs2L;
+  double* gs2M;
+  double* gs2R;
+  double* grad;  // [nMat][1 + 2K + 4L]: Rinf, A[K], zeta[K], B[L], C[L], alpha[L], beta[L]
+};
+
+template <class R>
+cudaError_t launch_adj_centres(const AdjStageArgs<R>& a, cudaStream_t s);
+template <class R>
+cudaError_t launch_adj_gather(const AdjStageArgs<R>& a, cudaStream_t s);
+template <class R>
+cudaError_t launch_adj_band(int stage, const AdjBandArgs<R>& a, cudaStream_t s);
+// adjoint of the receiver gather: lp[cell_r] += 2 (ir[r][n] - target[r][n])
+template <class R>
+cudaError_t launch_adj_receivers(R* lp, const int64_t* rcell, int nrec, const double* ir, int64_t cap,
+                                 const double* target, int64_t tlen, int64_t n, cudaStream_t s);
+// zero every field value of cells no kernel writes (class bytes without UPDATE or BAND)
+template <class R>
+cudaError_t launch_clear_inactive(R* f, const uint8_t* cls, int64_t n, cudaStream_t s);
+
+}  // namespace fz

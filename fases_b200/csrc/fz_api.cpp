@@ -275,6 +275,8 @@ int build_band(fz_handle* h) {
       }
       mat.push_back(mat[(size_t)b]);
     }
+  for (int64_t c : cell) h->cls_host[(size_t)c] |= fz::CLS_BAND;
+  FZ_CUDA(h, cudaMemcpy(h->d_cls, h->cls_host.data(), h->cls_host.size(), cudaMemcpyHostToDevice), "cls H2D");
   std::vector<int4> rec((size_t)h->nB);
   for (size_t b = 0; b < rec.size(); b++) {
     const uint64_t c = (uint64_t)cell[b];
@@ -514,32 +516,38 @@ struct Timer {
   }
 };
 
-// One time step (main3D.cu:1280-1319 + receivers 1399-1414).
+// Stage st of the current step: the stage kernel, then the immersed band (main3D.cu:1286-1306).
 template <class R>
-cudaError_t enqueue_step(fz_handle* h) {
+cudaError_t enqueue_stage(fz_handle* h, int st) {
   cudaError_t e;
-  for (int st = 0; st < 3; st++) {
-    {
-      Timer t(h, st);
-      const int in_set = (st == 0) ? h->i0 : (st == 1) ? h->i1 : h->i2;
-      fz::StageMaps m;
-      m.p = h->halo_map[in_set][0];
-      m.u = h->halo_map[in_set][1];
-      m.v = h->halo_map[in_set][2];
-      m.bp = h->own_map[h->i0][0];
-      m.bu = h->own_map[h->i0][1];
-      m.bv = h->own_map[h->i0][2];
-      m.bw = h->own_map[h->i0][3];
-      m.cls = h->cls_map;
-      e = fz::launch_stage<R>(st, h->prm.two_d != 0, stage_args<R>(h, st), m, h->stage_grid, h->stream);
-      if (e != cudaSuccess) return e;
-    }
-    if (h->nB > 0) {
-      Timer t(h, 3);
-      e = fz::launch_band<R>(st, band_args<R>(h, st), h->stream);
-      if (e != cudaSuccess) return e;
-    }
+  {
+    Timer t(h, st);
+    const int in_set = (st == 0) ? h->i0 : (st == 1) ? h->i1 : h->i2;
+    fz::StageMaps m;
+    m.p = h->halo_map[in_set][0];
+    m.u = h->halo_map[in_set][1];
+    m.v = h->halo_map[in_set][2];
+    m.bp = h->own_map[h->i0][0];
+    m.bu = h->own_map[h->i0][1];
+    m.bv = h->own_map[h->i0][2];
+    m.bw = h->own_map[h->i0][3];
+    m.cls = h->cls_map;
+    e = fz::launch_stage<R>(st, h->prm.two_d != 0, stage_args<R>(h, st), m, h->stage_grid, h->stream);
+    if (e != cudaSuccess) return e;
   }
+  if (h->nB > 0) {
+    Timer t(h, 3);
+    e = fz::launch_band<R>(st, band_args<R>(h, st), h->stream);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// End of a step: receiver gather, device step counter, buffer rotation (main3D.cu:1312-1319,
+// 1399-1414).
+template <class R>
+cudaError_t enqueue_finish(fz_handle* h) {
+  cudaError_t e;
   {
     Timer t(h, 4);
     R* const* u1 = (R* const*)h->U[h->i1];
@@ -550,6 +558,16 @@ cudaError_t enqueue_step(fz_handle* h) {
   std::swap(h->i0, h->i1);
   std::swap(h->ph_old, h->ph_cur);
   return cudaSuccess;
+}
+
+// One time step (main3D.cu:1280-1319 + receivers 1399-1414).
+template <class R>
+cudaError_t enqueue_step(fz_handle* h) {
+  for (int st = 0; st < 3; st++) {
+    const cudaError_t e = enqueue_stage<R>(h, st);
+    if (e != cudaSuccess) return e;
+  }
+  return enqueue_finish<R>(h);
 }
 
 template <class R>
@@ -706,6 +724,10 @@ int prepare(fz_handle* h) {
   return h->fp64 ? finalize<double>(h) : finalize<float>(h);
 }
 cudaError_t enqueue(fz_handle* h) { return h->fp64 ? enqueue_step<double>(h) : enqueue_step<float>(h); }
+cudaError_t enqueue_stage(fz_handle* h, int st) {
+  return h->fp64 ? ::enqueue_stage<double>(h, st) : ::enqueue_stage<float>(h, st);
+}
+cudaError_t enqueue_finish(fz_handle* h) { return h->fp64 ? ::enqueue_finish<double>(h) : ::enqueue_finish<float>(h); }
 }  // namespace fzi
 
 // ==========================================================================================

@@ -26,6 +26,7 @@ constexpr int NBUF = 3;  // plane tiles in flight (TMA ring)
 // Cell-class bits (one byte per cell, replaces the reference's 4-byte S read per stage).
 constexpr uint8_t CLS_UPDATE = 1;  // interior cell with S >= h: written by the stage kernels
 constexpr uint8_t CLS_SOURCE = 2;  // a point source sits here
+constexpr uint8_t CLS_BAND = 4;    // an immersed band cell (written by the band kernel)
 
 // Per-axis cPML coefficients at one index along the axis (functions3D.cuh:681-756), precomputed
 // on the host once instead of powf/expf per cell and stage.

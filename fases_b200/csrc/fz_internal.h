@@ -121,4 +121,7 @@ int cuda_fail(fz_handle* h, cudaError_t e, const char* what);
 int prepare(fz_handle* h);
 // enqueues one time step on the handle's stream (or into the capture the stream takes part in)
 cudaError_t enqueue(fz_handle* h);
+// the parts of one step: stage st (stage kernel + band), then receivers and buffer rotation
+cudaError_t enqueue_stage(fz_handle* h, int st);
+cudaError_t enqueue_finish(fz_handle* h);
 }  // namespace fzi

@@ -198,6 +198,33 @@ class Solver:
         self._chk(lib().fz_get_fields(self._h, *[_dptr(a) for a in out]))
         return out
 
+    def material_layout(self):
+        """(nMat, K, L) of the material table after setup (K, L >= 1, zero-padded)."""
+        n, k, l = C.c_int32(), C.c_int32(), C.c_int32()
+        self._chk(lib().fz_material_layout(self._h, C.byref(n), C.byref(k), C.byref(l)))
+        return n.value, k.value, l.value
+
+    def misfit_gradient(self, target, nsteps=None, segment_steps=250):
+        """J = sum (IR - target)^2 over nsteps steps from the current (step-0) state and dJ/d(ADE
+        coefficients) by the discrete adjoint. target: [n_rec, >= nsteps]. Returns a dict with J,
+        the gradient split per coefficient (arrays [nMat], [nMat, K] or [nMat, L]), the raw
+        [nMat, 1 + 2K + 4L] array and the forward / backward device times in ms."""
+        target = np.ascontiguousarray(target, dtype=np.float64)
+        if target.ndim != 2 or target.shape[0] != self._nrec:
+            raise ValueError("target must be [n_rec, n_steps]")
+        nsteps = target.shape[1] if nsteps is None else int(nsteps)
+        nm, K, L = self.material_layout()
+        P = 1 + 2 * K + 4 * L
+        grad = np.zeros((nm, P), np.float64)
+        J = C.c_double()
+        ms = (C.c_double * 2)()
+        self._chk(lib().fz_misfit_gradient(self._h, nsteps, int(segment_steps), _dptr(target), target.shape[1],
+                                           C.byref(J), _dptr(grad), grad.size, ms))
+        o = 1 + 2 * K
+        return {"J": J.value, "raw": grad, "Rinf": grad[:, 0], "A": grad[:, 1:1 + K], "zeta": grad[:, 1 + K:o],
+                "B": grad[:, o:o + L], "C": grad[:, o + L:o + 2 * L], "alpha": grad[:, o + 2 * L:o + 3 * L],
+                "beta": grad[:, o + 3 * L:o + 4 * L], "forward_ms": ms[0], "backward_ms": ms[1]}
+
     def energy(self):
         e = C.c_double()
         self._chk(lib().fz_energy(self._h, C.byref(e)))

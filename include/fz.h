@@ -167,6 +167,28 @@ int fz_group_run_timed(fz_group* g, int64_t nsteps, double* ms);
 int fz_group_sync(fz_group* g, int64_t timeout_ms);
 void fz_group_destroy(fz_group* g);
 
+/* Gradient of the receiver misfit J = sum_r sum_{n < nsteps} (IR_r[n] - target[r][n])^2 (IR_r[n] = p
+ * at receiver r after step n+1, FP64) with respect to every ADE coefficient of every material, by
+ * the discrete adjoint of the stepping scheme (WENO-Z weights linearised, Godunov flux, RK stages,
+ * cPML, immersed band and ADE recursion). Runs nsteps forward from the handle's current state
+ * (which must be at step 0; cells no kernel writes are first set to zero in every field set),
+ * saving a checkpoint every segment_steps steps, then recomputes each segment while storing its
+ * stage states and sweeps it backwards. target is [n_rec][target_steps] (target_steps >= nsteps).
+ * grad gets [nMat][1 + 2K + 4L] = Rinf, A[K], zeta[K], B[L], C[L], alpha[L], beta[L] per material,
+ * in the layout of fz_set_materials (K, L as fz_material_layout reports them). ms[2] (may be
+ * NULL) gets the device time of the forward pass and of the backward pass. On return the handle
+ * holds the state after nsteps and the forward receiver traces. Device memory: about
+ * (nsteps/segment_steps + 1) states + segment_steps x 3 field sets + 50 field arrays; FZ_ENOMEM
+ * (nothing allocated) when it does not fit. 3D, batch 1, sources in updated cells only. No
+ * counterpart in the reference (its material fit, common/fminconFIT.py:239-348, works on octave
+ * absorption and never differentiates the solver). */
+int fz_misfit_gradient(fz_handle* h, int64_t nsteps, int32_t segment_steps, const double* target,
+                       int64_t target_steps, double* J, double* grad, int64_t grad_cap, double* ms);
+
+/* Material table layout after setup: number of materials (>= 1) and the real-pole / complex-pair
+ * counts K, L (each >= 1, zero-padded as read_fit_file pads, common/filterABC.h:52-89). */
+int fz_material_layout(fz_handle* h, int32_t* nMat, int32_t* K, int32_t* L);
+
 /* Receiver traces [n_rec][n_steps] (float32, as IR<r>_<s>.bin, main3D.cu:1403-1404) and
  * [n_rec][n_steps][3] velocities (as VEL<r>_<s>.bin, main3D.cu:1408-1412). cap = elements. */
 int fz_get_ir(fz_handle* h, float* out, int64_t cap);
