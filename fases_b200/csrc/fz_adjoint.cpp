@@ -75,8 +75,9 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
   const int64_t nseg = (nsteps + seg - 1) / seg;
   const size_t state_b = 4 * round256(fb) + ade_sum + psi_sum;
   const size_t seg_b = (size_t)seg * (3 * 4 * round256(fb) + 4 * ade_sum);
-  const size_t adj_b = 4 * 4 * round256(fb) + 30 * round256(fb) + 4 * ade_sum + psi_sum +
-                       round256((size_t)nMat * Pn * 8) + round256((size_t)h->nrec * tsteps * 8);
+  const size_t adj_b = 4 * 4 * round256(fb) + 4 * ade_sum + 2 * psi_sum +
+                       round256((size_t)nMat * Pn * 8) + round256((size_t)Pn * nB * 8) + round256(4 * nB * sizeof(R)) +
+                       round256((size_t)h->nrec * tsteps * 8);
   const size_t total = (size_t)(nseg + 1) * state_b + seg_b + adj_b + 4096;
   size_t free_b = 0, tot_b = 0;
   FZ_ACUDA(h, cudaMemGetInfo(&free_b, &tot_b), "cudaMemGetInfo");
@@ -111,13 +112,15 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
   R* lam[4][4];  // adjoint field sets A (carried), B, C, D
   for (int q = 0; q < 4; q++)
     for (int f = 0; f < 4; f++) lam[q][f] = (R*)ar.take(fb);
-  R* contrib = (R*)ar.take(30 * round256(fb));
   double* lade[4][3];  // ADE adjoint sets: next, old, 1, 2
   for (int q = 0; q < 4; q++)
     for (int a = 0; a < 3; a++) lade[q][a] = (double*)ar.take(ade_b[a]);
-  P* lpsi[3];
-  for (int a = 0; a < 3; a++) lpsi[a] = psi_b[a] ? (P*)ar.take(psi_b[a]) : nullptr;
+  P* lpsi[2][3];  // adjoint of psi^{n+1} (read) and of psi^n (written), swapped every step
+  for (int q = 0; q < 2; q++)
+    for (int a = 0; a < 3; a++) lpsi[q][a] = psi_b[a] ? (P*)ar.take(psi_b[a]) : nullptr;
   double* d_grad = (double*)ar.take((size_t)nMat * Pn * 8);
+  double* d_gcell = (double*)ar.take((size_t)Pn * nB * 8);
+  R* d_probe = (R*)ar.take(4 * nB * sizeof(R));
   double* d_target = (double*)ar.take((size_t)h->nrec * tsteps * 8);
   if (!d_target) return fzi::set_error(h, FZ_ENOMEM, "fz_misfit_gradient: arena layout overflow");
 
@@ -187,18 +190,17 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
   for (int f = 0; f < 4; f++) FZ_ACUDA(h, cudaMemsetAsync(lam[0][f], 0, fb, s), "memset");
   for (int a = 0; a < 3; a++)
     if (ade_b[a]) FZ_ACUDA(h, cudaMemsetAsync(lade[0][a], 0, ade_b[a], s), "memset");
-  for (int a = 0; a < 3; a++)
-    if (psi_b[a]) FZ_ACUDA(h, cudaMemsetAsync(lpsi[a], 0, psi_b[a], s), "memset");
-  FZ_ACUDA(h, cudaMemsetAsync(d_grad, 0, (size_t)nMat * Pn * 8, s), "memset");
+  for (int q = 0; q < 2; q++)
+    for (int a = 0; a < 3; a++)
+      if (psi_b[a]) FZ_ACUDA(h, cudaMemsetAsync(lpsi[q][a], 0, psi_b[a], s), "memset");
+  if (nB > 0) FZ_ACUDA(h, cudaMemsetAsync(d_gcell, 0, (size_t)Pn * nB * 8, s), "memset");
 
   const fz_params& p = h->prm;
   fz::AdjStageArgs<R> sa;
   std::memset(&sa, 0, sizeof(sa));
-  sa.contrib = contrib;
   sa.cls = h->d_cls;
   sa.Nx = h->Nx; sa.Ny = h->Ny; sa.Nz = h->Nz;
   sa.Sx = h->Sx; sa.plane = h->plane;
-  sa.ncell = (int64_t)(round256(fb) / sizeof(R));
   sa.inv_h = (R)(1.0 / p.h);
   sa.fc = (R)(0.5 * p.c);
   sa.frc2 = (R)(0.5 * p.rho * p.c * p.c);
@@ -208,7 +210,31 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
   sa.pcx = (const fz::PmlCoef<R>*)h->d_pml_coef[0];
   sa.pcy = (const fz::PmlCoef<R>*)h->d_pml_coef[1];
   sa.pcz = (const fz::PmlCoef<R>*)h->d_pml_coef[2];
-  sa.lpsix = lpsi[0]; sa.lpsiy = lpsi[1]; sa.lpsiz = lpsi[2];
+  // launch geometry of the fused stage adjoint: z chunks that fill whole waves, each chunk paying
+  // four extra centre planes
+  const int ntx = (h->Nx - 2 * GHOST + fz::TX - 1) / fz::TX, nty = (h->Ny - 2 * GHOST + fz::TY - 1) / fz::TY;
+  const int nzi = h->Nz - 2 * GHOST;
+  const size_t smem_max = fz::adj_stage_smem<R>(nzi);
+  FZ_ACUDA(h, fz::adj_stage_setup<R>(smem_max), "adjoint setup");
+  int occ = 1;
+  FZ_ACUDA(h, fz::adj_stage_occupancy<R>(&occ, smem_max), "adjoint occupancy");
+  occ = std::max(1, occ);
+  const int64_t slots = (int64_t)h->nsm * occ;
+  int best = 1;
+  double best_eff = -1.0;
+  for (int nk = 1; nk <= std::max(1, nzi / 8); nk++) {
+    const int chunk = (nzi + nk - 1) / nk;
+    const int64_t items = (int64_t)ntx * nty * ((nzi + chunk - 1) / chunk);
+    const int64_t waves = (items + slots - 1) / slots;
+    const double eff = ((double)items / (double)(waves * slots)) * ((double)chunk / (chunk + 4.0));
+    if (eff > best_eff + 1e-9) {
+      best_eff = eff;
+      best = nk;
+    }
+  }
+  sa.kz_chunk = (nzi + best - 1) / best;
+  const dim3 agrid((unsigned)ntx, (unsigned)nty, (unsigned)((nzi + sa.kz_chunk - 1) / sa.kz_chunk));
+  int ps = 0;  // lpsi[ps]: adjoint of psi^{n+1}; lpsi[1 - ps]: of psi^n
 
   fz::AdjBandArgs<R> ba;
   std::memset(&ba, 0, sizeof(ba));
@@ -230,7 +256,8 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
     ba.alpha = m; m += (size_t)nMat * L;
     ba.beta = m;
   }
-  ba.grad = d_grad;
+  ba.gcell = d_gcell;
+  ba.probe = d_probe;
 
   // buffer roles: A = adjoint of the step's output, B/D = of the stage-2/stage-1 inputs, C = of U0
   int iA = 0, iB = 1, iC = 2, iD = 3;
@@ -269,8 +296,6 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
     // reverse sweep
     for (int t = len - 1; t >= 0; t--) {
       const int64_t n = q * seg + t;
-      for (int qq : {iB, iC, iD})
-        for (int f = 0; f < 4; f++) FZ_ACUDA(h, cudaMemsetAsync(lam[qq][f], 0, fb, s), "memset");
       for (int qq : {jO, j1, j2})
         for (int a = 0; a < 3; a++)
           if (ade_b[a]) FZ_ACUDA(h, cudaMemsetAsync(lade[qq][a], 0, ade_b[a], s), "memset");
@@ -307,13 +332,21 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
         sa.a_base = (R)((st == 0) ? 0.0 : (st == 1) ? 0.75 : 1.0 / 3.0);
         sa.cb = (R)(w * p.dt / p.h);
         sa.wdt = (R)(w * p.dt);
-        FZ_ACUDA(h, fz::launch_adj_centres<R>(sa, s), "adjoint centres");
-        FZ_ACUDA(h, fz::launch_adj_gather<R>(sa, s), "adjoint gather");
+        sa.lpsix = lpsi[ps][0]; sa.lpsiy = lpsi[ps][1]; sa.lpsiz = lpsi[ps][2];
+        sa.opsix = lpsi[1 - ps][0]; sa.opsiy = lpsi[1 - ps][1]; sa.opsiz = lpsi[1 - ps][2];
+        // stage 2 stores both adjoints fresh; stage 1 stores the input's and adds to U0's; stage 0's
+        // input is U0, whose adjoint the later stages have started
+        sa.acc_in = (st == 0) ? 1 : 0;
+        sa.acc_base = (st == 1) ? 1 : 0;
+        FZ_ACUDA(h, fz::launch_adj_stage<R>(sa, agrid, s), "adjoint stage");
+        if (nB > 0) FZ_ACUDA(h, fz::launch_adj_probe_scatter<R>(ba, s), "adjoint probe scatter");
       }
       std::swap(iA, iC);  // the adjoint of U0^n is the next (earlier) step's output adjoint
       std::swap(jN, jO);
+      ps = 1 - ps;
     }
   }
+  FZ_ACUDA(h, fz::launch_adj_grad_reduce(h->d_brec, d_gcell, nB, Pn, nMat, d_grad, s), "gradient reduce");
   FZ_ACUDA(h, cudaEventRecord(ev[3], s), "event record");
   FZ_ACUDA(h, cudaStreamSynchronize(s), "adjoint sync");
   FZ_ACUDA(h, cudaMemcpy(grad, d_grad, (size_t)nMat * Pn * 8, cudaMemcpyDeviceToHost), "grad D2H");

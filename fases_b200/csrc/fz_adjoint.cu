@@ -7,6 +7,7 @@
 // adjoint. Arithmetic follows the restated formulas (as the CPU oracle writes them), not the
 // forward kernels' rearranged forms: both are the same function.
 #include "fz_adjoint.h"
+#include "fz_pair.cuh"
 
 namespace fz {
 
@@ -32,63 +33,89 @@ struct WenoTables {
   }
 };
 
-// Reverse mode of one WENO-Z cell centre: u[0..4] are the values at c-2 .. c+2; the centre gives
-// V-(c+1/2) (side 1) and V+(c-1/2) (side 0) from one set of smoothness indicators. g[0..4] +=
-// lam_m dV-/du + lam_p dV+/du.
+// Reverse mode of one WENO-Z cell centre for a pair of variables (pressure and the velocity
+// component along the sweep): u[0..4] are the values at c-2 .. c+2; the centre gives V-(c+1/2)
+// (side 1) and V+(c-1/2) (side 0) from one set of smoothness indicators. g[0..4] += lam_m dV-/du +
+// lam_p dV+/du. Reciprocals as in the forward kernels (one MUFU op in FP32).
 template <class R>
-__device__ __forceinline__ void weno_centre_rev(const R u[5], R lam_m, R lam_p, R g[5]) {
+__device__ __forceinline__ void weno_centre_rev(const typename Pair<R>::T u[5], typename Pair<R>::T lam_m,
+                                                typename Pair<R>::T lam_p, typename Pair<R>::T g[5]) {
+  typedef typename Pair<R>::T P;
   typedef WenoTables<R> T;
-  const R eps = R(1e-10);
-  R b1[3], b2[3], beta[3];
+  const P eps = psplat<R>(R(1e-10));
+  P b1[3], b2[3], tib[3], ib[3];
+  P lbeta[3];
 #pragma unroll
   for (int r = 0; r < 3; r++) {
-    b1[r] = u[2 - r] - R(2) * u[3 - r] + u[4 - r];
-    b2[r] = T::brl(r, 0) * u[2 - r] + T::brl(r, 1) * u[3 - r] + T::brl(r, 2) * u[4 - r];
-    beta[r] = R(13.0 / 12.0) * b1[r] * b1[r] + R(0.25) * b2[r] * b2[r];
+    b1[r] = pfma(u[3 - r], psplat<R>(R(-2)), padd(u[2 - r], u[4 - r]));
+    b2[r] = pfma(psplat<R>(T::brl(r, 0)), u[2 - r],
+                 pfma(psplat<R>(T::brl(r, 1)), u[3 - r], pmul(psplat<R>(T::brl(r, 2)), u[4 - r])));
   }
-  const R diff = beta[0] - beta[2];
-  const R tau = diff >= R(0) ? diff : -diff;
-  const R sg = (diff > R(0)) ? R(1) : ((diff < R(0)) ? R(-1) : R(0));
-  R ib[3];
+  P beta[3];
 #pragma unroll
-  for (int r = 0; r < 3; r++) ib[r] = R(1) / (beta[r] + eps);
-  R lbeta[3] = {R(0), R(0), R(0)};
-  R ltau = R(0);
+  for (int r = 0; r < 3; r++) {
+    beta[r] = pfma(pmul(b1[r], psplat<R>(R(13.0 / 12.0))), b1[r], pmul(pmul(b2[r], psplat<R>(R(0.25))), b2[r]));
+    ib[r] = prcp(padd(beta[r], eps));
+    lbeta[r] = psplat<R>(R(0));
+  }
+  const P diff = psub(beta[0], beta[2]);
+  const P tau = pabs(diff);
+#pragma unroll
+  for (int r = 0; r < 3; r++) tib[r] = pmul(tau, ib[r]);
+  P ltau = psplat<R>(R(0));
 #pragma unroll
   for (int side = 0; side < 2; side++) {
-    const R lam = side ? lam_m : lam_p;
-    R cand[3], alpha[3], S = R(0), num = R(0);
+    const P lam = side ? lam_m : lam_p;
+    P cand[3], alpha[3];
+    P S = psplat<R>(R(0)), num = psplat<R>(R(0));
 #pragma unroll
     for (int r = 0; r < 3; r++) {
-      cand[r] = T::crl(r + side, 0) * u[2 - r] + T::crl(r + side, 1) * u[3 - r] + T::crl(r + side, 2) * u[4 - r];
-      alpha[r] = T::dd(side ? r : 2 - r) * (R(1) + tau * ib[r]);
-      S += alpha[r];
-      num += alpha[r] * cand[r];
+      cand[r] = pfma(psplat<R>(T::crl(r + side, 0)), u[2 - r],
+                     pfma(psplat<R>(T::crl(r + side, 1)), u[3 - r], pmul(psplat<R>(T::crl(r + side, 2)), u[4 - r])));
+      const P d = psplat<R>(T::dd(side ? r : 2 - r));
+      alpha[r] = pfma(d, tib[r], d);
+      S = padd(S, alpha[r]);
+      num = pfma(alpha[r], cand[r], num);
     }
-    const R iS = R(1) / S;
-    const R V = num * iS;
+    const P iS = prcp(S);
+    const P V = pmul(num, iS);
+    const P sl = pmul(iS, lam);
 #pragma unroll
     for (int r = 0; r < 3; r++) {
-      const R lc = alpha[r] * iS * lam;
-      g[2 - r] += T::crl(r + side, 0) * lc;
-      g[3 - r] += T::crl(r + side, 1) * lc;
-      g[4 - r] += T::crl(r + side, 2) * lc;
-      const R la = (cand[r] - V) * iS * lam;
-      const R d = T::dd(side ? r : 2 - r);
-      ltau += d * ib[r] * la;
-      lbeta[r] -= d * tau * ib[r] * ib[r] * la;
+      const P lc = pmul(alpha[r], sl);
+      g[2 - r] = pfma(psplat<R>(T::crl(r + side, 0)), lc, g[2 - r]);
+      g[3 - r] = pfma(psplat<R>(T::crl(r + side, 1)), lc, g[3 - r]);
+      g[4 - r] = pfma(psplat<R>(T::crl(r + side, 2)), lc, g[4 - r]);
+      // t = d ib (cand - V) lam / S: d alpha / d tau and d alpha / d beta share it
+      const P t = pmul(pmul(psplat<R>(T::dd(side ? r : 2 - r)), ib[r]), pmul(psub(cand[r], V), sl));
+      ltau = padd(ltau, t);
+      lbeta[r] = psub(lbeta[r], pmul(t, tib[r]));
     }
   }
-  lbeta[0] += sg * ltau;
-  lbeta[2] -= sg * ltau;
+  // tau = |beta0 - beta2|: subgradient sign(0) = 0
+  const P sl = pmk(diff.x > R(0) ? ltau.x : (diff.x < R(0) ? -ltau.x : R(0)),
+                   diff.y > R(0) ? ltau.y : (diff.y < R(0) ? -ltau.y : R(0)));
+  lbeta[0] = padd(lbeta[0], sl);
+  lbeta[2] = psub(lbeta[2], sl);
 #pragma unroll
   for (int r = 0; r < 3; r++) {
-    const R l1 = R(13.0 / 6.0) * b1[r] * lbeta[r];
-    const R l2 = R(0.5) * b2[r] * lbeta[r];
-    g[2 - r] += l1 + T::brl(r, 0) * l2;
-    g[3 - r] += R(-2) * l1 + T::brl(r, 1) * l2;
-    g[4 - r] += l1 + T::brl(r, 2) * l2;
+    const P l1 = pmul(pmul(b1[r], psplat<R>(R(13.0 / 6.0))), lbeta[r]);
+    const P l2 = pmul(pmul(b2[r], psplat<R>(R(0.5))), lbeta[r]);
+    g[2 - r] = padd(g[2 - r], pfma(psplat<R>(T::brl(r, 0)), l2, l1));
+    g[3 - r] = padd(g[3 - r], pfma(psplat<R>(T::brl(r, 1)), l2, pmul(psplat<R>(R(-2)), l1)));
+    g[4 - r] = padd(g[4 - r], pfma(psplat<R>(T::brl(r, 2)), l2, l1));
   }
+}
+
+// Adjoint of the Godunov flux of a face: the adjoints of its left state (from the face's
+// adjoint lF) and of its right state, each as a (pressure, velocity) pair.
+template <class R>
+__device__ __forceinline__ typename Pair<R>::T god_left(const AdjStageArgs<R>& A, typename Pair<R>::T lF) {
+  return pfma(psplat<R>(A.fc), lF, pmul(pswap(lF), pmk(A.firho, A.frc2)));
+}
+template <class R>
+__device__ __forceinline__ typename Pair<R>::T god_right(const AdjStageArgs<R>& A, typename Pair<R>::T lF) {
+  return pfma(psplat<R>(-A.fc), lF, pmul(pswap(lF), pmk(A.firho, A.frc2)));
 }
 
 // psi tile index of cell (i, j, k) on axis d with tile index t along d (the stage kernel's
@@ -101,246 +128,503 @@ __device__ __forceinline__ int64_t psi_index(const AdjStageArgs<R>& A, int d, in
   return (int64_t)i + (int64_t)A.Nx * ((int64_t)j + (int64_t)A.Ny * t);
 }
 
+// Shared-memory layout of the fused stage adjoint (units of R). Two buffers of raw plane tiles
+// with a 4-cell x/y halo (40 x 24): the stage input p, u, v, the output adjoint lp, lu, lv and the
+// class bytes -- the next plane's arrives while the current one is worked on. Then the
+// flux-difference weights g of the x faces (38 x 16 pairs) and y faces (32 x 22 pairs), and the
+// five stencil contributions of every x centre (36 x 16) and y centre (32 x 20) of the tile and
+// its 2-cell halo.
+template <class R>
+struct AdjSmem {
+  static constexpr int TW = TX + 8, TH = TY + 8, TN = TW * TH;
+  static constexpr int GXW = TX + 6, GYH = TY + 6;
+  static constexpr int XCW = TX + 4, YCH = TY + 4;
+  static constexpr int NX_C = XCW * TY, NY_C = TX * YCH;
+  static constexpr int RAW = 6 * TN;  // p, u, v, lp, lu, lv of one plane
+  static constexpr int G_X = 2 * RAW;
+  static constexpr int G_Y = G_X + 2 * GXW * TY;
+  static constexpr int X_C = G_Y + 2 * TX * GYH;
+  static constexpr int Y_C = X_C + 2 * 5 * NX_C;
+  static constexpr int END = Y_C + 2 * 5 * NY_C;
+  static constexpr size_t CLS_OFF = (size_t)END * sizeof(R);  // two class-byte tiles
+  static constexpr size_t PML_OFF = (CLS_OFF + 2 * TN + 31) & ~(size_t)31;
+  // cPML coefficients of the tile's x range (38), y range (22) and the chunk's z range (chunk + 6)
+  static size_t bytes(int kz_chunk) { return PML_OFF + (size_t)(TX + 6 + TY + 6 + kz_chunk + 6) * sizeof(PmlCoef<R>); }
+};
+
 // Weighted output adjoint of cell (i, j, k) for the flux differences along axis d, as the pair
 // (pressure, velocity d): the coefficient of (F_lo - F_hi) in the cell's outputs (and, in stage 2,
-// in psi^{n+1}) applied to their adjoints. Zero for cells the stage kernel does not update.
+// in psi^{n+1}) applied to their adjoints; lp, lvel are the cell's output adjoints, pc its cPML
+// coefficient along d. Zero for cells the stage kernel does not update.
 template <class R>
-__device__ __forceinline__ void adj_g(const AdjStageArgs<R>& A, int d, int i, int j, int k, R& gp, R& gv) {
+__device__ __forceinline__ void adj_g_local(const AdjStageArgs<R>& A, int d, int i, int j, int k, uint8_t cls,
+                                            R lp, R lvel, const PmlCoef<R>& pc, R& gp, R& gv) {
   typedef typename Pair<R>::T P;
-  const int64_t c = XOFF + i + A.Sx * ((int64_t)j + (int64_t)A.Ny * k);
   gp = R(0);
   gv = R(0);
-  if (!(A.cls[c] & CLS_UPDATE)) return;
-  const R* lvel = (d == 0) ? A.lu : (d == 1) ? A.lv : A.lw;
+  if (!(cls & CLS_UPDATE)) return;
   R coef = A.cb;
-  if (A.pml_on) {
-    const PmlCoef<R> pc = (d == 0) ? A.pcx[i] : (d == 1) ? A.pcy[j] : A.pcz[k];
-    if (pc.tile >= 0) {
-      coef += A.wdt * pc.kinv1 * A.inv_h;
-      if (A.stage == 2) {
-        const P* lpsi = (d == 0) ? A.lpsix : (d == 1) ? A.lpsiy : A.lpsiz;
-        const P l = lpsi[psi_index(A, d, i, j, k, pc.tile)];
-        gp = pc.ca * A.inv_h * l.x;
-        gv = pc.ca * A.inv_h * l.y;
-      }
+  if (A.pml_on && pc.tile >= 0) {
+    coef += A.wdt * pc.kinv1 * A.inv_h;
+    if (A.stage == 2) {
+      const P* lpsi = (d == 0) ? A.lpsix : (d == 1) ? A.lpsiy : A.lpsiz;
+      const P l = lpsi[psi_index(A, d, i, j, k, pc.tile)];
+      gp = pc.ca * A.inv_h * l.x;
+      gv = pc.ca * A.inv_h * l.y;
     }
   }
-  gp += coef * A.lp[c];
-  gv += coef * lvel[c];
+  gp += coef * lp;
+  gv += coef * lvel;
 }
 
+// Adjoint of one stage kernel launch. CTA = 32 x 16 columns marching up a z chunk, as the forward
+// stage kernel. At centre plane kc: the x and y centres of the tile and its 2-cell halo through
+// shared memory (each centre's five contributions written once, then gathered by the five cells
+// they land on), the z centre of every column (register queues of p, w and of the z weights),
+// and the flush of plane kc - 2, whose z contributions are complete once centre kc is done. The
+// global loads of the next plane, of the z queues and of the flush are issued at the top of the
+// iteration and consumed after the x/y work.
 template <class R>
-__global__ void __launch_bounds__(256) k_adj_centres(const AdjStageArgs<R> A) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
-  if (i >= A.Nx || j >= A.Ny || k >= A.Nz) return;
-  const int64_t c = XOFF + i + A.Sx * ((int64_t)j + (int64_t)A.Ny * k);
-  const int64_t st[3] = {1, A.Sx, A.plane};
-  const int N[3] = {A.Nx, A.Ny, A.Nz};
-  const int cd[3] = {i, j, k};
-  for (int d = 0; d < 3; d++) {
-    R gP[5] = {R(0), R(0), R(0), R(0), R(0)};
-    R gV[5] = {R(0), R(0), R(0), R(0), R(0)};
-    if (cd[d] >= 2 && cd[d] <= N[d] - 3) {
-      R gpm, gvm, gp0, gv0, gpp, gvp;
-      const int di = (d == 0), dj = (d == 1), dk = (d == 2);
-      adj_g(A, d, i - di, j - dj, k - dk, gpm, gvm);
-      adj_g(A, d, i, j, k, gp0, gv0);
-      adj_g(A, d, i + di, j + dj, k + dk, gpp, gvp);
-      if (gpm != R(0) || gvm != R(0) || gp0 != R(0) || gv0 != R(0) || gpp != R(0) || gvp != R(0)) {
-        // face adjoints: F(c+1/2) enters L(c) with -1 and L(c+1) with +1
-        const R lFp_hi = gpp - gp0, lFu_hi = gvp - gv0;
-        const R lFp_lo = gp0 - gpm, lFu_lo = gv0 - gvm;
-        // V-(c+1/2) is the left state of face c+1/2, V+(c-1/2) the right state of face c-1/2
-        const R lpm = A.fc * lFp_hi + A.firho * lFu_hi;
-        const R lum = A.frc2 * lFp_hi + A.fc * lFu_hi;
-        const R lpp = -A.fc * lFp_lo + A.firho * lFu_lo;
-        const R lup = A.frc2 * lFp_lo - A.fc * lFu_lo;
-        const R* vel = (d == 0) ? A.ui : (d == 1) ? A.vi : A.wi;
-        R up[5], uv[5];
-#pragma unroll
-        for (int q = 0; q < 5; q++) {
-          up[q] = A.pi[c + (q - 2) * st[d]];
-          uv[q] = vel[c + (q - 2) * st[d]];
-        }
-        weno_centre_rev<R>(up, lpm, lpp, gP);
-        weno_centre_rev<R>(uv, lum, lup, gV);
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < 5; q++) {
-      A.contrib[(int64_t)((d * 5 + q) * 2 + 0) * A.ncell + c] = gP[q];
-      A.contrib[(int64_t)((d * 5 + q) * 2 + 1) * A.ncell + c] = gV[q];
-    }
-  }
-}
-
-template <class R>
-__global__ void __launch_bounds__(256) k_adj_gather(const AdjStageArgs<R> A) {
+__global__ void __launch_bounds__(NTHREADS, 1) k_adj_stage(const AdjStageArgs<R> A) {
   typedef typename Pair<R>::T P;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
-  if (i >= A.Nx || j >= A.Ny || k >= A.Nz) return;
-  const int64_t c = XOFF + i + A.Sx * ((int64_t)j + (int64_t)A.Ny * k);
-  const int64_t st[3] = {1, A.Sx, A.plane};
-  const int N[3] = {A.Nx, A.Ny, A.Nz};
-  const int cd[3] = {i, j, k};
-  R sp = R(0), sv[3] = {R(0), R(0), R(0)};
-  for (int d = 0; d < 3; d++) {
+  typedef AdjSmem<R> S;
+  extern __shared__ __align__(16) unsigned char adj_smem[];
+  R* sm = reinterpret_cast<R*>(adj_smem);
+  P* gX = reinterpret_cast<P*>(sm + S::G_X);
+  P* gY = reinterpret_cast<P*>(sm + S::G_Y);
+  P* xC = reinterpret_cast<P*>(sm + S::X_C);
+  P* yC = reinterpret_cast<P*>(sm + S::Y_C);
+  uint8_t* clsT = adj_smem + S::CLS_OFF;
+  PmlCoef<R>* sPx = reinterpret_cast<PmlCoef<R>*>(adj_smem + S::PML_OFF);  // x = i0 - 3 + q
+  PmlCoef<R>* sPy = sPx + (TX + 6);                                         // y = j0 - 3 + q
+  PmlCoef<R>* sPz = sPy + (TY + 6);                                         // k = kb - 3 + q
+
+  const int tx = threadIdx.x, ty = threadIdx.y, lt = ty * TX + tx;
+  const int i0 = GHOST + blockIdx.x * TX, j0 = GHOST + blockIdx.y * TY;
+  const int i = i0 + tx, j = j0 + ty;
+  const int kb = GHOST + blockIdx.z * A.kz_chunk;
+  const int ke = min(kb + A.kz_chunk, A.Nz - GHOST);
+  if (kb >= ke) return;
+  const int Nx = A.Nx, Ny = A.Ny, Nz = A.Nz;
+  const int64_t Sx = A.Sx, plane = A.plane;
+  const bool col_in = (i < Nx) && (j < Ny);
+  const bool valid = (i < Nx - GHOST) && (j < Ny - GHOST);
+  const int64_t col = XOFF + i + Sx * (int64_t)j;
+
+  // raw-tile elements of this thread: e = lt and e = lt + 512 (when < 960)
+  constexpr int NE = (S::TN + NTHREADS - 1) / NTHREADS;
+  int64_t roff[NE];
+  bool rin[NE];
 #pragma unroll
-    for (int q = 0; q < 5; q++) {
-      const int src = cd[d] - (q - 2);  // the centre whose offset q - 2 lands on this cell
-      if (src < 0 || src >= N[d]) continue;
-      const int64_t cc = c - (q - 2) * st[d];
-      sp += A.contrib[(int64_t)((d * 5 + q) * 2 + 0) * A.ncell + cc];
-      sv[d] += A.contrib[(int64_t)((d * 5 + q) * 2 + 1) * A.ncell + cc];
-    }
+  for (int q = 0; q < NE; q++) {
+    const int e = lt + q * NTHREADS;
+    const int r = e / S::TW, ci = e - r * S::TW;
+    const int x = i0 - 4 + ci, y = j0 - 4 + r;
+    rin[q] = (e < S::TN) && x >= 0 && x < Nx && y >= 0 && y < Ny;
+    roff[q] = rin[q] ? (XOFF + x + Sx * (int64_t)y) : 0;
   }
-  R ap = sp, au = sv[0], av = sv[1], aw = sv[2];
-  if (A.cls[c] & CLS_UPDATE) {
-    const R Lp = A.lp[c], Lu = A.lu[c], Lv = A.lv[c], Lw = A.lw[c];
-    ap += A.b_in * Lp;
-    au += A.b_in * Lu;
-    av += A.b_in * Lv;
-    aw += A.b_in * Lw;
-    if (A.stage > 0) {
-      A.bp[c] += A.a_base * Lp;
-      A.bu[c] += A.a_base * Lu;
-      A.bv[c] += A.a_base * Lv;
-      A.bw[c] += A.a_base * Lw;
+  R pre[NE][6];
+  uint8_t prc[NE];
+  auto prefetch = [&](int k) {
+#pragma unroll
+    for (int q = 0; q < NE; q++) {
+      const bool ok = rin[q] && k < Nz;
+      const int64_t g = roff[q] + plane * (int64_t)k;
+      pre[q][0] = ok ? A.pi[g] : R(0);
+      pre[q][1] = ok ? A.ui[g] : R(0);
+      pre[q][2] = ok ? A.vi[g] : R(0);
+      pre[q][3] = ok ? A.lp[g] : R(0);
+      pre[q][4] = ok ? A.lu[g] : R(0);
+      pre[q][5] = ok ? A.lv[g] : R(0);
+      prc[q] = ok ? A.cls[g] : (uint8_t)0;
     }
-    if (A.pml_on) {
-      const PmlCoef<R> pc[3] = {A.pcx[i], A.pcy[j], A.pcz[k]};
-      const R Lvel[3] = {Lu, Lv, Lw};
-      P* lpsi[3] = {A.lpsix, A.lpsiy, A.lpsiz};
-      for (int d = 0; d < 3; d++) {
-        if (pc[d].tile < 0) continue;
-        const int64_t x = psi_index(A, d, i, j, k, pc[d].tile);
-        P l = lpsi[d][x];
-        if (A.stage == 2) {  // psi^{n+1} = b psi^n + ca D: carry b, then psi^n's own uses
-          l.x *= pc[d].b;
-          l.y *= pc[d].b;
-        }
-        l.x += A.wdt * Lp;
-        l.y += A.wdt * Lvel[d];
-        lpsi[d][x] = l;
+  };
+  auto stash = [&](int buf) {
+    R* raw = sm + buf * S::RAW;
+#pragma unroll
+    for (int q = 0; q < NE; q++) {
+      const int e = lt + q * NTHREADS;
+      if (e < S::TN) {
+#pragma unroll
+        for (int f = 0; f < 6; f++) raw[f * S::TN + e] = pre[q][f];
+        clsT[buf * S::TN + e] = prc[q];
       }
     }
+  };
+  auto ldz = [&](const R* f, int k) -> R { return (col_in && k >= 0 && k < Nz) ? f[col + plane * k] : R(0); };
+
+  // z queues at centre plane kc: values at kc-2 .. kc+2, weights at kc-1 .. kc+1, contribution
+  // windows for planes kc-2 .. kc+2
+  P zq[5], gzq[3], acq[5];  // (p, w) pairs
+#pragma unroll
+  for (int q = 0; q < 4; q++) zq[q] = pmk(ldz(A.pi, kb - 4 + q), ldz(A.wi, kb - 4 + q));
+  {
+    PmlCoef<R> none;
+    none.tile = -1;
+    none.kinv1 = none.b = none.ca = R(0);
+    const int nz_t = A.kz_chunk + 6;
+    for (int e = lt; e < TX + 6 + TY + 6 + nz_t; e += NTHREADS) {
+      PmlCoef<R> c = none;
+      if (e < TX + 6) {
+        const int x = i0 - 3 + e;
+        if (x >= 0 && x < Nx) c = A.pcx[x];
+      } else if (e < TX + 6 + TY + 6) {
+        const int y = j0 - 3 + (e - (TX + 6));
+        if (y >= 0 && y < Ny) c = A.pcy[y];
+      } else {
+        const int k = kb - 3 + (e - (TX + 6 + TY + 6));
+        if (k >= 0 && k < Nz) c = A.pcz[k];
+      }
+      sPx[e] = c;
+    }
   }
-  A.ip[c] += ap;
-  A.iu[c] += au;
-  A.iv[c] += av;
-  A.iw[c] += aw;
+  __syncthreads();
+  const PmlCoef<R> pci = sPx[tx + 3], pcj = sPy[ty + 3];
+  auto gz_cell = [&](int k) -> P {
+    R gp = R(0), gv = R(0);
+    if (col_in && k >= 0 && k < Nz) {
+      const int64_t c = col + plane * (int64_t)k;
+      adj_g_local(A, 2, i, j, k, A.cls[c], A.lp[c], A.lw[c], sPz[k - kb + 3], gp, gv);
+    }
+    return pmk(gp, gv);
+  };
+  gzq[0] = gz_cell(kb - 3);
+  gzq[1] = gz_cell(kb - 2);
+#pragma unroll
+  for (int q = 0; q < 5; q++) acq[q] = psplat<R>(R(0));
+  R d1p = R(0), d1u = R(0), d1v = R(0), d2p = R(0), d2u = R(0), d2v = R(0);  // x/y sums of kc-1, kc-2
+
+  prefetch(kb);
+  stash(kb & 1);
+
+  const int nit = (ke - kb) + 4;
+  for (int it = 0; it < nit; ++it) {
+    const int kc = kb - 2 + it;
+    const bool xy = (kc >= kb && kc < ke);  // block-uniform
+    // ---- loads for later in this iteration and for the next plane
+    zq[4] = pmk(ldz(A.pi, kc + 2), ldz(A.wi, kc + 2));
+    const int kz1 = kc + 1;
+    const bool z1 = col_in && kz1 >= 0 && kz1 < Nz;
+    const int64_t cz1 = col + plane * (int64_t)kz1;
+    const uint8_t cls_z1 = z1 ? A.cls[cz1] : (uint8_t)0;
+    const R lpz1 = z1 ? A.lp[cz1] : R(0), lwz1 = z1 ? A.lw[cz1] : R(0);
+    const int kf = kc - 2;
+    const bool fl = (kf >= kb) && valid;
+    const int64_t cf = col + plane * (int64_t)kf;
+    const uint8_t cls_f = fl ? A.cls[cf] : (uint8_t)0;
+    R Lf[4] = {R(0), R(0), R(0), R(0)};
+    R Pf[4] = {R(0), R(0), R(0), R(0)};  // the accumulator this stage adds to (input or U0 adjoint)
+    if (fl) {
+      Lf[0] = A.lp[cf];
+      Lf[1] = A.lu[cf];
+      Lf[2] = A.lv[cf];
+      Lf[3] = A.lw[cf];
+      if (A.acc_in) {
+        Pf[0] = A.ip[cf];
+        Pf[1] = A.iu[cf];
+        Pf[2] = A.iv[cf];
+        Pf[3] = A.iw[cf];
+      } else if (A.acc_base) {
+        Pf[0] = A.bp[cf];
+        Pf[1] = A.bu[cf];
+        Pf[2] = A.bv[cf];
+        Pf[3] = A.bw[cf];
+      }
+    }
+    const bool nxt = (kc + 1 >= kb && kc + 1 < ke && kc + 1 > kb);  // plane kb is already stashed
+    if (nxt) prefetch(kc + 1);
+
+    // ---- x and y centres of plane kc
+    R xyp = R(0), xyu = R(0), xyv = R(0);
+    if (xy) {
+      __syncthreads();  // raw tiles of plane kc stashed; previous plane's shared data consumed
+      const R* raw = sm + (kc & 1) * S::RAW;
+      const R* tP = raw;
+      const R* tU = raw + S::TN;
+      const R* tV = raw + 2 * S::TN;
+      const R* tLp = raw + 3 * S::TN;
+      const R* tLu = raw + 4 * S::TN;
+      const R* tLv = raw + 5 * S::TN;
+      const uint8_t* tC = clsT + (kc & 1) * S::TN;
+      for (int e = lt; e < S::GXW * TY + TX * S::GYH; e += NTHREADS) {
+        R a, b;
+        if (e < S::GXW * TY) {
+          const int r = e / S::GXW, ci = e - r * S::GXW;
+          const int t = (r + 4) * S::TW + ci + 1;
+          adj_g_local(A, 0, i0 - 3 + ci, j0 + r, kc, tC[t], tLp[t], tLu[t], sPx[ci], a, b);
+          gX[e] = pmk(a, b);
+        } else {
+          const int f = e - S::GXW * TY;
+          const int r = f / TX, ci = f - r * TX;
+          const int t = (r + 1) * S::TW + ci + 4;
+          adj_g_local(A, 1, i0 + ci, j0 - 3 + r, kc, tC[t], tLp[t], tLv[t], sPy[r], a, b);
+          gY[f] = pmk(a, b);
+        }
+      }
+      __syncthreads();
+      for (int e = lt; e < S::NX_C + S::NY_C; e += NTHREADS) {
+        P cc[5];
+#pragma unroll
+        for (int q = 0; q < 5; q++) cc[q] = psplat<R>(R(0));
+        const bool isx = e < S::NX_C;
+        const int f = isx ? e : e - S::NX_C;
+        int r, ci, cpos, npos;
+        P gm, g0, gp;
+        if (isx) {
+          r = f / S::XCW;
+          ci = f - r * S::XCW;
+          cpos = i0 - 2 + ci;
+          npos = Nx;
+          gm = gX[r * S::GXW + ci];
+          g0 = gX[r * S::GXW + ci + 1];
+          gp = gX[r * S::GXW + ci + 2];
+        } else {
+          r = f / TX;
+          ci = f - r * TX;
+          cpos = j0 - 2 + r;
+          npos = Ny;
+          gm = gY[r * TX + ci];
+          g0 = gY[(r + 1) * TX + ci];
+          gp = gY[(r + 2) * TX + ci];
+        }
+        if (cpos >= 2 && cpos <= npos - 3) {
+          // face adjoints: F(c+1/2) enters L(c) with -1 and L(c+1) with +1
+          const P lF_hi = psub(gp, g0), lF_lo = psub(g0, gm);
+          if (lF_hi.x != R(0) || lF_hi.y != R(0) || lF_lo.x != R(0) || lF_lo.y != R(0)) {
+            // stencil cpos-2 .. cpos+2: tile columns ci .. ci+4 of row r+4 (x), or rows r .. r+4 of
+            // column ci+4 (y)
+            const int t0 = isx ? (r + 4) * S::TW + ci : r * S::TW + ci + 4;
+            const int st = isx ? 1 : S::TW;
+            const R* tw = isx ? tU : tV;
+            P uq[5];
+#pragma unroll
+            for (int q = 0; q < 5; q++) uq[q] = pmk(tP[t0 + q * st], tw[t0 + q * st]);
+            // V-(c+1/2) is the left state of face c+1/2, V+(c-1/2) the right state of face c-1/2
+            weno_centre_rev<R>(uq, god_left(A, lF_hi), god_right(A, lF_lo), cc);
+          }
+        }
+        P* dst = isx ? xC + f * 5 : yC + f * 5;
+#pragma unroll
+        for (int q = 0; q < 5; q++) dst[q] = cc[q];
+      }
+      __syncthreads();
+      // cell (i, j) receives offset q - 2 of the x centre i - (q - 2) and of the y centre j - (q - 2)
+#pragma unroll
+      for (int q = 0; q < 5; q++) {
+        const P a = xC[(ty * S::XCW + tx + 4 - q) * 5 + q];
+        const P b = yC[((ty + 4 - q) * TX + tx) * 5 + q];
+        xyp += a.x + b.x;
+        xyu += a.y;
+        xyv += b.y;
+      }
+    }
+    // ---- z centre kc
+    {
+      R gp, gv;
+      adj_g_local(A, 2, i, j, kz1, cls_z1, lpz1, lwz1, sPz[kz1 - kb + 3], gp, gv);
+      gzq[2] = pmk(gp, gv);
+    }
+    if (col_in && kc >= 2 && kc <= Nz - 3) {
+      const P lF_hi = psub(gzq[2], gzq[1]), lF_lo = psub(gzq[1], gzq[0]);
+      if (lF_hi.x != R(0) || lF_hi.y != R(0) || lF_lo.x != R(0) || lF_lo.y != R(0))
+        weno_centre_rev<R>(zq, god_left(A, lF_hi), god_right(A, lF_lo), acq);
+    }
+    // ---- flush plane kc - 2: the stage input's adjoint (and U0's) at every interior cell
+    if (fl) {
+      R ip = d2p + acq[0].x, iu = d2u, iv = d2v, iw = acq[0].y;
+      R bq[4] = {R(0), R(0), R(0), R(0)};
+      if (cls_f & CLS_UPDATE) {
+        ip += A.b_in * Lf[0];
+        iu += A.b_in * Lf[1];
+        iv += A.b_in * Lf[2];
+        iw += A.b_in * Lf[3];
+#pragma unroll
+        for (int f = 0; f < 4; f++) bq[f] = A.a_base * Lf[f];
+        if (A.pml_on) {
+          const PmlCoef<R> pc[3] = {pci, pcj, sPz[kf - kb + 3]};
+          const P* lin[3] = {A.lpsix, A.lpsiy, A.lpsiz};
+          P* lout[3] = {A.opsix, A.opsiy, A.opsiz};
+#pragma unroll
+          for (int d = 0; d < 3; d++) {
+            if (pc[d].tile < 0) continue;
+            const int64_t x = psi_index(A, d, i, j, kf, pc[d].tile);
+            P l;
+            if (A.stage == 2) {  // psi^{n+1} = b psi^n + ca D: carry b, then psi^n's own uses
+              const P o = lin[d][x];
+              l = pmk(pc[d].b * o.x, pc[d].b * o.y);
+            } else {
+              l = lout[d][x];
+            }
+            l.x += A.wdt * Lf[0];
+            l.y += A.wdt * Lf[1 + d];
+            lout[d][x] = l;
+          }
+        }
+      }
+      if (A.acc_in) {
+        ip += Pf[0];
+        iu += Pf[1];
+        iv += Pf[2];
+        iw += Pf[3];
+      }
+      A.ip[cf] = ip;
+      A.iu[cf] = iu;
+      A.iv[cf] = iv;
+      A.iw[cf] = iw;
+      if (A.stage > 0) {
+        if (A.acc_base) {
+#pragma unroll
+          for (int f = 0; f < 4; f++) bq[f] += Pf[f];
+        }
+        A.bp[cf] = bq[0];
+        A.bu[cf] = bq[1];
+        A.bv[cf] = bq[2];
+        A.bw[cf] = bq[3];
+      }
+    }
+    // ---- the next plane's raw tiles (its buffer was last read before this iteration's barriers)
+    if (nxt) stash((kc + 1) & 1);
+    // ---- advance the queues
+    d2p = d1p; d2u = d1u; d2v = d1v;
+    d1p = xyp; d1u = xyu; d1v = xyv;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      zq[q] = zq[q + 1];
+      acq[q] = acq[q + 1];
+    }
+    acq[4] = psplat<R>(R(0));
+    gzq[0] = gzq[1];
+    gzq[1] = gzq[2];
+  }
 }
 
+// One thread per band cell. Each cell's contributions to the coefficient gradients go to its own
+// slots gcell[e][b] (no atomics); k_adj_grad_reduce sums them per material once, at the end.
 template <class R, int STAGE>
-__global__ void __launch_bounds__(256) k_adj_band(const AdjBandArgs<R> B, int use_smem) {
-  extern __shared__ double sgrad[];
-  const int P = 1 + 2 * B.K + 4 * B.L;
-  const int ng = B.nMat * P;
-  if (use_smem) {
-    for (int e = threadIdx.x; e < ng; e += blockDim.x) sgrad[e] = 0.0;
-    __syncthreads();
-  }
+__global__ void __launch_bounds__(256) k_adj_band(const AdjBandArgs<R> B) {
   const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (b < B.nB) {
-    double* gacc = use_smem ? sgrad : B.grad;
-    const int4 rc = B.rec[b];
-    const int64_t cell = (int64_t)(((uint64_t)(uint32_t)rc.y << 32) | (uint32_t)rc.x);
-    const int64_t q = cell + rc.z;
-    const int m = rc.w;
-    const R sx = B.geo[4 * b + 0], sy = B.geo[4 * b + 1], sz = B.geo[4 * b + 2], chi = B.geo[4 * b + 3];
-    const R nx = B.nrm[4 * b + 0], ny = B.nrm[4 * b + 1], nz = B.nrm[4 * b + 2];
-    const int64_t Sx = B.Sx, pl = B.plane;
-    const int64_t off[8] = {0, 1, Sx, Sx + 1, pl, pl + 1, pl + Sx, pl + Sx + 1};
-    const R wt[8] = {(R(1) - sx) * (R(1) - sy) * (R(1) - sz), sx * (R(1) - sy) * (R(1) - sz),
-                     (R(1) - sx) * sy * (R(1) - sz),           sx * sy * (R(1) - sz),
-                     (R(1) - sx) * (R(1) - sy) * sz,           sx * (R(1) - sy) * sz,
-                     (R(1) - sx) * sy * sz,                    sx * sy * sz};
-    // forward values needed by the linearisation (the probe as the forward evaluates it)
-    auto tri = [&](const R* f) {
-      const R c00 = f[q] * (R(1) - sx) + f[q + 1] * sx;
-      const R c10 = f[q + Sx] * (R(1) - sx) + f[q + Sx + 1] * sx;
-      const R c01 = f[q + pl] * (R(1) - sx) + f[q + pl + 1] * sx;
-      const R c11 = f[q + pl + Sx] * (R(1) - sx) + f[q + pl + Sx + 1] * sx;
-      const R c0 = c00 * (R(1) - sy) + c10 * sy, c1 = c01 * (R(1) - sy) + c11 * sy;
-      return c0 * (R(1) - sz) + c1 * sz;
-    };
-    const R pD = tri(B.pi), uD = tri(B.ui), vD = tri(B.vi), wD = tri(B.wi);
-    const R un = uD * nx + vD * ny + wD * nz;
-    const double Z0 = B.Z0, dt = B.dt;
-    const double wout = (double)pD + Z0 * (double)un;
-    constexpr double aa = (STAGE == 0) ? 0.0 : (STAGE == 1) ? 3.0 : 1.0;
-    constexpr double bb = (STAGE == 2) ? 2.0 : 1.0;
-    constexpr double ic = (STAGE == 0) ? 1.0 : (STAGE == 1) ? 0.25 : 1.0 / 3.0;
-    // output adjoint at the band cell: blend out = (1 - chi) pre + chi (pb, ub)
-    const R Lp = B.lp[cell], Lu = B.lu[cell], Lv = B.lv[cell], Lw = B.lw[cell];
-    const R omc = R(1) - chi;
-    B.lp[cell] = omc * Lp;
-    B.lu[cell] = omc * Lu;
-    B.lv[cell] = omc * Lv;
-    B.lw[cell] = omc * Lw;
-    const double lpb = (double)chi * Lp;
-    const double lux = (double)chi * Lu, luy = (double)chi * Lv, luz = (double)chi * Lw;
-    const double lunb = nx * lux + ny * luy + nz * luz;
-    const double lwin = 0.5 * lpb - lunb / (2.0 * Z0);
-    double lwout = 0.5 * lpb + lunb / (2.0 * Z0);
-    double* g = gacc + (int64_t)m * P;
-    const int64_t nB = B.nB;
-    atomicAdd(&g[0], wout * lwin);
-    lwout += B.Rinf[m] * lwin;
-    for (int k = 0; k < B.K; ++k) {
-      const int mi = m * B.K + k;
-      const int64_t si = (int64_t)k * nB + b;
-      const double lphi = B.gphL[si] + B.A[mi] * lwin;
-      const double phR = B.phR[si];
-      atomicAdd(&g[1 + k], B.phL[si] * lwin);
-      atomicAdd(&g[1 + B.K + k], -bb * dt * phR * ic * lphi);
-      B.gphR[si] += bb * (1.0 - dt * B.zeta[mi]) * ic * lphi;
-      if (STAGE > 0) B.gphM[si] += aa * ic * lphi;
-      lwout += bb * dt * ic * lphi;
+  if (b >= B.nB) return;
+  const int4 rc = B.rec[b];
+  const int64_t cell = (int64_t)(((uint64_t)(uint32_t)rc.y << 32) | (uint32_t)rc.x);
+  const int64_t q = cell + rc.z;
+  const int m = rc.w;
+  const int64_t nB = B.nB;
+  double* gc = B.gcell + b;
+  auto gadd = [&](int e, double v) { gc[(int64_t)e * nB] += v; };
+  const R sx = B.geo[4 * b + 0], sy = B.geo[4 * b + 1], sz = B.geo[4 * b + 2], chi = B.geo[4 * b + 3];
+  const R nx = B.nrm[4 * b + 0], ny = B.nrm[4 * b + 1], nz = B.nrm[4 * b + 2];
+  const int64_t Sx = B.Sx, pl = B.plane;
+  // forward values needed by the linearisation (the probe as the forward evaluates it)
+  auto tri = [&](const R* f) {
+    const R c00 = f[q] * (R(1) - sx) + f[q + 1] * sx;
+    const R c10 = f[q + Sx] * (R(1) - sx) + f[q + Sx + 1] * sx;
+    const R c01 = f[q + pl] * (R(1) - sx) + f[q + pl + 1] * sx;
+    const R c11 = f[q + pl + Sx] * (R(1) - sx) + f[q + pl + Sx + 1] * sx;
+    const R c0 = c00 * (R(1) - sy) + c10 * sy, c1 = c01 * (R(1) - sy) + c11 * sy;
+    return c0 * (R(1) - sz) + c1 * sz;
+  };
+  const R pD = tri(B.pi), uD = tri(B.ui), vD = tri(B.vi), wD = tri(B.wi);
+  const R un = uD * nx + vD * ny + wD * nz;
+  const double Z0 = B.Z0, dt = B.dt;
+  const double wout = (double)pD + Z0 * (double)un;
+  constexpr double aa = (STAGE == 0) ? 0.0 : (STAGE == 1) ? 3.0 : 1.0;
+  constexpr double bb = (STAGE == 2) ? 2.0 : 1.0;
+  constexpr double ic = (STAGE == 0) ? 1.0 : (STAGE == 1) ? 0.25 : 1.0 / 3.0;
+  // output adjoint at the band cell: blend out = (1 - chi) pre + chi (pb, ub)
+  const R Lp = B.lp[cell], Lu = B.lu[cell], Lv = B.lv[cell], Lw = B.lw[cell];
+  const R omc = R(1) - chi;
+  B.lp[cell] = omc * Lp;
+  B.lu[cell] = omc * Lu;
+  B.lv[cell] = omc * Lv;
+  B.lw[cell] = omc * Lw;
+  const double lpb = (double)chi * Lp;
+  const double lux = (double)chi * Lu, luy = (double)chi * Lv, luz = (double)chi * Lw;
+  const double lunb = nx * lux + ny * luy + nz * luz;
+  const double lwin = 0.5 * lpb - lunb / (2.0 * Z0);
+  double lwout = 0.5 * lpb + lunb / (2.0 * Z0);
+  gadd(0, wout * lwin);
+  lwout += B.Rinf[m] * lwin;
+  for (int k = 0; k < B.K; ++k) {
+    const int mi = m * B.K + k;
+    const int64_t si = (int64_t)k * nB + b;
+    const double lphi = B.gphL[si] + B.A[mi] * lwin;
+    const double phR = B.phR[si];
+    gadd(1 + k, B.phL[si] * lwin);
+    gadd(1 + B.K + k, -bb * dt * phR * ic * lphi);
+    B.gphR[si] += bb * (1.0 - dt * B.zeta[mi]) * ic * lphi;
+    if (STAGE > 0) B.gphM[si] += aa * ic * lphi;
+    lwout += bb * dt * ic * lphi;
+  }
+  const int o = 1 + 2 * B.K;
+  for (int l = 0; l < B.L; ++l) {
+    const int mi = m * B.L + l;
+    const int64_t si = (int64_t)l * nB + b;
+    const double l1 = B.gs1L[si] + B.B[mi] * lwin;
+    const double l2 = B.gs2L[si] + B.C[mi] * lwin;
+    const double r1 = B.s1R[si], r2 = B.s2R[si];
+    const double al = B.alpha[mi], be = B.beta[mi];
+    const double kd = bb * dt * ic;
+    gadd(o + l, B.s1L[si] * lwin);
+    gadd(o + B.L + l, B.s2L[si] * lwin);
+    gadd(o + 2 * B.L + l, kd * (-r1 * l1 - r2 * l2));
+    gadd(o + 3 * B.L + l, kd * (-r2 * l1 + r1 * l2));
+    B.gs1R[si] += bb * ic * l1 - kd * al * l1 + kd * be * l2;
+    B.gs2R[si] += -kd * be * l1 + bb * ic * l2 - kd * al * l2;
+    if (STAGE > 0) {
+      B.gs1M[si] += aa * ic * l1;
+      B.gs2M[si] += aa * ic * l2;
     }
-    const int o = 1 + 2 * B.K;
-    for (int l = 0; l < B.L; ++l) {
-      const int mi = m * B.L + l;
-      const int64_t si = (int64_t)l * nB + b;
-      const double l1 = B.gs1L[si] + B.B[mi] * lwin;
-      const double l2 = B.gs2L[si] + B.C[mi] * lwin;
-      const double r1 = B.s1R[si], r2 = B.s2R[si];
-      const double al = B.alpha[mi], be = B.beta[mi];
-      const double kd = bb * dt * ic;
-      atomicAdd(&g[o + l], B.s1L[si] * lwin);
-      atomicAdd(&g[o + B.L + l], B.s2L[si] * lwin);
-      atomicAdd(&g[o + 2 * B.L + l], kd * (-r1 * l1 - r2 * l2));
-      atomicAdd(&g[o + 3 * B.L + l], kd * (-r2 * l1 + r1 * l2));
-      B.gs1R[si] += bb * ic * l1 - kd * al * l1 + kd * be * l2;
-      B.gs2R[si] += -kd * be * l1 + bb * ic * l2 - kd * al * l2;
-      if (STAGE > 0) {
-        B.gs1M[si] += aa * ic * l1;
-        B.gs2M[si] += aa * ic * l2;
-      }
-      lwout += kd * l1;
-    }
-    // wout = pD + Z0 un; ub = unb n + (uD - un n)
-    const double lun = Z0 * lwout - (nx * lux + ny * luy + nz * luz);
-    const R lpD = (R)lwout;
-    const R luD = (R)(lux + lun * nx), lvD = (R)(luy + lun * ny), lwD = (R)(luz + lun * nz);
+    lwout += kd * l1;
+  }
+  // wout = pD + Z0 un; ub = unb n + (uD - un n)
+  const double lun = Z0 * lwout - (nx * lux + ny * luy + nz * luz);
+  const R lpD = (R)lwout;
+  const R luD = (R)(lux + lun * nx), lvD = (R)(luy + lun * ny), lwD = (R)(luz + lun * nz);
+  // the probe's adjoint, scattered into the stage input's adjoint after the stage adjoint
+  B.probe[b] = lpD;
+  B.probe[nB + b] = luD;
+  B.probe[2 * nB + b] = lvD;
+  B.probe[3 * nB + b] = lwD;
+}
+
+// Transposed trilinear probe: adds each band cell's probe adjoint to the 8 corner cells of the
+// stage input's adjoint (corners of neighbouring band cells overlap, hence the atomics).
+template <class R>
+__global__ void __launch_bounds__(256) k_adj_probe_scatter(const AdjBandArgs<R> B) {
+  const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B.nB) return;
+  const int4 rc = B.rec[b];
+  const int64_t cell = (int64_t)(((uint64_t)(uint32_t)rc.y << 32) | (uint32_t)rc.x);
+  const int64_t q = cell + rc.z;
+  const R sx = B.geo[4 * b + 0], sy = B.geo[4 * b + 1], sz = B.geo[4 * b + 2];
+  const int64_t nB = B.nB, Sx = B.Sx, pl = B.plane;
+  const R lpD = B.probe[b], luD = B.probe[nB + b], lvD = B.probe[2 * nB + b], lwD = B.probe[3 * nB + b];
+  const int64_t off[8] = {0, 1, Sx, Sx + 1, pl, pl + 1, pl + Sx, pl + Sx + 1};
+  const R wt[8] = {(R(1) - sx) * (R(1) - sy) * (R(1) - sz), sx * (R(1) - sy) * (R(1) - sz),
+                   (R(1) - sx) * sy * (R(1) - sz),           sx * sy * (R(1) - sz),
+                   (R(1) - sx) * (R(1) - sy) * sz,           sx * (R(1) - sy) * sz,
+                   (R(1) - sx) * sy * sz,                    sx * sy * sz};
 #pragma unroll
-    for (int e = 0; e < 8; e++) {
-      const int64_t x = q + off[e];
-      atomicAdd(B.ip + x, wt[e] * lpD);
-      atomicAdd(B.iu + x, wt[e] * luD);
-      atomicAdd(B.iv + x, wt[e] * lvD);
-      atomicAdd(B.iw + x, wt[e] * lwD);
-    }
+  for (int e = 0; e < 8; e++) {
+    const int64_t x = q + off[e];
+    atomicAdd(B.ip + x, wt[e] * lpD);
+    atomicAdd(B.iu + x, wt[e] * luD);
+    atomicAdd(B.iv + x, wt[e] * lvD);
+    atomicAdd(B.iw + x, wt[e] * lwD);
   }
-  if (use_smem) {
-    __syncthreads();
-    for (int e = threadIdx.x; e < ng; e += blockDim.x)
-      if (sgrad[e] != 0.0) atomicAdd(&B.grad[e], sgrad[e]);
-  }
+}
+
+// grad[m][e] = sum of gcell[e][b] over the band cells b of material m; one block per coefficient
+// slot e, per-material bins in shared memory.
+__global__ void __launch_bounds__(256) k_adj_grad_reduce(const int4* rec, const double* gcell, int64_t nB, int P,
+                                                         int nMat, double* grad) {
+  extern __shared__ double bins[];
+  const int e = blockIdx.x;
+  for (int m = threadIdx.x; m < nMat; m += blockDim.x) bins[m] = 0.0;
+  __syncthreads();
+  for (int64_t b = threadIdx.x; b < nB; b += blockDim.x) atomicAdd(&bins[rec[b].w], gcell[(int64_t)e * nB + b]);
+  __syncthreads();
+  for (int m = threadIdx.x; m < nMat; m += blockDim.x) grad[(int64_t)m * P + e] = bins[m];
 }
 
 template <class R>
@@ -357,22 +641,34 @@ __global__ void k_clear_inactive(R* f, const uint8_t* cls, int64_t n) {
     if (!(cls[c] & (CLS_UPDATE | CLS_BAND))) f[c] = R(0);
 }
 
-template <class R>
-dim3 cell_grid(const AdjStageArgs<R>& a) {
-  return dim3((unsigned)((a.Nx + 63) / 64), (unsigned)((a.Ny + 3) / 4), (unsigned)a.Nz);
-}
-
 }  // namespace
 
 template <class R>
-cudaError_t launch_adj_centres(const AdjStageArgs<R>& a, cudaStream_t s) {
-  k_adj_centres<R><<<cell_grid(a), dim3(64, 4, 1), 0, s>>>(a);
+size_t adj_stage_smem(int kz_chunk) {
+  return AdjSmem<R>::bytes(kz_chunk);
+}
+
+template <class R>
+cudaError_t adj_stage_setup(size_t smem_bytes) {
+  return cudaFuncSetAttribute((const void*)k_adj_stage<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)smem_bytes);
+}
+
+template <class R>
+cudaError_t adj_stage_occupancy(int* blocks_per_sm, size_t smem_bytes) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_adj_stage<R>, NTHREADS, smem_bytes);
+}
+
+template <class R>
+cudaError_t launch_adj_stage(const AdjStageArgs<R>& a, dim3 grid, cudaStream_t s) {
+  k_adj_stage<R><<<grid, dim3(TX, TY, 1), AdjSmem<R>::bytes(a.kz_chunk), s>>>(a);
   return cudaGetLastError();
 }
 
 template <class R>
-cudaError_t launch_adj_gather(const AdjStageArgs<R>& a, cudaStream_t s) {
-  k_adj_gather<R><<<cell_grid(a), dim3(64, 4, 1), 0, s>>>(a);
+cudaError_t launch_adj_probe_scatter(const AdjBandArgs<R>& a, cudaStream_t s) {
+  if (a.nB <= 0) return cudaSuccess;
+  k_adj_probe_scatter<R><<<(unsigned)((a.nB + 255) / 256), 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -381,15 +677,19 @@ cudaError_t launch_adj_band(int stage, const AdjBandArgs<R>& a, cudaStream_t s) 
   if (a.nB <= 0) return cudaSuccess;
   const int bs = 256;
   const unsigned nb = (unsigned)((a.nB + bs - 1) / bs);
-  const size_t gbytes = (size_t)a.nMat * (1 + 2 * a.K + 4 * a.L) * sizeof(double);
-  const int use_smem = gbytes <= 32768 ? 1 : 0;
-  const size_t smem = use_smem ? gbytes : 0;
   if (stage == 0)
-    k_adj_band<R, 0><<<nb, bs, smem, s>>>(a, use_smem);
+    k_adj_band<R, 0><<<nb, bs, 0, s>>>(a);
   else if (stage == 1)
-    k_adj_band<R, 1><<<nb, bs, smem, s>>>(a, use_smem);
+    k_adj_band<R, 1><<<nb, bs, 0, s>>>(a);
   else
-    k_adj_band<R, 2><<<nb, bs, smem, s>>>(a, use_smem);
+    k_adj_band<R, 2><<<nb, bs, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adj_grad_reduce(const int4* rec, const double* gcell, int64_t nB, int P, int nMat, double* grad,
+                                   cudaStream_t s) {
+  if (nB <= 0) return cudaMemsetAsync(grad, 0, (size_t)nMat * P * sizeof(double), s);
+  k_adj_grad_reduce<<<(unsigned)P, 256, (size_t)nMat * sizeof(double), s>>>(rec, gcell, nB, P, nMat, grad);
   return cudaGetLastError();
 }
 
@@ -407,8 +707,11 @@ cudaError_t launch_clear_inactive(R* f, const uint8_t* cls, int64_t n, cudaStrea
 }
 
 #define FZ_ADJ_INSTANTIATE(R)                                                                        \
-  template cudaError_t launch_adj_centres<R>(const AdjStageArgs<R>&, cudaStream_t);                  \
-  template cudaError_t launch_adj_gather<R>(const AdjStageArgs<R>&, cudaStream_t);                   \
+  template size_t adj_stage_smem<R>(int);                                                            \
+  template cudaError_t adj_stage_setup<R>(size_t);                                                   \
+  template cudaError_t adj_stage_occupancy<R>(int*, size_t);                                         \
+  template cudaError_t launch_adj_probe_scatter<R>(const AdjBandArgs<R>&, cudaStream_t);             \
+  template cudaError_t launch_adj_stage<R>(const AdjStageArgs<R>&, dim3, cudaStream_t);              \
   template cudaError_t launch_adj_band<R>(int, const AdjBandArgs<R>&, cudaStream_t);                 \
   template cudaError_t launch_adj_receivers<R>(R*, const int64_t*, int, const double*, int64_t,      \
                                                const double*, int64_t, int64_t, cudaStream_t);       \

@@ -33,10 +33,9 @@ struct AdjStageArgs {
   R* bu;
   R* bv;
   R* bw;
-  R* contrib;  // [30][ncell]: per axis d, stencil offset k - 2, component (p, normal velocity)
   const uint8_t* cls;
   int32_t Nx, Ny, Nz;
-  int64_t Sx, plane, ncell;
+  int64_t Sx, plane;
   R cb;      // b dt / h
   R a_base;  // a
   R b_in;    // b
@@ -48,9 +47,15 @@ struct AdjStageArgs {
   const PmlCoef<R>* pcx;
   const PmlCoef<R>* pcy;
   const PmlCoef<R>* pcz;
-  P* lpsix;  // adjoint of the cPML psi tiles (stage 2: of psi^{n+1} on entry, of psi^n on exit)
-  P* lpsiy;
-  P* lpsiz;
+  const P* lpsix;  // adjoint of psi^{n+1} (read by stage 2's flux weights)
+  const P* lpsiy;
+  const P* lpsiz;
+  P* opsix;  // adjoint of psi^n: stage 2 writes b lpsi + w dt out, stages 1 and 0 add w dt out
+  P* opsiy;
+  P* opsiz;
+  int32_t kz_chunk;  // z planes per CTA of the fused stage adjoint
+  int32_t acc_in;    // 1: add to the input adjoint (it holds U0's adjoint already), 0: store it
+  int32_t acc_base;  // 1: add to U0's adjoint, 0: store it (stages 1 and 2)
 };
 
 // Adjoint of the immersed band of one stage (functions3D.cuh:426-565), with the gradient of the
@@ -73,6 +78,7 @@ struct AdjBandArgs {
   R* iu;
   R* iv;
   R* iw;
+  R* probe;  // [4][nB]: adjoint of the probed p, u, v, w of every band cell
   int64_t Sx, plane;
   double Z0, dt;
   int32_t K, L, nMat;
@@ -103,15 +109,27 @@ struct AdjBandArgs {
   const double* gs2L;
   double* gs2M;
   double* gs2R;
-  double* grad;  // [nMat][1 + 2K + 4L]: Rinf, A[K], zeta[K], B[L], C[L], alpha[L], beta[L]
+  double* gcell;  // [1 + 2K + 4L][nB]: per band cell, d J / d (Rinf, A[K], zeta[K], B[L], C[L],
+                  // alpha[L], beta[L]) of its material, accumulated over stages and steps
 };
 
+// fused adjoint of one stage kernel launch over the interior cells, grid (x tiles, y tiles, z chunks)
 template <class R>
-cudaError_t launch_adj_centres(const AdjStageArgs<R>& a, cudaStream_t s);
+cudaError_t launch_adj_stage(const AdjStageArgs<R>& a, dim3 grid, cudaStream_t s);
 template <class R>
-cudaError_t launch_adj_gather(const AdjStageArgs<R>& a, cudaStream_t s);
+size_t adj_stage_smem(int kz_chunk);
+template <class R>
+cudaError_t adj_stage_setup(size_t smem_bytes);
+template <class R>
+cudaError_t adj_stage_occupancy(int* blocks_per_sm, size_t smem_bytes);
+// the band cells' probe adjoints (k_adj_band's output) into the stage input's adjoint
+template <class R>
+cudaError_t launch_adj_probe_scatter(const AdjBandArgs<R>& a, cudaStream_t s);
 template <class R>
 cudaError_t launch_adj_band(int stage, const AdjBandArgs<R>& a, cudaStream_t s);
+// grad[m][e] = sum over the band cells of material m of gcell[e][b]
+cudaError_t launch_adj_grad_reduce(const int4* rec, const double* gcell, int64_t nB, int P, int nMat, double* grad,
+                                   cudaStream_t s);
 // adjoint of the receiver gather: lp[cell_r] += 2 (ir[r][n] - target[r][n])
 template <class R>
 cudaError_t launch_adj_receivers(R* lp, const int64_t* rcell, int nrec, const double* ir, int64_t cap,
