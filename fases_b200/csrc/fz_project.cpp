@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <filesystem>
 #include <fstream>
 #include <sstream>
 #include <string>
@@ -304,25 +305,61 @@ int fz_load_project(const char* scene_path, const char* config_path, const char*
   // U D R L F B = config lines 7..12 (main3D.cu:155-160)
   for (int f = 0; f < 6; f++) p.pml[f] = (conf[6 + f] != 0.0f) ? 1 : 0;
 
-  // scene cache (main3D.cu:334-380): dims on line 2 of scene_cache.txt, S.bin, oid.bin
-  std::ifstream ck(out_dir + "/scene_cache.txt");
+  // scene cache (main3D.cu:334-428): output/S.bin and output/oid.bin, valid while the first line of
+  // output/scene_cache.txt carries the key "<scene path> <scene mtime> <h> <tol>" (the path made
+  // absolute and normal, main3D.cu:66-72); otherwise the geometry is built from the OBJ on the
+  // device and the cache is rewritten, dims and domain size on its second line
+  namespace fs = std::filesystem;
+  fs::path sp(scene_path);
+  if (sp.is_relative()) sp = fs::current_path() / sp;
+  sp = sp.lexically_normal();
+  const float tol = 3.0f * h;
+  std::error_code fec;
+  std::ostringstream key_s;
+  key_s << sp.string() << " " << fs::last_write_time(sp, fec).time_since_epoch().count() << " " << h << " " << tol;
+  const std::string cache_key = key_s.str();
   std::string key;
   int Nx = 0, Ny = 0, Nz = 0;
   float Lx = 0, Ly = 0, Lz = 0;
-  if (!(std::getline(ck, key) && (ck >> Nx >> Ny >> Nz >> Lx >> Ly >> Lz)))
-    return set_global_error(FZ_ESTATE, "no scene cache (" + out_dir +
-                                           "/scene_cache.txt, S.bin, oid.bin) for this project: build the "
-                                           "geometry first");
-  const size_t N = (size_t)Nx * Ny * Nz;
-  std::vector<float> S(N);
-  std::vector<uint8_t> oid(N);
+  std::vector<float> S;
+  std::vector<uint8_t> oid;
+  bool cached = false;
   {
+    std::ifstream ck(out_dir + "/scene_cache.txt");
+    cached = std::getline(ck, key) && key == cache_key && (ck >> Nx >> Ny >> Nz >> Lx >> Ly >> Lz);
+  }
+  if (cached) {
+    const size_t N = (size_t)Nx * Ny * Nz;
+    S.resize(N);
+    oid.resize(N);
     FILE* fS = std::fopen((out_dir + "/S.bin").c_str(), "rb");
     FILE* fO = std::fopen((out_dir + "/oid.bin").c_str(), "rb");
-    const bool ok = fS && fO && std::fread(S.data(), 4, N, fS) == N && std::fread(oid.data(), 1, N, fO) == N;
+    cached = fS && fO && std::fread(S.data(), 4, N, fS) == N && std::fread(oid.data(), 1, N, fO) == N;
     if (fS) std::fclose(fS);
     if (fO) std::fclose(fO);
-    if (!ok) return set_global_error(FZ_EIO, "S.bin/oid.bin missing or short for the cached grid");
+  }
+  if (!cached) {
+    int32_t dims[3];
+    double Ld[3];
+    int rc = fz_scene_dims(sp.string().c_str(), h, dims, Ld);
+    if (rc != FZ_OK) return rc;
+    Nx = dims[0]; Ny = dims[1]; Nz = dims[2];
+    Lx = (float)Ld[0]; Ly = (float)Ld[1]; Lz = (float)Ld[2];
+    const size_t N = (size_t)Nx * Ny * Nz;
+    S.assign(N, 0.f);
+    oid.assign(N, 0xFF);
+    rc = fz_build_scene(sp.string().c_str(), h, 3.0, device, S.data(), oid.data(), (int64_t)N);
+    if (rc != FZ_OK) return rc;
+    fs::create_directories(out_dir, fec);
+    FILE* fS = std::fopen((out_dir + "/S.bin").c_str(), "wb");
+    FILE* fO = std::fopen((out_dir + "/oid.bin").c_str(), "wb");
+    const bool ok = fS && fO && std::fwrite(S.data(), 4, N, fS) == N && std::fwrite(oid.data(), 1, N, fO) == N;
+    if (fS) std::fclose(fS);
+    if (fO) std::fclose(fO);
+    if (ok) {  // stamp the cache only after both arrays are written
+      std::ofstream(out_dir + "/scene_cache.txt", std::ios::trunc)
+          << cache_key << "\n" << Nx << " " << Ny << " " << Nz << " " << Lx << " " << Ly << " " << Lz << "\n";
+    }
   }
   // materials: poles.txt (main3D.cu:592-603), layer names from the OBJ, one .fit per layer except
   // BoundingBox-like layers (main3D.cu:624-634)
@@ -422,7 +459,7 @@ int fz_load_project(const char* scene_path, const char* config_path, const char*
   rc = fz_create(&p, &H);
   if (rc != FZ_OK) return rc;
   H->Lx = Lx; H->Ly = Ly; H->Lz = Lz;
-  H->scene_name = scene_path;
+  H->scene_name = sp.string();  // header.txt carries the absolute scene path (main3D.cu:1445)
   rc = fz_load_geometry_raw(H, S.data(), oid.data(), Nx, Ny, Nz);
   std::vector<double> sv(spress.begin(), spress.end()), sfr(sfreq.begin(), sfreq.end());
   if (rc == FZ_OK) rc = fz_set_materials(H, nMat, Km, Lm, Rinf.data(), A.data(), zeta.data(), B.data(), C.data(), al.data(), be.data());

@@ -11,6 +11,8 @@ z-lo, z-hi; 6.. = obstacles.
 """
 from dataclasses import dataclass, field
 
+import os
+
 import numpy as np
 
 from . import materials as mats
@@ -244,3 +246,47 @@ def benchmark_2d(room_cells=(256, 256), h=0.02, seed=0, c=343.0, rho=1.2, cfl=0.
     p0[GHOST + 1:] = 0.0
     return {"scene": scene, "materials": wall_mats, "pml": pml, "pml_cells": pml_cells, "c": c, "rho": rho,
             "dt": dt, "h": h, "source_cell": src, "receivers": recs, "p0": p0, "seed": seed}
+
+
+def obj_layers(path):
+    """Group (layer) names of an OBJ in material order: a group is created at its first face, named
+    by the second token of its o/g line when there are two or more (3D-solver/include/parsing3D.h:
+    167-288); material m of the scene is layer m (oid m + 1)."""
+    names, seen, cur, named, pending = [], set(), "unnamed", False, True
+    with open(path) as f:
+        for line in f:
+            line = line.strip(" \t\r\n")
+            if not line or line[0] == "#":
+                continue
+            if line.startswith("o ") or line.startswith("g "):
+                parts = line.split()[1:]
+                nm = parts[1] if len(parts) >= 2 else (parts[0] if parts else "unnamed")
+                if not named or nm != cur:
+                    cur, named, pending = nm, True, True
+            elif line.startswith("f ") and len(line.split()) >= 4 and pending:
+                nm = cur if named else "unnamed"
+                if nm not in seen:
+                    seen.add(nm)
+                    names.append(nm)
+                pending = False
+    return names
+
+
+def from_obj(path, h, tol_cells=3.0, device=0):
+    """Scene of an OBJ file built on the GPU by the library (fz_build_scene): the signed distance
+    and material ids the reference solver caches in output/S.bin and output/oid.bin."""
+    import ctypes as C
+
+    from ._abi import check, lib
+    dims = (C.c_int32 * 3)()
+    L = (C.c_double * 3)()
+    check(lib().fz_scene_dims(os.fsencode(path), float(h), dims, L))
+    Nx, Ny, Nz = dims
+    S = np.zeros((Nz, Ny, Nx), np.float32)
+    oid = np.zeros((Nz, Ny, Nx), np.uint8)
+    check(lib().fz_build_scene(os.fsencode(path), float(h), float(tol_cells), int(device),
+                               S.ctypes.data_as(C.POINTER(C.c_float)), oid.ctypes.data_as(C.POINTER(C.c_uint8)),
+                               S.size))
+    return Scene(S=S, oid=oid, h=float(h), room_cells=(Nx - 2 * GHOST, Ny - 2 * GHOST, Nz - 2 * GHOST),
+                 layers=obj_layers(path))
+

@@ -101,6 +101,19 @@ void fz_destroy(fz_handle* h);
 int fz_load_geometry_raw(fz_handle* h, const float* S, const uint8_t* oid, int32_t Nx, int32_t Ny,
                          int32_t Nz);
 
+/* Scene geometry from an OBJ file (replaces parse_obj3d + build_sdf + build_oid_dense,
+ * 3D-solver/include/parsing3D.h:150-288, 389-452, 574-661, 815-1154, run by main3D.cu:300-428):
+ * fz_scene_dims gives the padded grid (mesh shifted so its minimum corner sits at 3h; domain
+ * [0, max + 3h]; N = ceil(L/h) per axis) and the domain size L (may be NULL), host only.
+ * fz_build_scene fills S (float32 signed distance, positive in air, exact within 8h of the
+ * surface and +-8h beyond) and oid (material id = OBJ group index + 1 in order of first face,
+ * for band cells 0 <= S <= tol_cells*h; 0xFF elsewhere) in the reference layout, computed on
+ * `device`; cap = cells available in each array. These are the arrays fz_load_geometry_raw takes
+ * and the reference caches in output/S.bin and output/oid.bin. */
+int fz_scene_dims(const char* obj_path, double h, int32_t* dims, double* L);
+int fz_build_scene(const char* obj_path, double h, double tol_cells, int32_t device, float* S, uint8_t* oid,
+                   int64_t cap);
+
 /* ADE materials. Replaces read_fit_file per layer (common/filterABC.h:31-90) plus the device
  * copies (main3D.cu:639-658). Arrays use the reference's flat(k, m, K) = m*K + k layout:
  * Rinf[nMat], A/zeta[nMat*K], B/C/alpha/beta[nMat*L]. Material m is oid m+1. */
