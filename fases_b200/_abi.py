@@ -77,12 +77,15 @@ SIGNATURES = {
     "fz_create": (C.c_int, [C.POINTER(FzParams), C.POINTER(_P)]),
     "fz_destroy": (None, [_P]),
     "fz_load_geometry_raw": (C.c_int, [_P, _fp, _u8p, _i32, _i32, _i32]),
+    "fz_device_memory": (C.c_int, [_i32, _i64p, _i64p]),
     "fz_scene_dims": (C.c_int, [C.c_char_p, C.c_double, _ip, _dp]),
     "fz_build_scene": (C.c_int, [C.c_char_p, C.c_double, C.c_double, _i32, _fp, _u8p, _i64]),
     "fz_set_materials": (C.c_int, [_P, _i32, _i32, _i32, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
     "fz_set_sources": (C.c_int, [_P, _i32, _ip, _dp, _i32, _dp, _dp, _i64]),
     "fz_set_source_members": (C.c_int, [_P, _i32, _ip]),
     "fz_set_receivers": (C.c_int, [_P, _i32, _ip, _i64]),
+    "fz_set_slices": (C.c_int, [_P, _i32, _i32, _i32, _i64, _i64]),
+    "fz_get_slices": (C.c_int, [_P, _fp, _i64, _i64p]),
     "fz_set_fields": (C.c_int, [_P, _dp, _dp, _dp, _dp]),
     "fz_run": (C.c_int, [_P, _i64]),
     "fz_run_timed": (C.c_int, [_P, _i64, _dp]),

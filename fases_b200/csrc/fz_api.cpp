@@ -91,6 +91,8 @@ void free_device(fz_handle* h) {
   dfree(h->d_rec_cell);
   dfree(h->d_ir);
   dfree(h->d_vel);
+  dfree(h->d_slices);
+  h->sl_on = false;
 }
 
 // cuTensorMapEncodeTiled, fetched from the driver at run time (no link-time libcuda dependency).
@@ -554,6 +556,11 @@ cudaError_t enqueue_finish(fz_handle* h) {
     e = fz::launch_receivers<R>(u1[0], u1[1], u1[2], u1[3], h->d_rec_cell, h->nrec * h->nb, h->d_ir, h->d_vel,
                                 h->rec_cap, h->d_step, h->stream);
     if (e != cudaSuccess) return e;
+    if (h->sl_on) {
+      e = fz::launch_slices<R>(u1[0], u1[1], u1[2], u1[3], h->Nx, h->Ny, h->Nz, h->Sx, h->sl_i, h->sl_j, h->sl_k,
+                               h->d_step, h->sl_step, h->sl_cap, h->d_slices, h->nsm, h->stream);
+      if (e != cudaSuccess) return e;
+    }
   }
   std::swap(h->i0, h->i1);
   std::swap(h->ph_old, h->ph_cur);
@@ -916,6 +923,44 @@ int fz_set_receivers(fz_handle* h, int32_t n, const int32_t* cell_ijk, int64_t c
   return FZ_OK;
 }
 
+int fz_set_slices(fz_handle* h, int32_t i0, int32_t j0, int32_t k0, int64_t anim_step, int64_t max_frames) {
+  if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  if (!h->have_geometry) return set_error(h, FZ_ESTATE, "fz_set_slices before fz_load_geometry_raw");
+  if (h->steps_enqueued != 0 || h->nb != 1)
+    return set_error(h, FZ_ESTATE, "fz_set_slices: set before the first step, on a single-member solve");
+  if (i0 < 0 || i0 >= h->Nx || j0 < 0 || j0 >= h->Ny || k0 < 0 || k0 >= h->Nz || anim_step < 1 || max_frames < 0)
+    return set_error(h, FZ_EINVAL, "fz_set_slices: planes inside the grid, anim_step >= 1, max_frames >= 0");
+  cudaSetDevice(h->device);
+  dfree(h->d_slices);
+  h->sl_on = false;
+  if (max_frames == 0) return FZ_OK;
+  const int64_t frame = 3 * ((int64_t)h->Ny * h->Nz + (int64_t)h->Nx * h->Nz + (int64_t)h->Nx * h->Ny);
+  FZ_CUDA(h, cudaMalloc(&h->d_slices, (size_t)frame * max_frames * sizeof(float)), "cudaMalloc(slices)");
+  h->sl_i = i0; h->sl_j = j0; h->sl_k = k0;
+  h->sl_step = anim_step;
+  h->sl_cap = max_frames;
+  h->sl_frame = frame;
+  h->sl_on = true;
+  free_graphs(h);  // captured steps must include the slice launch
+  return FZ_OK;
+}
+
+int fz_get_slices(fz_handle* h, float* out, int64_t cap, int64_t* frames) {
+  if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  int rc = fz_sync(h, 0);
+  if (rc != FZ_OK) return rc;
+  int64_t n = 0;
+  FZ_CUDA(h, cudaMemcpy(&n, h->d_step, sizeof(int64_t), cudaMemcpyDeviceToHost), "step D2H");
+  const int64_t nf = h->sl_on ? std::min(h->sl_cap, n > 0 ? (n - 1) / h->sl_step + 1 : 0) : 0;
+  if (frames) *frames = nf;
+  if (!out) return FZ_OK;
+  if (cap < nf * h->sl_frame) return set_error(h, FZ_EINVAL, "fz_get_slices: buffer too small");
+  if (nf > 0)
+    FZ_CUDA(h, cudaMemcpy(out, h->d_slices, (size_t)(nf * h->sl_frame) * sizeof(float), cudaMemcpyDeviceToHost),
+            "slices D2H");
+  return FZ_OK;
+}
+
 int fz_set_fields(fz_handle* h, const double* p, const double* u, const double* v, const double* w) {
   if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
   if (!h->have_geometry) return set_error(h, FZ_ESTATE, "fz_set_fields before fz_load_geometry_raw");
@@ -1084,6 +1129,19 @@ int fz_profile_read(fz_handle* h, double* ms, int64_t* launches, int32_t nkinds)
     if (launches) launches[k] = h->prof_n[k];
   }
   for (int k = 0; k < 8; k++) { h->prof_ms[k] = 0; h->prof_n[k] = 0; }
+  return FZ_OK;
+}
+
+int fz_device_memory(int32_t device, int64_t* free_bytes, int64_t* total_bytes) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+    return fzi::set_global_error(FZ_ENODEV, "fz_device_memory: no such CUDA device");
+  cudaSetDevice(device);
+  size_t f = 0, t = 0;
+  const cudaError_t e = cudaMemGetInfo(&f, &t);
+  if (e != cudaSuccess) return fzi::set_global_error(FZ_ECUDA, std::string("cudaMemGetInfo: ") + cudaGetErrorString(e));
+  if (free_bytes) *free_bytes = (int64_t)f;
+  if (total_bytes) *total_bytes = (int64_t)t;
   return FZ_OK;
 }
 

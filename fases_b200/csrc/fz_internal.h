@@ -82,6 +82,12 @@ struct fz_handle {
   double* d_ir = nullptr;
   double* d_vel = nullptr;
 
+  // animation slices (planes x = sl_i, y = sl_j, z = sl_k) every sl_step steps, up to sl_cap frames
+  bool sl_on = false;
+  int sl_i = 0, sl_j = 0, sl_k = 0;
+  int64_t sl_step = 1, sl_cap = 0, sl_frame = 0;  // sl_frame: floats per frame
+  float* d_slices = nullptr;
+
   // TMA descriptors: halo tiles of p, u, v and own tiles of p, u, v, w of each field set, and
   // the class bytes
   CUtensorMap halo_map[3][3];

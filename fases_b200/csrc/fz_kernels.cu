@@ -564,6 +564,50 @@ __global__ void k_receivers(const R* __restrict__ p, const R* __restrict__ u, co
   if (threadIdx.x == 0) *step = n + 1;
 }
 
+// Animation frame after a step (main3D.cu:1326-1394): pressure on the planes x = i0, y = j0, z = k0
+// and the in-plane components of the unit energy-flow direction sign(p) u / |u|, written when the
+// step just completed (the device step counter, already advanced) is a multiple of anim_step
+// counted from the first. Frame layout: pX[Ny Nz] pY[Nx Nz] pZ[Nx Ny], then (Iy, Iz) on X,
+// (Ix, Iz) on Y, (Ix, Iy) on Z -- each plane in the reference's order (j + Ny k, i + Nx k, i + Nx j).
+template <class R>
+__global__ void k_slices(const R* __restrict__ p, const R* __restrict__ u, const R* __restrict__ v,
+                         const R* __restrict__ w, int Nx, int Ny, int Nz, int64_t Sx, int i0, int j0, int k0,
+                         const int64_t* __restrict__ step, int64_t anim_step, int64_t cap, float* __restrict__ out) {
+  const int64_t n = *step - 1;
+  if (n < 0 || n % anim_step != 0) return;
+  const int64_t f = n / anim_step;
+  if (f >= cap) return;
+  const int64_t nX = (int64_t)Ny * Nz, nY = (int64_t)Nx * Nz, nZ = (int64_t)Nx * Ny, tot = nX + nY + nZ;
+  float* fr = out + f * 3 * tot;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+    int i, j, k;
+    if (e < nX) {
+      j = (int)(e % Ny); k = (int)(e / Ny); i = i0;
+    } else if (e < nX + nY) {
+      const int64_t q = e - nX;
+      i = (int)(q % Nx); k = (int)(q / Nx); j = j0;
+    } else {
+      const int64_t q = e - nX - nY;
+      i = (int)(q % Nx); j = (int)(q / Nx); k = k0;
+    }
+    const int64_t c = XOFF + i + Sx * ((int64_t)j + (int64_t)Ny * k);
+    const float pp = (float)p[c], uu = (float)u[c], vv = (float)v[c], ww = (float)w[c];
+    const float sp = (pp >= 0.f) ? 1.f : -1.f;
+    const float inv = sp / (sqrtf(uu * uu + vv * vv + ww * ww) + 1e-20f);
+    fr[e] = pp;
+    float c1, c2;
+    if (e < nX) { c1 = vv * inv; c2 = ww * inv; }
+    else if (e < nX + nY) { c1 = uu * inv; c2 = ww * inv; }
+    else { c1 = uu * inv; c2 = vv * inv; }
+    // component planes follow the pressure planes: [c1X c2X | c1Y c2Y | c1Z c2Z]
+    const int64_t base = (e < nX) ? tot : (e < nX + nY) ? tot + 2 * nX : tot + 2 * nX + 2 * nY;
+    const int64_t off = (e < nX) ? e : (e < nX + nY) ? e - nX : e - nX - nY;
+    const int64_t m = (e < nX) ? nX : (e < nX + nY) ? nY : nZ;
+    fr[base + off] = c1;
+    fr[base + m + off] = c2;
+  }
+}
+
 // FP64 energy 0.5 sum(p^2/(rho c^2) + rho |u|^2) (functions3D.cuh:111-129). Padding cells are
 // zero, so summing the whole allocation sums the grid.
 template <class R>
@@ -658,6 +702,14 @@ cudaError_t launch_receivers(const R* p, const R* u, const R* v, const R* w, con
 }
 
 template <class R>
+cudaError_t launch_slices(const R* p, const R* u, const R* v, const R* w, int Nx, int Ny, int Nz, int64_t Sx, int i0,
+                          int j0, int k0, const int64_t* step, int64_t anim_step, int64_t cap, float* out,
+                          int nsm, cudaStream_t s) {
+  k_slices<R><<<nsm, 256, 0, s>>>(p, u, v, w, Nx, Ny, Nz, Sx, i0, j0, k0, step, anim_step, cap, out);
+  return cudaGetLastError();
+}
+
+template <class R>
 cudaError_t launch_energy(const R* p, const R* u, const R* v, const R* w, int64_t n, double inv_rc2,
                           double rho, double* out, int nsm, cudaStream_t s) {
   k_energy<R><<<nsm * 4, 256, 0, s>>>(p, u, v, w, n, inv_rc2, rho, out);
@@ -673,6 +725,8 @@ cudaError_t launch_energy(const R* p, const R* u, const R* v, const R* w, int64_
   template cudaError_t launch_receivers<R>(const R*, const R*, const R*, const R*, const int64_t*, \
                                            int, double*, double*, int64_t, int64_t*,               \
                                            cudaStream_t);                                          \
+  template cudaError_t launch_slices<R>(const R*, const R*, const R*, const R*, int, int, int, int64_t, int, int, \
+                                        int, const int64_t*, int64_t, int64_t, float*, int, cudaStream_t);       \
   template cudaError_t launch_energy<R>(const R*, const R*, const R*, const R*, int64_t, double,   \
                                         double, double*, int, cudaStream_t);
 

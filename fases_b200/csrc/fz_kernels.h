@@ -23,6 +23,10 @@ cudaError_t launch_receivers(const R* p, const R* u, const R* v, const R* w, con
                              int nrec, double* ir, double* vel, int64_t cap, int64_t* step,
                              cudaStream_t s);
 template <class R>
+cudaError_t launch_slices(const R* p, const R* u, const R* v, const R* w, int Nx, int Ny, int Nz, int64_t Sx, int i0,
+                          int j0, int k0, const int64_t* step, int64_t anim_step, int64_t cap, float* out,
+                          int nsm, cudaStream_t s);
+template <class R>
 cudaError_t launch_energy(const R* p, const R* u, const R* v, const R* w, int64_t n, double inv_rc2,
                           double rho, double* out, int nsm, cudaStream_t s);
 

@@ -243,16 +243,46 @@ int fz_write_outputs(fz_handle* h, const char* output_dir, int32_t src_idx, cons
     std::fclose(a);
     std::fclose(b);
   }
-  // header.txt (main3D.cu:1441-1449): Nx Ny Nz Nt Lx Ly Lz pbin anim_step dt scene h tol/h.
-  // No animation slices are written, so pbin is 0.
+  // animation slices (main3D.cu:1206-1235, 1337-1393): pressure{X,Y,Z}.bin and the in-plane unit
+  // energy-flow components I{y,z}_X, I{x,z}_Y, I{x,y}_Z, one frame after another
+  int64_t pbin = 0, anim_step = 1;
+  if (h->sl_on) {
+    int64_t nf = 0;
+    rc = fz_get_slices(h, nullptr, 0, &nf);
+    if (rc != FZ_OK) return rc;
+    std::vector<float> fr((size_t)(nf * h->sl_frame));
+    if (nf > 0) {
+      rc = fz_get_slices(h, fr.data(), (int64_t)fr.size(), &nf);
+      if (rc != FZ_OK) return rc;
+    }
+    const int64_t nX = (int64_t)h->Ny * h->Nz, nY = (int64_t)h->Nx * h->Nz, nZ = (int64_t)h->Nx * h->Ny;
+    const int64_t tot = nX + nY + nZ;
+    // file, offset in the frame, plane size
+    const struct { const char* name; int64_t off, len; } files[9] = {
+        {"pressureX.bin", 0, nX},          {"pressureY.bin", nX, nY},          {"pressureZ.bin", nX + nY, nZ},
+        {"Iy_X.bin", tot, nX},             {"Iz_X.bin", tot + nX, nX},         {"Ix_Y.bin", tot + 2 * nX, nY},
+        {"Iz_Y.bin", tot + 2 * nX + nY, nY}, {"Ix_Z.bin", tot + 2 * nX + 2 * nY, nZ},
+        {"Iy_Z.bin", tot + 2 * nX + 2 * nY + nZ, nZ}};
+    for (const auto& fl : files) {
+      const std::string fn = dir + "/" + fl.name;
+      FILE* fo = std::fopen(fn.c_str(), "wb");
+      if (!fo) return set_error(h, FZ_EIO, "cannot write " + fn);
+      for (int64_t q = 0; q < nf; q++) std::fwrite(fr.data() + q * h->sl_frame + fl.off, sizeof(float), (size_t)fl.len, fo);
+      std::fclose(fo);
+    }
+    pbin = nf;
+    anim_step = h->sl_step;
+  } else {
+    const int64_t frames = std::max<int64_t>(1, std::min<int64_t>(300, n));
+    anim_step = std::max<int64_t>(1, n / frames);
+  }
+  // header.txt (main3D.cu:1441-1449): Nx Ny Nz Nt Lx Ly Lz pbin anim_step dt scene h tol/h
   const std::string hdr = dir + "/header.txt";
   FILE* f = std::fopen(hdr.c_str(), "w");
   if (!f) return set_error(h, FZ_EIO, "cannot write " + hdr);
-  const int64_t frames = std::max<int64_t>(1, std::min<int64_t>(300, n));
-  const int64_t anim_step = std::max<int64_t>(1, n / frames);
   const std::string scene = scene_name ? std::string(scene_name) : h->scene_name;
   std::fprintf(f, "%d %d %d %d %f %f %f %d %d %f %s %f %d\n", h->Nx, h->Ny, h->Nz, (int)n, (float)h->Lx,
-               (float)h->Ly, (float)h->Lz, 0, (int)anim_step, (float)h->prm.dt, scene.c_str(),
+               (float)h->Ly, (float)h->Lz, (int)pbin, (int)anim_step, (float)h->prm.dt, scene.c_str(),
                (float)h->prm.h, (int)(h->prm.tol_cells * h->prm.h / h->prm.h));
   std::fclose(f);
   return FZ_OK;
@@ -467,6 +497,24 @@ int fz_load_project(const char* scene_path, const char* config_path, const char*
     rc = fz_set_sources(H, nsrc, sijk.data(), sv.data(), src_opt, sfr.data(), src_opt == 2 ? nullptr : us.data(),
                         src_opt == 2 ? 0 : (int64_t)us.size());
   if (rc == FZ_OK) rc = fz_set_receivers(H, (int)(rijk.size() / 3), rijk.data(), Nt);
+  // animation slices (main3D.cu:1152-1199): planes at config lines 19-21 ((int)(x/h) + 3), frames
+  // from line 22 (default 300, at least 60, at most Nt), every Nt / frames steps. The reference caps
+  // the frames by 85 % of host RAM; here they are kept in device memory, capped at a quarter of it.
+  if (rc == FZ_OK && conf.size() > 20) {
+    const int si = (int)(conf[18] / h) + 3, sj = (int)(conf[19] / h) + 3, sk = (int)(conf[20] / h) + 3;
+    if (si >= 0 && si < Nx && sj >= 0 && sj < Ny && sk >= 0 && sk < Nz) {
+      int64_t wanted = (conf.size() > 21 && conf[21] > 0) ? (int64_t)conf[21] : 300;
+      wanted = std::max<int64_t>(wanted, 60);
+      const int64_t per_frame = 3 * 4 * ((int64_t)Ny * Nz + (int64_t)Nx * Nz + (int64_t)Nx * Ny);
+      size_t fr = 0, tot = 0;
+      cudaMemGetInfo(&fr, &tot);
+      int64_t frames = std::min<int64_t>(wanted, std::max<int64_t>(1, (int64_t)(fr / 4) / per_frame));
+      frames = std::min<int64_t>(frames, Nt);
+      const int64_t anim_step = std::max<int64_t>(1, Nt / std::max<int64_t>(frames, 1));
+      frames = Nt / anim_step;
+      rc = fz_set_slices(H, si, sj, sk, anim_step, frames);
+    }
+  }
   if (rc != FZ_OK) {
     fzi::set_global_error(rc, H->err);
     fz_destroy(H);

@@ -1,13 +1,18 @@
 """Command-line drop-in for the FVM part of `fases3D` (3D-solver/core/main3D.cu:26-1449):
 
-    python -m fases_b200.fz3d <scene.obj> <config.txt> <src.txt> <rec.txt> [--fp64]
+    python -m fases_b200.fz3d <scene.obj> <config.txt> <src.txt> <rec.txt> [--fp64] [--estimate]
 
 Reads the same project files through libfz.so (fz_load_project), runs the Nt time steps of the
 configuration on the GPU, prints the integer progress lines the GUI parses ("NN%" every 5 %,
 functions3D.cuh:1431-1439, parsed by the regex (\\d+)\\s*% in common/gui.py:6713), and writes
 output/IR<r>_<s>.bin, output/VEL<r>_<s>.bin and output/header.txt in the reference formats
-(config/p_ref.bin and output/pre_header.txt are written by the loader). Geometry comes from the
-project's scene cache (output/S.bin, output/oid.bin, output/scene_cache.txt).
+(config/p_ref.bin and output/pre_header.txt are written by the loader), plus the animation slices
+pressure{X,Y,Z}.bin and I*_*.bin. The geometry is built from the OBJ on the GPU and cached in
+output/S.bin, output/oid.bin, output/scene_cache.txt exactly as the reference caches it.
+
+--estimate (main3D.cu:505-525) runs no time step: it prints the effective air volume (air cells x h^3)
+and the "[MEM] key=value" pre-flight line the GUI parses (common/gui.py:11017-11033) for this
+library's memory needs.
 """
 import os
 import sys
@@ -37,6 +42,57 @@ def _src_index(config_path):
     return int(vals[17]) if len(vals) > 17 else 0
 
 
+def _config_values(config_path):
+    vals = []
+    for line in open(config_path):
+        line = line.split("#", 1)[0].strip()
+        if not line:
+            continue
+        try:
+            vals.append(float(line.split()[0]))
+        except ValueError:
+            continue
+    return vals
+
+
+def estimate(scene, config, precision="fp32", device=0):
+    """The --estimate pre-flight line: voxel count of the padded grid and this library's memory
+    model -- host ~11 B per voxel (S, oid, class bytes and copies), device 49 B (FP32 fields) or
+    97 B (FP64) -- against free memory (thresholds 0.7 host, 0.9 device as in the reference)."""
+    import ctypes as C
+
+    from ._abi import check, lib
+    h = _config_values(config)[0]
+    dims = (C.c_int32 * 3)()
+    check(lib().fz_scene_dims(os.fsencode(scene), float(h), dims, None))
+    nvox = dims[0] * dims[1] * dims[2]
+    avail = 0
+    try:
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable:"):
+                avail = int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    free, total = C.c_int64(), C.c_int64()
+    gpu_ok = lib().fz_device_memory(int(device), C.byref(free), C.byref(total)) == 0
+    need_host = 11.0 * nvox
+    need_dev = (97.0 if precision == "fp64" else 49.0) * nvox
+    over = 0.0
+    if avail > 0 and need_host > 0.7 * avail:
+        over = max(over, need_host / (0.7 * avail))
+    if gpu_ok and need_dev > 0.9 * free.value:
+        over = max(over, need_dev / (0.9 * free.value))
+    min_h = h * over ** (1.0 / 3.0) if over > 0.0 else h
+    if gpu_ok:  # effective air volume: air cells x h^3 (main3D.cu:445-446), from the GPU-built scene
+        from .scenes import from_obj
+        sc = from_obj(scene, h, device=device)
+        print("[OK] estimate: V = %.3f m^3" % (float((sc.S > 0).sum()) * h ** 3), flush=True)
+    print("[MEM] voxels=%d need_host_gb=%.3f need_dev_gb=%.3f free_host_gb=%.3f free_dev_gb=%.3f over=%.4f min_h=%.4g"
+          % (nvox, need_host / 1e9, need_dev / 1e9, avail / 1e9, (free.value if gpu_ok else 0) / 1e9, over, min_h),
+          flush=True)
+    return 0
+
+
 def main(argv=None):
     argv = list(sys.argv[1:] if argv is None else argv)
     if len(argv) < 4:
@@ -44,6 +100,8 @@ def main(argv=None):
         return 1
     precision = "fp64" if "--fp64" in argv else "fp32"
     scene, config, src, rec = argv[:4]
+    if "--estimate" in argv:
+        return estimate(scene, config, precision)
     s, nt = Solver.from_project(scene, config, src, rec, precision=precision)
     print(f"[OK] Will now start {nt} iterations", flush=True)
     t0 = time.perf_counter()

@@ -129,6 +129,32 @@ class Solver:
         self._nrec = cells.shape[0]
         self._cap = int(capacity_steps)
 
+    def set_slices(self, i0, j0, k0, anim_step, max_frames):
+        """Animation slices on the planes x = i0, y = j0, z = k0 (cell indices) every anim_step steps."""
+        self._chk(lib().fz_set_slices(self._h, int(i0), int(j0), int(k0), int(anim_step), int(max_frames)))
+
+    def slices(self):
+        """Frames taken so far: dict of pX [F, Nz, Ny], pY [F, Nz, Nx], pZ [F, Ny, Nx] and the in-plane
+        unit energy-flow components IyX, IzX, IxY, IzY, IxZ, IyZ of the same shapes."""
+        n = C.c_int64()
+        self._chk(lib().fz_get_slices(self._h, None, 0, C.byref(n)))
+        Nz, Ny, Nx = self.shape
+        sizes = [Ny * Nz, Nx * Nz, Nx * Ny]
+        per = 3 * sum(sizes)
+        buf = np.zeros(n.value * per, np.float32)
+        if n.value:
+            self._chk(lib().fz_get_slices(self._h, buf.ctypes.data_as(C.POINTER(C.c_float)), buf.size, C.byref(n)))
+        fr = buf.reshape(n.value, per)
+        shapes = [(Nz, Ny), (Nz, Nx), (Ny, Nx)]
+        out, o = {}, 0
+        for name, q in (("pX", 0), ("pY", 1), ("pZ", 2)):
+            out[name] = fr[:, o:o + sizes[q]].reshape((n.value,) + shapes[q])
+            o += sizes[q]
+        for name, q in (("IyX", 0), ("IzX", 0), ("IxY", 1), ("IzY", 1), ("IxZ", 2), ("IyZ", 2)):
+            out[name] = fr[:, o:o + sizes[q]].reshape((n.value,) + shapes[q])
+            o += sizes[q]
+        return out
+
     def set_fields(self, p=None, u=None, v=None, w=None):
         """Arrays of shape [Nz, Ny, Nx] (or [batch, Nz, Ny, Nx] for batched solves)."""
         if self.batch > 1:

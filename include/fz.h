@@ -101,6 +101,9 @@ void fz_destroy(fz_handle* h);
 int fz_load_geometry_raw(fz_handle* h, const float* S, const uint8_t* oid, int32_t Nx, int32_t Ny,
                          int32_t Nz);
 
+/* Free and total device memory of a CUDA device (the --estimate pre-flight, main3D.cu:505-525). */
+int fz_device_memory(int32_t device, int64_t* free_bytes, int64_t* total_bytes);
+
 /* Scene geometry from an OBJ file (replaces parse_obj3d + build_sdf + build_oid_dense,
  * 3D-solver/include/parsing3D.h:150-288, 389-452, 574-661, 815-1154, run by main3D.cu:300-428):
  * fz_scene_dims gives the padded grid (mesh shifted so its minimum corner sits at 3h; domain
@@ -137,6 +140,17 @@ int fz_set_source_members(fz_handle* h, int32_t n, const int32_t* member);
  * (u,v,w) after every step into a device buffer of capacity_steps samples per receiver
  * (replaces the per-step cudaMemcpy at main3D.cu:1399-1414). */
 int fz_set_receivers(fz_handle* h, int32_t n, const int32_t* cell_ijk, int64_t capacity_steps);
+
+/* Animation slices (main3D.cu:1152-1237, 1326-1394): after every step whose index is a multiple of
+ * anim_step (the first step included), the pressure on the planes x = i0, y = j0, z = k0 and the
+ * in-plane components of the unit energy-flow direction sign(p) u/|u| are stored in device memory,
+ * up to max_frames frames (0 turns slicing off). Set before the first step, single-member solves.
+ * fz_get_slices copies the frames taken so far (*frames = their count; out may be NULL to ask):
+ * per frame pX[Ny*Nz] pY[Nx*Nz] pZ[Nx*Ny] IyX IzX IxY IzY IxZ IyZ, each plane in the reference's
+ * order (j + Ny*k, i + Nx*k, i + Nx*j); fz_write_outputs writes them as pressure{X,Y,Z}.bin and
+ * I{y,z}_X.bin, I{x,z}_Y.bin, I{x,y}_Z.bin with the frame count in header.txt. */
+int fz_set_slices(fz_handle* h, int32_t i0, int32_t j0, int32_t k0, int64_t anim_step, int64_t max_frames);
+int fz_get_slices(fz_handle* h, float* out, int64_t cap, int64_t* frames);
 
 /* Initial fields in the reference layout (any pointer may be NULL = zero). The reference always
  * starts quiescent (main3D.cu:1134-1135); this is the Gaussian-pulse initial condition of the
