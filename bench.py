@@ -50,35 +50,17 @@ def parse():
 
 
 def dist_setup(n):
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    pg = None
-    if world > 1:
-        import datetime
-
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-        pg = dist
-    return rank, world, local, pg
+    from fases_b200.replicas import Replicas
+    rep = Replicas()
+    return rep.rank, rep.world, rep.local, rep
 
 
-def barrier(pg):
-    if pg is not None:
-        import torch
-        pg.barrier()
-        torch.cuda.synchronize()
+def barrier(rep):
+    rep.barrier()
 
 
-def max_over_ranks(pg, x):
-    if pg is None:
-        return x
-    import torch
-    t = torch.tensor([float(x)], device="cuda")
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    return float(t.item())
+def max_over_ranks(rep, x):
+    return rep.max(x)
 
 
 class Clocks:
@@ -424,24 +406,15 @@ def run_adjoint(args):
 def main():
     args = parse()
     rank, world, local, pg = dist_setup(args.gpus)
-    if args.impl == "reference":
-        run_reference(args, rank)
-        return
-    if args.config == "plain2d":
+    # the reference arm and the side configurations run on rank 0 only; the other ranks leave
+    side = {"plain2d": run_plain2d, "precision": run_precision, "batched": run_batched, "adjoint": run_adjoint}
+    if args.impl == "reference" or args.config in side:
         if rank == 0:
-            run_plain2d(args)
-        return
-    if args.config == "precision":
-        if rank == 0:
-            run_precision(args)
-        return
-    if args.config == "batched":
-        if rank == 0:
-            run_batched(args)
-        return
-    if args.config == "adjoint":
-        if rank == 0:
-            run_adjoint(args)
+            if args.impl == "reference":
+                run_reference(args, rank)
+            else:
+                side[args.config](args)
+        pg.close()
         return
     room = args.room
     b = workload(room)
@@ -543,8 +516,7 @@ def main():
             "finite": finite,
         }
         print(json.dumps(line), flush=True)
-    if pg is not None:
-        pg.destroy_process_group()
+    pg.close()
 
 
 if __name__ == "__main__":
