@@ -92,6 +92,10 @@ SIGNATURES = {
     "fz_run_progress": (C.c_int, [_P, _i64, _i32, C.c_void_p, C.c_void_p]),
     "fz_sync": (C.c_int, [_P, _i64]),
     "fz_steps_done": (C.c_int, [_P, _i64p]),
+    "fz_check_health": (C.c_int, [_P, _i64p]),
+    "fz_state_bytes": (C.c_int, [_P, _i64p]),
+    "fz_state_save": (C.c_int, [_P, _P, _i64]),
+    "fz_state_load": (C.c_int, [_P, _P, _i64]),
     "fz_misfit_gradient": (C.c_int, [_P, _i64, _i32, _dp, _i64, _dp, _dp, _i64, _dp]),
     "fz_material_layout": (C.c_int, [_P, _ip, _ip, _ip]),
     "fz_group_create": (C.c_int, [C.POINTER(_P), _i32, C.POINTER(_P)]),

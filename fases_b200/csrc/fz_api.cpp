@@ -554,7 +554,7 @@ cudaError_t enqueue_finish(fz_handle* h) {
     Timer t(h, 4);
     R* const* u1 = (R* const*)h->U[h->i1];
     e = fz::launch_receivers<R>(u1[0], u1[1], u1[2], u1[3], h->d_rec_cell, h->nrec * h->nb, h->d_ir, h->d_vel,
-                                h->rec_cap, h->d_step, h->stream);
+                                h->rec_cap, h->d_step, h->d_err, h->stream);
     if (e != cudaSuccess) return e;
     if (h->sl_on) {
       e = fz::launch_slices<R>(u1[0], u1[1], u1[2], u1[3], h->Nx, h->Ny, h->Nz, h->Sx, h->sl_i, h->sl_j, h->sl_k,
@@ -965,9 +965,159 @@ int fz_set_fields(fz_handle* h, const double* p, const double* u, const double* 
   if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
   if (!h->have_geometry) return set_error(h, FZ_ESTATE, "fz_set_fields before fz_load_geometry_raw");
   int rc = fz_sync(h, 0);
-  if (rc != FZ_OK) return rc;
+  if (rc != FZ_OK && rc != FZ_ENONFINITE) return rc;  // a blown-up state is what this call replaces
   cudaSetDevice(h->device);
+  // a new initial state, as a fresh solver has it: the two other field sets zero (cells the stage
+  // kernels skip keep their values from set to set), quiescent ADE and cPML auxiliary states and
+  // a clean health word
+  FZ_CUDA(h, cudaMemset(h->d_err, 0, sizeof(int32_t)), "error word reset");
+  for (int q : {h->i1, h->i2})
+    for (int f = 0; f < 4; f++)
+      FZ_CUDA(h, cudaMemset(h->U[q][f], 0, (size_t)h->ncell_dev * h->nb * h->rsize), "field set reset");
+  if (h->nB > 0)
+    for (int q = 0; q < 3; q++)
+      for (int a = 0; a < 3; a++)
+        if (h->d_ade[q][a]) {
+          const size_t n = (size_t)h->nB * (a == 0 ? h->K : h->L) * 8;
+          FZ_CUDA(h, cudaMemset(h->d_ade[q][a], 0, n), "ADE reset");
+        }
+  {
+    const int64_t d2 = 2 * (int64_t)h->prm.pml_cells;
+    const int64_t tile_n[3] = {d2 * h->Ny * h->Nz * h->nb, (int64_t)h->Nx * d2 * h->Nz * h->nb,
+                               (int64_t)h->Nx * h->Ny * d2 * h->nb};
+    for (int a = 0; a < 3; a++)
+      if (h->d_psi[a]) FZ_CUDA(h, cudaMemset(h->d_psi[a], 0, (size_t)tile_n[a] * 2 * h->rsize), "psi reset");
+  }
   return h->fp64 ? set_fields<double>(h, p, u, v, w) : set_fields<float>(h, p, u, v, w);
+}
+
+// ---- checkpoint / resume -------------------------------------------------------------------
+// Layout of a saved state: StateHeader, then the field sets in rotation roles (U0, U1, U2; 4
+// fields each), the ADE sets in roles (old, cur, nu; phi, psi1, psi2), the cPML psi tiles, the
+// receiver traces and velocities, the animation frames.
+namespace {
+struct StateHeader {
+  char magic[8];
+  int32_t precision, nb, Nx, Ny, Nz, K, L, nrec, slices;
+  int64_t nB, rec_cap, step, sl_cap, psi_bytes[3];
+};
+
+struct StatePart {
+  void* dev;
+  size_t bytes;
+};
+
+std::vector<StatePart> state_parts(fz_handle* h) {
+  std::vector<StatePart> v;
+  const size_t fb = (size_t)h->ncell_dev * h->nb * h->rsize;
+  for (int role : {h->i0, h->i1, h->i2})
+    for (int f = 0; f < 4; f++) v.push_back({h->U[role][f], fb});
+  const size_t ab[3] = {(size_t)h->K * h->nB * 8, (size_t)h->L * h->nB * 8, (size_t)h->L * h->nB * 8};
+  for (int role : {h->ph_old, h->ph_cur, h->ph_nu})
+    for (int q = 0; q < 3; q++)
+      if (h->nB > 0) v.push_back({h->d_ade[role][q], ab[q]});
+  const int64_t d2 = 2 * (int64_t)h->prm.pml_cells;
+  const int64_t tile_n[3] = {d2 * h->Ny * h->Nz * h->nb, (int64_t)h->Nx * d2 * h->Nz * h->nb,
+                             (int64_t)h->Nx * h->Ny * d2 * h->nb};
+  for (int a = 0; a < 3; a++)
+    if (h->d_psi[a]) v.push_back({h->d_psi[a], (size_t)tile_n[a] * 2 * h->rsize});
+  if (h->nrec > 0) {
+    const size_t n = (size_t)h->nrec * h->nb * (size_t)std::max<int64_t>(1, h->rec_cap);
+    v.push_back({h->d_ir, n * 8});
+    v.push_back({h->d_vel, n * 3 * 8});
+  }
+  if (h->sl_on) v.push_back({h->d_slices, (size_t)(h->sl_frame * h->sl_cap) * sizeof(float)});
+  return v;
+}
+
+void state_header(fz_handle* h, StateHeader& hd) {
+  std::memset(&hd, 0, sizeof(hd));
+  std::memcpy(hd.magic, "FZSTATE1", 8);
+  hd.precision = h->prm.precision;
+  hd.nb = h->nb; hd.Nx = h->Nx; hd.Ny = h->Ny; hd.Nz = h->Nz; hd.K = h->K; hd.L = h->L;
+  hd.nrec = h->nrec; hd.slices = h->sl_on ? 1 : 0;
+  hd.nB = h->nB; hd.rec_cap = h->rec_cap; hd.sl_cap = h->sl_on ? h->sl_cap : 0;
+  for (int a = 0; a < 3; a++) hd.psi_bytes[a] = h->d_psi[a] ? 1 : 0;
+}
+}  // namespace
+
+int fz_state_bytes(fz_handle* h, int64_t* bytes) {
+  if (!check_handle(h) || !bytes) return fzi::set_global_error(FZ_EINVAL, "fz_state_bytes: NULL argument");
+  if (!h->have_geometry) return set_error(h, FZ_ESTATE, "fz_state_bytes before fz_load_geometry_raw");
+  int rc = fzi::prepare(h);
+  if (rc != FZ_OK) return rc;
+  int64_t n = (int64_t)sizeof(StateHeader);
+  for (const auto& p : state_parts(h)) n += (int64_t)p.bytes;
+  *bytes = n;
+  return FZ_OK;
+}
+
+int fz_state_save(fz_handle* h, void* buf, int64_t cap) {
+  int64_t need = 0;
+  int rc = fz_state_bytes(h, &need);
+  if (rc != FZ_OK) return rc;
+  if (!buf || cap < need) return set_error(h, FZ_EINVAL, "fz_state_save: buffer needs " + std::to_string(need) + " bytes");
+  rc = fz_sync(h, 0);
+  if (rc != FZ_OK) return rc;
+  StateHeader hd;
+  state_header(h, hd);
+  FZ_CUDA(h, cudaMemcpy(&hd.step, h->d_step, sizeof(int64_t), cudaMemcpyDeviceToHost), "step D2H");
+  char* o = (char*)buf;
+  std::memcpy(o, &hd, sizeof(hd));
+  o += sizeof(hd);
+  for (const auto& p : state_parts(h)) {
+    FZ_CUDA(h, cudaMemcpy(o, p.dev, p.bytes, cudaMemcpyDeviceToHost), "state D2H");
+    o += p.bytes;
+  }
+  return FZ_OK;
+}
+
+int fz_state_load(fz_handle* h, const void* buf, int64_t len) {
+  int64_t need = 0;
+  int rc = fz_state_bytes(h, &need);
+  if (rc != FZ_OK) return rc;
+  if (!buf || len < need) return set_error(h, FZ_EINVAL, "fz_state_load: state of the wrong size for this solver");
+  rc = fz_sync(h, 0);
+  if (rc != FZ_OK) return rc;
+  StateHeader mine, hd;
+  state_header(h, mine);
+  std::memcpy(&hd, buf, sizeof(hd));
+  const int64_t step = hd.step;
+  hd.step = 0;
+  if (std::memcmp(&mine, &hd, sizeof(hd)) != 0)
+    return set_error(h, FZ_EINVAL, "fz_state_load: the state was saved by a solver of another configuration "
+                                   "(grid, precision, batch, band, poles, receivers, cPML or slices differ)");
+  const char* o = (const char*)buf + sizeof(hd);
+  for (const auto& p : state_parts(h)) {
+    FZ_CUDA(h, cudaMemcpy(p.dev, o, p.bytes, cudaMemcpyHostToDevice), "state H2D");
+    o += p.bytes;
+  }
+  FZ_CUDA(h, cudaMemcpy(h->d_step, &step, sizeof(step), cudaMemcpyHostToDevice), "step H2D");
+  FZ_CUDA(h, cudaMemset(h->d_err, 0, sizeof(int32_t)), "error word reset");
+  h->steps_enqueued = step;
+  return FZ_OK;
+}
+
+int fz_check_health(fz_handle* h, int64_t* nonfinite) {
+  if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  if (!h->have_geometry) return set_error(h, FZ_ESTATE, "fz_check_health before fz_load_geometry_raw");
+  cudaSetDevice(h->device);
+  unsigned long long* d = (unsigned long long*)h->d_scratch;  // 64-byte per-handle scratch
+  FZ_CUDA(h, cudaMemsetAsync(d, 0, sizeof(*d), h->stream), "health reset");
+  const int64_t n = h->ncell_dev * h->nb;
+  cudaError_t e = h->fp64 ? fz::launch_count_nonfinite<double>((const double*)h->U[h->i0][0], (const double*)h->U[h->i0][1],
+                                                               (const double*)h->U[h->i0][2], (const double*)h->U[h->i0][3],
+                                                               n, d, h->nsm, h->stream)
+                          : fz::launch_count_nonfinite<float>((const float*)h->U[h->i0][0], (const float*)h->U[h->i0][1],
+                                                              (const float*)h->U[h->i0][2], (const float*)h->U[h->i0][3],
+                                                              n, d, h->nsm, h->stream);
+  if (e != cudaSuccess) return cuda_fail(h, e, "health launch");
+  int rc = fz_sync(h, 0);
+  unsigned long long cnt = 0;
+  FZ_CUDA(h, cudaMemcpy(&cnt, d, sizeof(cnt), cudaMemcpyDeviceToHost), "health D2H");
+  if (nonfinite) *nonfinite = (int64_t)cnt;
+  if (cnt > 0) return set_error(h, FZ_ENONFINITE, std::to_string(cnt) + " non-finite values in the current state");
+  return rc;
 }
 
 int fz_run(fz_handle* h, int64_t nsteps) {
@@ -1031,9 +1181,13 @@ int fz_sync(fz_handle* h, int64_t timeout_ms) {
       int32_t kerr = 0;
       e = cudaMemcpy(&kerr, h->d_err, sizeof(kerr), cudaMemcpyDeviceToHost);
       if (e != cudaSuccess) return cuda_fail(h, e, "error word D2H");
-      if (kerr != 0)
+      if (kerr & fz::KERR_TMA_TIMEOUT)
         return set_error(h, FZ_ETIMEOUT, "a kernel's bounded wait gave up (code " + std::to_string(kerr) +
                                              "); results of this run are invalid");
+      if (kerr & fz::KERR_NONFINITE)
+        return set_error(h, FZ_ENONFINITE, "a receiver sampled NaN or Inf: the solution blew up (check the "
+                                               "materials' passivity, the CFL number and the initial fields)");
+      if (kerr != 0) return set_error(h, FZ_ECUDA, "device error word " + std::to_string(kerr));
       return FZ_OK;
     }
     if (e != cudaErrorNotReady) return cuda_fail(h, e, "stream");

@@ -103,6 +103,7 @@ struct StageArgs {
 
 // Kernel error codes written to the handle's device error word.
 constexpr int32_t KERR_TMA_TIMEOUT = 1;
+constexpr int32_t KERR_NONFINITE = 2;  // a receiver sampled NaN or Inf (the solution blew up)
 
 // TMA descriptors of one stage launch: the stage-input fields p, u, v as halo tiles
 // (PW x PH x 1), the base state U0 as own tiles (TX x TY x 1; stages 1 and 2) and the class bytes

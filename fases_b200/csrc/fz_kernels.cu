@@ -548,20 +548,34 @@ __global__ void __launch_bounds__(256, 4) k_band(const BandArgs<R> B) {
 template <class R>
 __global__ void k_receivers(const R* __restrict__ p, const R* __restrict__ u, const R* __restrict__ v,
                             const R* __restrict__ w, const int64_t* __restrict__ rcell, int nrec,
-                            double* ir, double* vel, int64_t cap, int64_t* step) {
+                            double* ir, double* vel, int64_t cap, int64_t* step, int32_t* err) {
   const int64_t n = *step;
-  if (n < cap) {
-    for (int r = threadIdx.x; r < nrec; r += blockDim.x) {
-      const int64_t c = rcell[r];
+  for (int r = threadIdx.x; r < nrec; r += blockDim.x) {
+    const int64_t c = rcell[r];
+    const double pp = (double)p[c], uu = (double)u[c], vv = (double)v[c], ww = (double)w[c];
+    // health word: a blown-up solution reaches the receivers (their samples are read anyway)
+    if (!isfinite(pp) || !isfinite(uu) || !isfinite(vv) || !isfinite(ww)) atomicOr(err, KERR_NONFINITE);
+    if (n < cap) {
       const int64_t o = (int64_t)r * cap + n;
-      ir[o] = (double)p[c];
-      vel[3 * o + 0] = (double)u[c];
-      vel[3 * o + 1] = (double)v[c];
-      vel[3 * o + 2] = (double)w[c];
+      ir[o] = pp;
+      vel[3 * o + 0] = uu;
+      vel[3 * o + 1] = vv;
+      vel[3 * o + 2] = ww;
     }
   }
   __syncthreads();
   if (threadIdx.x == 0) *step = n + 1;
+}
+
+// Non-finite values in a state (p, u, v, w over n cells), counted into *count.
+template <class R>
+__global__ void k_count_nonfinite(const R* __restrict__ p, const R* __restrict__ u, const R* __restrict__ v,
+                                  const R* __restrict__ w, int64_t n, unsigned long long* count) {
+  unsigned long long k = 0;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x)
+    k += (!isfinite(p[c])) + (!isfinite(u[c])) + (!isfinite(v[c])) + (!isfinite(w[c]));
+  for (int o = 16; o > 0; o >>= 1) k += __shfl_down_sync(0xffffffffu, k, o);
+  if ((threadIdx.x & 31) == 0 && k) atomicAdd(count, k);
 }
 
 // Animation frame after a step (main3D.cu:1326-1394): pressure on the planes x = i0, y = j0, z = k0
@@ -696,8 +710,15 @@ cudaError_t launch_band(int stage, const BandArgs<R>& a, cudaStream_t s) {
 
 template <class R>
 cudaError_t launch_receivers(const R* p, const R* u, const R* v, const R* w, const int64_t* rcell, int nrec,
-                             double* ir, double* vel, int64_t cap, int64_t* step, cudaStream_t s) {
-  k_receivers<R><<<1, 256, 0, s>>>(p, u, v, w, rcell, nrec, ir, vel, cap, step);
+                             double* ir, double* vel, int64_t cap, int64_t* step, int32_t* err, cudaStream_t s) {
+  k_receivers<R><<<1, 256, 0, s>>>(p, u, v, w, rcell, nrec, ir, vel, cap, step, err);
+  return cudaGetLastError();
+}
+
+template <class R>
+cudaError_t launch_count_nonfinite(const R* p, const R* u, const R* v, const R* w, int64_t n,
+                                   unsigned long long* count, int nsm, cudaStream_t s) {
+  k_count_nonfinite<R><<<nsm * 4, 256, 0, s>>>(p, u, v, w, n, count);
   return cudaGetLastError();
 }
 
@@ -723,8 +744,10 @@ cudaError_t launch_energy(const R* p, const R* u, const R* v, const R* w, int64_
   template cudaError_t launch_stage<R>(int, bool, const StageArgs<R>&, const StageMaps&, dim3, cudaStream_t); \
   template cudaError_t launch_band<R>(int, const BandArgs<R>&, cudaStream_t);                      \
   template cudaError_t launch_receivers<R>(const R*, const R*, const R*, const R*, const int64_t*, \
-                                           int, double*, double*, int64_t, int64_t*,               \
+                                           int, double*, double*, int64_t, int64_t*, int32_t*,     \
                                            cudaStream_t);                                          \
+  template cudaError_t launch_count_nonfinite<R>(const R*, const R*, const R*, const R*, int64_t,  \
+                                                 unsigned long long*, int, cudaStream_t);         \
   template cudaError_t launch_slices<R>(const R*, const R*, const R*, const R*, int, int, int, int64_t, int, int, \
                                         int, const int64_t*, int64_t, int64_t, float*, int, cudaStream_t);       \
   template cudaError_t launch_energy<R>(const R*, const R*, const R*, const R*, int64_t, double,   \

@@ -188,6 +188,28 @@ class Solver:
     def sync(self, timeout_ms=0):
         self._chk(lib().fz_sync(self._h, int(timeout_ms)))
 
+    def save_state(self, path=None):
+        """The solver's complete state (checkpoint) as a uint8 array, also written to `path` if given."""
+        n = C.c_int64()
+        self._chk(lib().fz_state_bytes(self._h, C.byref(n)))
+        buf = np.empty(n.value, np.uint8)
+        self._chk(lib().fz_state_save(self._h, buf.ctypes.data_as(C.c_void_p), buf.size))
+        if path is not None:
+            buf.tofile(path)
+        return buf
+
+    def load_state(self, state):
+        """Resumes from a checkpoint of save_state (an array or a file path) taken by a solver set up
+        the same way."""
+        buf = np.fromfile(state, np.uint8) if isinstance(state, (str, os.PathLike)) else np.ascontiguousarray(state, np.uint8)
+        self._chk(lib().fz_state_load(self._h, buf.ctypes.data_as(C.c_void_p), buf.size))
+
+    def check_health(self):
+        """Number of NaN/Inf values in the current state (raises FzError FZ_ENONFINITE if any)."""
+        n = C.c_int64()
+        self._chk(lib().fz_check_health(self._h, C.byref(n)))
+        return n.value
+
     def steps_done(self):
         n = C.c_int64()
         self._chk(lib().fz_steps_done(self._h, C.byref(n)))

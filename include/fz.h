@@ -154,7 +154,9 @@ int fz_get_slices(fz_handle* h, float* out, int64_t cap, int64_t* frames);
 
 /* Initial fields in the reference layout (any pointer may be NULL = zero). The reference always
  * starts quiescent (main3D.cu:1134-1135); this is the Gaussian-pulse initial condition of the
- * synthetic benchmarks and the hook the tests use. */
+ * synthetic benchmarks and the hook the tests use. A new initial state: the other two field
+ * sets and the ADE and cPML auxiliary states are zeroed and the health word cleared (the step
+ * counter and the receiver traces recorded so far are kept). */
 int fz_set_fields(fz_handle* h, const double* p, const double* u, const double* v, const double* w);
 
 /* Enqueues nsteps SSP-RK3 steps on the handle's stream and returns. One step is the reference
@@ -176,6 +178,23 @@ int fz_run_progress(fz_handle* h, int64_t nsteps, int32_t every_percent, fz_prog
 
 /* Bounded wait for all enqueued work (timeout_ms <= 0: 600000 ms). */
 int fz_sync(fz_handle* h, int64_t timeout_ms);
+
+/* Checkpoint / resume (no counterpart in the reference, whose time loop cannot be resumed): the
+ * complete state of a solver -- all three field sets, the ADE states, the cPML psi tiles, the step
+ * counter, the receiver traces so far and the animation frames -- copied into a caller-owned host
+ * buffer of fz_state_bytes bytes, and back. Loading needs a solver set up the same way (geometry,
+ * precision, batch, materials' pole counts, receivers and capacity, cPML faces, slices); the run
+ * then continues exactly as the saved one would have (same results bit for bit). */
+int fz_state_bytes(fz_handle* h, int64_t* bytes);
+int fz_state_save(fz_handle* h, void* buf, int64_t cap);
+int fz_state_load(fz_handle* h, const void* buf, int64_t len);
+
+/* Health of the current state (no counterpart in the reference, which never checks its fields):
+ * counts NaN/Inf values over every field of the state into *nonfinite (may be NULL) and returns
+ * FZ_ENONFINITE if there are any. Independently of this call, every step's receiver gather flags a
+ * non-finite sample in the device error word, which the next fz_sync (and every call that waits)
+ * reports as FZ_ENONFINITE; fz_set_fields starts a new state and clears the word. */
+int fz_check_health(fz_handle* h, int64_t* nonfinite);
 
 /* Steps completed so far (after fz_sync). */
 int fz_steps_done(fz_handle* h, int64_t* n);
