@@ -49,6 +49,26 @@ class FzParams(C.Structure):
         ("tol_cells", C.c_double),
         ("two_d", C.c_int32),
         ("batch", C.c_int32),
+        ("pml_R0", C.c_double),
+        ("pml_kappa_max", C.c_double),
+        ("pml_alpha_max", C.c_double),
+        ("pml_order", C.c_double),
+    ]
+
+
+class FzGradients(C.Structure):
+    _fields_ = [
+        ("cotangent", C.c_int32),
+        ("materials", C.POINTER(C.c_double)),
+        ("materials_cap", C.c_int64),
+        ("source_sval", C.POINTER(C.c_double)),
+        ("source_sval_cap", C.c_int64),
+        ("source_wave", C.POINTER(C.c_double)),
+        ("source_wave_cap", C.c_int64),
+        ("pml", C.POINTER(C.c_double)),
+        ("pml_cap", C.c_int64),
+        ("initial", C.POINTER(C.c_double)),
+        ("initial_cap", C.c_int64),
     ]
 
 
@@ -97,6 +117,7 @@ SIGNATURES = {
     "fz_state_save": (C.c_int, [_P, _P, _i64]),
     "fz_state_load": (C.c_int, [_P, _P, _i64]),
     "fz_misfit_gradient": (C.c_int, [_P, _i64, _i32, _dp, _i64, _dp, _dp, _i64, _dp]),
+    "fz_misfit_gradient_ex": (C.c_int, [_P, _i64, _i32, _dp, _i64, _dp, C.POINTER(FzGradients), _dp]),
     "fz_material_layout": (C.c_int, [_P, _ip, _ip, _ip]),
     "fz_group_create": (C.c_int, [C.POINTER(_P), _i32, C.POINTER(_P)]),
     "fz_group_run": (C.c_int, [_P, _i64]),

@@ -1,7 +1,9 @@
-// fz_adjoint.cpp -- gradient of a receiver misfit with respect to the ADE material coefficients by
-// the discrete adjoint of the stepping scheme (kernels in fz_adjoint.cu). No counterpart in the
-// reference: its material fit (common/fminconFIT.py:239-348) matches octave absorption in the
-// frequency domain and never differentiates the time-domain solver.
+// fz_adjoint.cpp -- gradient of a receiver misfit (or a vector-Jacobian product of the receiver
+// traces) with respect to the ADE material coefficients, the source strengths and waveform, the
+// cPML profile parameters and the initial fields, by the discrete adjoint of the stepping scheme
+// (kernels in fz_adjoint.cu). No counterpart in the reference: its material fit
+// (common/fminconFIT.py:239-348) matches octave absorption in the frequency domain and never
+// differentiates the time-domain solver.
 //
 // Schedule: one forward pass that saves the state (U0, the ADE "old" set, the cPML psi tiles)
 // every `seg` steps; then, last segment first, restore the segment's checkpoint, recompute its
@@ -50,7 +52,7 @@ struct State {
 
 template <class R>
 int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target, int64_t tsteps, double* J,
-                    double* grad, int64_t grad_cap, double* ms) {
+                    const fz_gradients& o, double* ms) {
   typedef typename fz::Pair<R>::T P;
   cudaStream_t s = h->stream;
   const int64_t N = h->ncell_dev;
@@ -59,9 +61,23 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
   const int K = h->K, L = h->L;
   const int nMat = std::max(1, h->nMat);
   const int Pn = 1 + 2 * K + 4 * L;
-  if (grad_cap < (int64_t)nMat * Pn)
+  if (o.materials && o.materials_cap < (int64_t)nMat * Pn)
     return fzi::set_error(h, FZ_EINVAL, "fz_misfit_gradient: grad needs nMat*(1+2K+4L) = " +
                                             std::to_string((int64_t)nMat * Pn) + " elements");
+  const int nsrc = h->nsrc_dev;
+  const int64_t n_us = (h->src_opt == 2) ? 0 : h->n_us;
+  const bool want_src = (o.source_sval || o.source_wave) && nsrc > 0;
+  if (o.source_sval && o.source_sval_cap < h->nsrc)
+    return fzi::set_error(h, FZ_EINVAL, "fz_misfit_gradient_ex: source_sval needs nsrc elements");
+  if (o.source_wave && o.source_wave_cap < (int64_t)h->nsrc * n_us)
+    return fzi::set_error(h, FZ_EINVAL, "fz_misfit_gradient_ex: source_wave needs nsrc * n_us elements");
+  if (want_src && nsrc != h->nsrc)
+    return fzi::set_error(h, FZ_EINVAL, "fz_misfit_gradient_ex: every source must belong to the solve");
+  if (o.pml && o.pml_cap < 4) return fzi::set_error(h, FZ_EINVAL, "fz_misfit_gradient_ex: pml needs 4 elements");
+  const bool want_pml = o.pml && h->pml_on;
+  const int64_t nref = (int64_t)h->Nx * h->Ny * h->Nz;
+  if (o.initial && o.initial_cap < 4 * nref)
+    return fzi::set_error(h, FZ_EINVAL, "fz_misfit_gradient_ex: initial needs 4 * Nx * Ny * Nz elements");
   const size_t ade_b[3] = {(size_t)K * nB * 8, (size_t)L * nB * 8, (size_t)L * nB * 8};
   const int64_t d2 = 2 * (int64_t)h->prm.pml_cells;
   const int64_t tile_n[3] = {d2 * h->Ny * h->Nz, (int64_t)h->Nx * d2 * h->Nz, (int64_t)h->Nx * h->Ny * d2};
@@ -74,11 +90,14 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
   }
   const int64_t nseg = (nsteps + seg - 1) / seg;
   const size_t state_b = 4 * round256(fb) + ade_sum + psi_sum;
-  const size_t seg_b = (size_t)seg * (3 * 4 * round256(fb) + 4 * ade_sum);
+  const size_t seg_b = (size_t)seg * (3 * 4 * round256(fb) + 4 * ade_sum + (want_pml ? psi_sum : 0));
+  const int d = h->prm.pml_cells;
+  const size_t extra_b = round256((size_t)std::max(1, nsrc) * 8) * 2 + round256((size_t)std::max(1, nsrc) * std::max<int64_t>(1, n_us) * 8) +
+                         round256((size_t)3 * 6 * d * 8);
   const size_t adj_b = 4 * 4 * round256(fb) + 4 * ade_sum + 2 * psi_sum +
                        round256((size_t)nMat * Pn * 8) + round256((size_t)Pn * nB * 8) + round256(4 * nB * sizeof(R)) +
                        round256((size_t)h->nrec * tsteps * 8);
-  const size_t total = (size_t)(nseg + 1) * state_b + seg_b + adj_b + 4096;
+  const size_t total = (size_t)(nseg + 1) * state_b + seg_b + adj_b + extra_b + 4096;
   size_t free_b = 0, tot_b = 0;
   FZ_ACUDA(h, cudaMemGetInfo(&free_b, &tot_b), "cudaMemGetInfo");
   if (total + ((size_t)256 << 20) > free_b)
@@ -103,11 +122,14 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
   // phi^{n+1}
   std::vector<void*> S[3];
   std::vector<double*> Ad[4][3];
+  std::vector<void*> Ps[3];  // psi^n of every step of the segment (cPML gradient only)
   for (int t = 0; t < seg; t++) {
     for (int q = 0; q < 3; q++)
       for (int f = 0; f < 4; f++) S[q].push_back(ar.take(fb));
     for (int q = 0; q < 4; q++)
       for (int a = 0; a < 3; a++) Ad[q][a].push_back((double*)ar.take(ade_b[a]));
+    if (want_pml)
+      for (int a = 0; a < 3; a++) Ps[a].push_back(psi_b[a] ? ar.take(psi_b[a]) : nullptr);
   }
   R* lam[4][4];  // adjoint field sets A (carried), B, C, D
   for (int q = 0; q < 4; q++)
@@ -122,7 +144,11 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
   double* d_gcell = (double*)ar.take((size_t)Pn * nB * 8);
   R* d_probe = (R*)ar.take(4 * nB * sizeof(R));
   double* d_target = (double*)ar.take((size_t)h->nrec * tsteps * 8);
-  if (!d_target) return fzi::set_error(h, FZ_ENOMEM, "fz_misfit_gradient: arena layout overflow");
+  double* d_sval = (double*)ar.take((size_t)std::max(1, nsrc) * 8);
+  double* d_gsval = (double*)ar.take((size_t)std::max(1, nsrc) * 8);
+  double* d_gwave = (double*)ar.take((size_t)std::max(1, nsrc) * std::max<int64_t>(1, n_us) * 8);
+  double* d_gpml = (double*)ar.take((size_t)3 * 6 * d * 8);
+  if (!d_gpml) return fzi::set_error(h, FZ_ENOMEM, "fz_misfit_gradient: arena layout overflow");
 
   auto save = [&](const State& st) -> cudaError_t {
     cudaError_t e = cudaSuccess;
@@ -180,8 +206,8 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
   double Jv = 0.0;
   for (int r = 0; r < h->nrec; r++)
     for (int64_t n = 0; n < nsteps; n++) {
-      const double d = ir[(size_t)r * h->rec_cap + n] - target[(size_t)r * tsteps + n];
-      Jv += d * d;
+      const double x = ir[(size_t)r * h->rec_cap + n], t = target[(size_t)r * tsteps + n];
+      Jv += o.cotangent ? t * x : (x - t) * (x - t);
     }
   if (J) *J = Jv;
   FZ_ACUDA(h, cudaMemcpy(d_target, target, (size_t)h->nrec * tsteps * 8, cudaMemcpyHostToDevice), "target H2D");
@@ -194,6 +220,14 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
     for (int a = 0; a < 3; a++)
       if (psi_b[a]) FZ_ACUDA(h, cudaMemsetAsync(lpsi[q][a], 0, psi_b[a], s), "memset");
   if (nB > 0) FZ_ACUDA(h, cudaMemsetAsync(d_gcell, 0, (size_t)Pn * nB * 8, s), "memset");
+  FZ_ACUDA(h, cudaMemsetAsync(d_gsval, 0, (size_t)std::max(1, nsrc) * 8, s), "memset");
+  FZ_ACUDA(h, cudaMemsetAsync(d_gwave, 0, (size_t)std::max(1, nsrc) * std::max<int64_t>(1, n_us) * 8, s), "memset");
+  FZ_ACUDA(h, cudaMemsetAsync(d_gpml, 0, (size_t)3 * 6 * d * 8, s), "memset");
+  if (nsrc > 0)
+    FZ_ACUDA(h, cudaMemcpy(d_sval, h->src_val.data(), (size_t)nsrc * 8, cudaMemcpyHostToDevice), "sval H2D");
+  // source injection per unit strength (the stage kernels' src_coef / sval)
+  const double src_unit = h->prm.dt * h->prm.c * h->prm.c * h->prm.rho * (6.0 * h->prm.h * h->prm.h) /
+                          (h->prm.h * h->prm.h * h->prm.h);
 
   const fz_params& p = h->prm;
   fz::AdjStageArgs<R> sa;
@@ -277,6 +311,8 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
         e = cudaMemcpyAsync(S[0][(size_t)t * 4 + f], h->U[h->i0][f], fb, cudaMemcpyDeviceToDevice, s);
       for (int a = 0; a < 3 && e == cudaSuccess; a++)
         if (ade_b[a]) e = cudaMemcpyAsync(Ad[0][a][(size_t)t], h->d_ade[h->ph_old][a], ade_b[a], cudaMemcpyDeviceToDevice, s);
+      for (int a = 0; a < 3 && e == cudaSuccess && want_pml; a++)
+        if (psi_b[a]) e = cudaMemcpyAsync(Ps[a][(size_t)t], h->d_psi[a], psi_b[a], cudaMemcpyDeviceToDevice, s);
       if (e == cudaSuccess) e = fzi::enqueue_stage(h, 0);
       for (int f = 0; f < 4 && e == cudaSuccess; f++)
         e = cudaMemcpyAsync(S[1][(size_t)t * 4 + f], h->U[h->i1][f], fb, cudaMemcpyDeviceToDevice, s);
@@ -300,7 +336,7 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
         for (int a = 0; a < 3; a++)
           if (ade_b[a]) FZ_ACUDA(h, cudaMemsetAsync(lade[qq][a], 0, ade_b[a], s), "memset");
       FZ_ACUDA(h, fz::launch_adj_receivers<R>(lam[iA][0], h->d_rec_cell, h->nrec, h->d_ir, h->rec_cap, d_target,
-                                               tsteps, n, s), "adjoint receivers");
+                                               tsteps, n, o.cotangent ? 1 : 0, s), "adjoint receivers");
       const void* const* in_st[3] = {&S[0][(size_t)t * 4], &S[1][(size_t)t * 4], &S[2][(size_t)t * 4]};
       for (int st = 2; st >= 0; st--) {
         // adjoint of the stage output (out), of its input (inb) and of U0 (base)
@@ -322,11 +358,41 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
           ba.gs2L = lade[gL][2]; ba.gs2M = lade[jO][2]; ba.gs2R = lade[gR][2];
           FZ_ACUDA(h, fz::launch_adj_band<R>(st, ba, s), "adjoint band");
         }
+        const double w = (st == 0) ? 1.0 : (st == 1) ? 0.25 : 2.0 / 3.0;
+        // parameter gradients of this stage, from the adjoint of its output (band cells scaled)
+        if (want_src)
+          FZ_ACUDA(h, fz::launch_adj_source<R>(lam[out][0], h->d_src_cell, nsrc, d_sval, src_unit, (const R*)h->d_us,
+                                               n_us, h->src_opt, (const R*)h->d_src_freq, (R)(0.5 * p.dt), w,
+                                               2 * n + ((st == 0) ? 0 : (st == 1) ? 2 : 1), o.source_sval ? d_gsval : nullptr,
+                                               o.source_wave ? d_gwave : nullptr, s),
+                   "adjoint sources");
+        if (want_pml)
+          for (int a = 0; a < 3; a++) {
+            if (!psi_b[a]) continue;
+            fz::AdjPmlArgs<R> pa;
+            std::memset(&pa, 0, sizeof(pa));
+            pa.pi = (const R*)in_st[st][0];
+            pa.vi = (const R*)in_st[st][1 + a];
+            pa.lp = lam[out][0];
+            pa.lv = lam[out][1 + a];
+            pa.lpsi = lpsi[ps][a];
+            pa.psin = (const P*)Ps[a][(size_t)t];
+            pa.pc = (const fz::PmlCoef<R>*)h->d_pml_coef[a];
+            pa.cls = h->d_cls;
+            pa.axis = a;
+            pa.Nx = h->Nx; pa.Ny = h->Ny; pa.Nz = h->Nz;
+            pa.d = d;
+            pa.stage = st;
+            pa.Sx = h->Sx; pa.plane = h->plane;
+            pa.inv_h = sa.inv_h; pa.frc2 = sa.frc2; pa.firho = sa.firho; pa.fc = sa.fc;
+            pa.wdt = w * p.dt;
+            pa.g = d_gpml + (size_t)a * 6 * d;
+            FZ_ACUDA(h, fz::launch_adj_pml_grad<R>(pa, h->nsm, s), "adjoint cPML gradient");
+          }
         set_in(sa, in_st[st]);
         sa.lp = lam[out][0]; sa.lu = lam[out][1]; sa.lv = lam[out][2]; sa.lw = lam[out][3];
         sa.ip = lam[inb][0]; sa.iu = lam[inb][1]; sa.iv = lam[inb][2]; sa.iw = lam[inb][3];
         sa.bp = lam[iC][0]; sa.bu = lam[iC][1]; sa.bv = lam[iC][2]; sa.bw = lam[iC][3];
-        const double w = (st == 0) ? 1.0 : (st == 1) ? 0.25 : 2.0 / 3.0;
         sa.stage = st;
         sa.b_in = (R)w;
         sa.a_base = (R)((st == 0) ? 0.0 : (st == 1) ? 0.75 : 1.0 / 3.0);
@@ -349,7 +415,57 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
   FZ_ACUDA(h, fz::launch_adj_grad_reduce(h->d_brec, d_gcell, nB, Pn, nMat, d_grad, s), "gradient reduce");
   FZ_ACUDA(h, cudaEventRecord(ev[3], s), "event record");
   FZ_ACUDA(h, cudaStreamSynchronize(s), "adjoint sync");
-  FZ_ACUDA(h, cudaMemcpy(grad, d_grad, (size_t)nMat * Pn * 8, cudaMemcpyDeviceToHost), "grad D2H");
+  if (o.materials)
+    FZ_ACUDA(h, cudaMemcpy(o.materials, d_grad, (size_t)nMat * Pn * 8, cudaMemcpyDeviceToHost), "grad D2H");
+  if (o.source_sval) {
+    std::fill(o.source_sval, o.source_sval + h->nsrc, 0.0);
+    if (want_src) FZ_ACUDA(h, cudaMemcpy(o.source_sval, d_gsval, (size_t)nsrc * 8, cudaMemcpyDeviceToHost), "grad D2H");
+  }
+  if (o.source_wave && h->nsrc > 0 && n_us > 0) {
+    std::fill(o.source_wave, o.source_wave + (size_t)h->nsrc * n_us, 0.0);
+    if (want_src)
+      FZ_ACUDA(h, cudaMemcpy(o.source_wave, d_gwave, (size_t)nsrc * n_us * 8, cudaMemcpyDeviceToHost), "grad D2H");
+  }
+  if (o.pml) {
+    // chain rule from the table entries to (R0, kappa_max, alpha_max) through the host's table
+    std::fill(o.pml, o.pml + 4, 0.0);
+    if (want_pml) {
+      std::vector<double> g((size_t)3 * 6 * d);
+      FZ_ACUDA(h, cudaMemcpy(g.data(), d_gpml, g.size() * 8, cudaMemcpyDeviceToHost), "grad D2H");
+      const int lo[3] = {p.pml[3] != 0, p.pml[5] != 0, p.pml[1] != 0};
+      const int hi[3] = {p.pml[2] != 0, p.pml[4] != 0, p.pml[0] != 0};
+      const int Na[3] = {h->Nx, h->Ny, h->Nz};
+      for (int a = 0; a < 3; a++) {
+        if (!psi_b[a]) continue;
+        for (int tl = 0; tl < 2 * d; tl++) {
+          const int ca = (tl < d) ? GHOST + tl : Na[a] - GHOST - 2 * d + tl;
+          fzi::PmlEntry e;
+          fzi::pml_entry(p, Na[a], lo[a], hi[a], ca, &e);
+          if (e.tile != tl) continue;
+          for (int v = 0; v < 3; v++)
+            for (int r = 0; r < 3; r++) o.pml[r] += g[(size_t)a * 6 * d + 3 * tl + v] * e.d[v][r];
+        }
+      }
+    }
+  }
+  if (o.initial) {
+    // after the sweep the carried adjoint is that of the step-0 state; cells no kernel writes were
+    // set to zero before the forward pass, so J does not depend on their initial values
+    const size_t rowb = (size_t)h->Nx * sizeof(R);
+    std::vector<R> tmp((size_t)nref);
+    for (int f = 0; f < 4; f++) {
+      FZ_ACUDA(h, cudaMemcpy2D(tmp.data(), rowb, lam[iA][f] + XOFF, (size_t)h->Sx * sizeof(R), rowb,
+                               (size_t)h->Ny * h->Nz, cudaMemcpyDeviceToHost), "grad D2H");
+      double* out = o.initial + (size_t)f * nref;
+      for (int k = 0; k < h->Nz; k++)
+        for (int j = 0; j < h->Ny; j++)
+          for (int i = 0; i < h->Nx; i++) {
+            const size_t c = (size_t)i + (size_t)h->Nx * ((size_t)j + (size_t)h->Ny * k);
+            const int64_t g = XOFF + i + h->Sx * ((int64_t)j + (int64_t)h->Ny * k);
+            out[c] = (h->cls_host[(size_t)g] & (fz::CLS_UPDATE | fz::CLS_BAND)) ? (double)tmp[c] : 0.0;
+          }
+    }
+  }
   if (ms) {
     float a = 0.f, b = 0.f;
     FZ_ACUDA(h, cudaEventElapsedTime(&a, ev[0], ev[1]), "event elapsed");
@@ -379,9 +495,20 @@ int fz_material_layout(fz_handle* h, int32_t* nMat, int32_t* K, int32_t* L) {
 int fz_misfit_gradient(fz_handle* h, int64_t nsteps, int32_t segment_steps, const double* target,
                        int64_t target_steps, double* J, double* grad, int64_t grad_cap, double* ms) {
   if (!h) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
-  if (nsteps < 1 || segment_steps < 1 || !target || !grad || target_steps < nsteps)
+  if (!grad) return fzi::set_error(h, FZ_EINVAL, "fz_misfit_gradient: grad required");
+  fz_gradients o;
+  std::memset(&o, 0, sizeof(o));
+  o.materials = grad;
+  o.materials_cap = grad_cap;
+  return fz_misfit_gradient_ex(h, nsteps, segment_steps, target, target_steps, J, &o, ms);
+}
+
+int fz_misfit_gradient_ex(fz_handle* h, int64_t nsteps, int32_t segment_steps, const double* target,
+                          int64_t target_steps, double* J, fz_gradients* out, double* ms) {
+  if (!h) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  if (nsteps < 1 || segment_steps < 1 || !target || !out || target_steps < nsteps)
     return fzi::set_error(h, FZ_EINVAL, "fz_misfit_gradient: nsteps >= 1, segment_steps >= 1, target of "
-                                        "[n_rec][target_steps >= nsteps], grad required");
+                                        "[n_rec][target_steps >= nsteps] and outputs required");
   if (h->prm.two_d || h->nb != 1)
     return fzi::set_error(h, FZ_EINVAL, "fz_misfit_gradient: 3D single-member solves only");
   int rc = fzi::prepare(h);
@@ -397,8 +524,8 @@ int fz_misfit_gradient(fz_handle* h, int64_t nsteps, int32_t segment_steps, cons
       return fzi::set_error(h, FZ_EINVAL, "fz_misfit_gradient: a source sits in a cell the stage kernels skip");
   }
   cudaSetDevice(h->device);
-  return h->fp64 ? misfit_gradient<double>(h, nsteps, segment_steps, target, target_steps, J, grad, grad_cap, ms)
-                 : misfit_gradient<float>(h, nsteps, segment_steps, target, target_steps, J, grad, grad_cap, ms);
+  return h->fp64 ? misfit_gradient<double>(h, nsteps, segment_steps, target, target_steps, J, *out, ms)
+                 : misfit_gradient<float>(h, nsteps, segment_steps, target, target_steps, J, *out, ms);
 }
 
 }  // extern "C"

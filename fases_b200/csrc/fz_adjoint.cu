@@ -6,6 +6,8 @@
 // (3D-solver/core/functions3D.cuh:56-78, 411-565, 661-1001, 1086-1327); the reference has no
 // adjoint. Arithmetic follows the restated formulas (as the CPU oracle writes them), not the
 // forward kernels' rearranged forms: both are the same function.
+#include <algorithm>
+
 #include "fz_adjoint.h"
 #include "fz_pair.cuh"
 
@@ -629,10 +631,78 @@ __global__ void __launch_bounds__(256) k_adj_grad_reduce(const int4* rec, const 
 
 template <class R>
 __global__ void k_adj_receivers(R* lp, const int64_t* rcell, int nrec, const double* ir, int64_t cap,
-                                const double* target, int64_t tlen, int64_t n) {
+                                const double* target, int64_t tlen, int64_t n, int cotangent) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  for (int r = 0; r < nrec; r++)  // one thread: receivers may share a cell
-    lp[rcell[r]] += (R)(2.0 * (ir[(int64_t)r * cap + n] - target[(int64_t)r * tlen + n]));
+  for (int r = 0; r < nrec; r++) {  // one thread: receivers may share a cell
+    const double t = target[(int64_t)r * tlen + n];
+    lp[rcell[r]] += (R)(cotangent ? t : 2.0 * (ir[(int64_t)r * cap + n] - t));
+  }
+}
+
+template <class R>
+__global__ void k_adj_source(const R* lp, const int64_t* cell, int nsrc, const double* sval, double unit,
+                             const R* u_s, int64_t n_us, int src_opt, const R* freq, R half_dt, double w, int64_t nn,
+                             double* gsval, double* gwave) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nsrc) return;
+  const double lam = (double)lp[cell[q]] * w * unit;
+  double amp;
+  if (src_opt == 2)  // the stage kernel's sine, in its precision
+    amp = (double)(R)sin(2.0 * 3.14159265358979323846 * (double)freq[q] * (double)nn * (double)half_dt);
+  else
+    amp = (nn < n_us) ? (double)u_s[nn] : 0.0;
+  if (gsval) gsval[q] += lam * amp;
+  if (gwave && src_opt != 2 && nn < n_us) gwave[(int64_t)q * n_us + nn] += lam * sval[q];
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_adj_pml_grad(const AdjPmlArgs<R> A) {
+  typedef typename Pair<R>::T P;
+  extern __shared__ double gs[];  // [2d][3]
+  const int d2 = 2 * A.d;
+  for (int e = threadIdx.x; e < 3 * d2; e += blockDim.x) gs[e] = 0.0;
+  __syncthreads();
+  const int ex = A.Nx - 2 * GHOST, ey = A.Ny - 2 * GHOST, ez = A.Nz - 2 * GHOST;
+  const int64_t E0 = (A.axis == 0) ? d2 : ex, E1 = (A.axis == 1) ? d2 : ey, E2 = (A.axis == 2) ? d2 : ez;
+  const int Na = (A.axis == 0) ? A.Nx : (A.axis == 1) ? A.Ny : A.Nz;
+  const int64_t st = (A.axis == 0) ? 1 : (A.axis == 1) ? A.Sx : A.plane;
+  const int64_t total = E0 * E1 * E2;
+  const P kA = pmk(A.frc2, A.firho);
+  const P kC = psplat<R>(-A.fc);
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t a0 = t % E0, r = t / E0;
+    const int64_t a1 = r % E1, a2 = r / E1;
+    const int tile = (int)((A.axis == 0) ? a0 : (A.axis == 1) ? a1 : a2);
+    // psi tile index -> coordinate along the axis (layers [3, 3+d) and [N-3-d, N-3))
+    const int ca = (tile < A.d) ? GHOST + tile : Na - GHOST - d2 + tile;
+    if (A.pc[ca].tile != tile) continue;  // that face is not a cPML face
+    const int i = (A.axis == 0) ? ca : GHOST + (int)a0;
+    const int j = (A.axis == 1) ? ca : GHOST + (int)a1;
+    const int k = (A.axis == 2) ? ca : GHOST + (int)a2;
+    const int64_t g = XOFF + i + A.Sx * ((int64_t)j + (int64_t)A.Ny * k);
+    if (!(A.cls[g] & CLS_UPDATE)) continue;
+    P q[7];
+#pragma unroll
+    for (int o = 0; o < 7; o++) q[o] = pmk(A.pi[g + (o - 3) * st], A.vi[g + (o - 3) * st]);
+    P ml, pl, mc, pc, mr, pr;
+    weno_center<R>(q[0], q[1], q[2], q[3], q[4], ml, pl);
+    weno_center<R>(q[1], q[2], q[3], q[4], q[5], mc, pc);
+    weno_center<R>(q[2], q[3], q[4], q[5], q[6], mr, pr);
+    const P L = psub(godunov<R>(ml, pc, kA, kC), godunov<R>(mc, pr, kA, kC));
+    const R Dp = L.x * A.inv_h, Dv = L.y * A.inv_h;
+    atomicAdd(&gs[3 * tile], A.wdt * ((double)A.lp[g] * (double)Dp + (double)A.lv[g] * (double)Dv));
+    if (A.stage == 2) {
+      const int64_t X = (A.axis == 0)   ? tile + (int64_t)d2 * ((int64_t)j + (int64_t)A.Ny * k)
+                        : (A.axis == 1) ? i + (int64_t)A.Nx * ((int64_t)tile + (int64_t)d2 * k)
+                                        : i + (int64_t)A.Nx * ((int64_t)j + (int64_t)A.Ny * tile);
+      const P lps = A.lpsi[X], ps = A.psin[X];
+      atomicAdd(&gs[3 * tile + 1], (double)lps.x * (double)ps.x + (double)lps.y * (double)ps.y);
+      atomicAdd(&gs[3 * tile + 2], (double)lps.x * (double)Dp + (double)lps.y * (double)Dv);
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < 3 * d2; e += blockDim.x)
+    if (gs[e] != 0.0) atomicAdd(&A.g[e], gs[e]);
 }
 
 template <class R>
@@ -695,8 +765,28 @@ cudaError_t launch_adj_grad_reduce(const int4* rec, const double* gcell, int64_t
 
 template <class R>
 cudaError_t launch_adj_receivers(R* lp, const int64_t* rcell, int nrec, const double* ir, int64_t cap,
-                                 const double* target, int64_t tlen, int64_t n, cudaStream_t s) {
-  k_adj_receivers<R><<<1, 32, 0, s>>>(lp, rcell, nrec, ir, cap, target, tlen, n);
+                                 const double* target, int64_t tlen, int64_t n, int cotangent, cudaStream_t s) {
+  k_adj_receivers<R><<<1, 32, 0, s>>>(lp, rcell, nrec, ir, cap, target, tlen, n, cotangent);
+  return cudaGetLastError();
+}
+
+template <class R>
+cudaError_t launch_adj_source(const R* lp, const int64_t* cell, int nsrc, const double* sval, double unit,
+                              const R* u_s, int64_t n_us, int src_opt, const R* freq, R half_dt, double w, int64_t nn,
+                              double* gsval, double* gwave, cudaStream_t s) {
+  if (nsrc <= 0) return cudaSuccess;
+  k_adj_source<R><<<(unsigned)((nsrc + 127) / 128), 128, 0, s>>>(lp, cell, nsrc, sval, unit, u_s, n_us, src_opt, freq,
+                                                                 half_dt, w, nn, gsval, gwave);
+  return cudaGetLastError();
+}
+
+template <class R>
+cudaError_t launch_adj_pml_grad(const AdjPmlArgs<R>& a, int nsm, cudaStream_t s) {
+  const int64_t ex = a.Nx - 2 * GHOST, ey = a.Ny - 2 * GHOST, ez = a.Nz - 2 * GHOST;
+  const int64_t total = 2 * (int64_t)a.d * ((a.axis == 0) ? ey * ez : (a.axis == 1) ? ex * ez : ex * ey);
+  if (total <= 0) return cudaSuccess;
+  const int64_t nblk = std::min<int64_t>((total + 255) / 256, (int64_t)nsm * 8);
+  k_adj_pml_grad<R><<<(unsigned)nblk, 256, (size_t)6 * a.d * sizeof(double), s>>>(a);
   return cudaGetLastError();
 }
 
@@ -714,7 +804,11 @@ cudaError_t launch_clear_inactive(R* f, const uint8_t* cls, int64_t n, cudaStrea
   template cudaError_t launch_adj_stage<R>(const AdjStageArgs<R>&, dim3, cudaStream_t);              \
   template cudaError_t launch_adj_band<R>(int, const AdjBandArgs<R>&, cudaStream_t);                 \
   template cudaError_t launch_adj_receivers<R>(R*, const int64_t*, int, const double*, int64_t,      \
-                                               const double*, int64_t, int64_t, cudaStream_t);       \
+                                               const double*, int64_t, int64_t, int, cudaStream_t);  \
+  template cudaError_t launch_adj_source<R>(const R*, const int64_t*, int, const double*, double,    \
+                                            const R*, int64_t, int, const R*, R, double, int64_t,    \
+                                            double*, double*, cudaStream_t);                         \
+  template cudaError_t launch_adj_pml_grad<R>(const AdjPmlArgs<R>&, int, cudaStream_t);              \
   template cudaError_t launch_clear_inactive<R>(R*, const uint8_t*, int64_t, cudaStream_t);
 
 FZ_ADJ_INSTANTIATE(float)

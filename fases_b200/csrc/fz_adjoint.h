@@ -113,6 +113,41 @@ struct AdjBandArgs {
                   // alpha[L], beta[L]) of its material, accumulated over stages and steps
 };
 
+// Gradient with respect to the cPML table entries (1/kappa - 1, b, ca) of one axis from one stage.
+// The forward correction (stage kernel) is  out += w dt ((1/kappa - 1) D + psi^n)  for the pressure
+// and the velocity along the axis, and in stage 2  psi^{n+1} = b psi^n + ca D,  with D the flux
+// difference along the axis over h. Per cPML cell of the axis this recomputes D from the stage
+// input exactly as the stage kernel does and adds
+//   g_kinv1 += w dt (lp Dp + lv Dv);   stage 2: g_b += lpsi . psi^n,   g_ca += lpsi . D
+// into g[tile][3] (tile = index in the psi tile's 2d layers).
+template <class R>
+struct AdjPmlArgs {
+  typedef typename Pair<R>::T P;
+  const R* pi;  // stage input: pressure and the velocity along the axis
+  const R* vi;
+  const R* lp;  // adjoint of the stage output (after the band adjoint)
+  const R* lv;
+  const P* lpsi;  // adjoint of psi^{n+1} (stage 2)
+  const P* psin;  // psi^n (stage 2)
+  const PmlCoef<R>* pc;
+  const uint8_t* cls;
+  int32_t axis, Nx, Ny, Nz, d, stage;
+  int64_t Sx, plane;
+  R inv_h, frc2, firho, fc;
+  double wdt;
+  double* g;
+};
+template <class R>
+cudaError_t launch_adj_pml_grad(const AdjPmlArgs<R>& a, int nsm, cudaStream_t s);
+
+// Gradient with respect to the source strengths sval[q] and the waveform samples u_s[nn] from one
+// stage (the stage kernel adds w * unit * sval[q] * u_s[nn] to p at the source cell, unit =
+// dt c^2 rho A_s / h^3): gsval[q] += lp w unit amp(nn), gwave[q][nn] += lp w unit sval[q].
+template <class R>
+cudaError_t launch_adj_source(const R* lp, const int64_t* cell, int nsrc, const double* sval, double unit,
+                              const R* u_s, int64_t n_us, int src_opt, const R* freq, R half_dt, double w, int64_t nn,
+                              double* gsval, double* gwave, cudaStream_t s);
+
 // fused adjoint of one stage kernel launch over the interior cells, grid (x tiles, y tiles, z chunks)
 template <class R>
 cudaError_t launch_adj_stage(const AdjStageArgs<R>& a, dim3 grid, cudaStream_t s);
@@ -130,10 +165,11 @@ cudaError_t launch_adj_band(int stage, const AdjBandArgs<R>& a, cudaStream_t s);
 // grad[m][e] = sum over the band cells of material m of gcell[e][b]
 cudaError_t launch_adj_grad_reduce(const int4* rec, const double* gcell, int64_t nB, int P, int nMat, double* grad,
                                    cudaStream_t s);
-// adjoint of the receiver gather: lp[cell_r] += 2 (ir[r][n] - target[r][n])
+// adjoint of the receiver gather: lp[cell_r] += 2 (ir[r][n] - target[r][n]), or += target[r][n]
+// when target holds a cotangent of the traces
 template <class R>
 cudaError_t launch_adj_receivers(R* lp, const int64_t* rcell, int nrec, const double* ir, int64_t cap,
-                                 const double* target, int64_t tlen, int64_t n, cudaStream_t s);
+                                 const double* target, int64_t tlen, int64_t n, int cotangent, cudaStream_t s);
 // zero every field value of cells no kernel writes (class bytes without UPDATE or BAND)
 template <class R>
 cudaError_t launch_clear_inactive(R* f, const uint8_t* cls, int64_t n, cudaStream_t s);

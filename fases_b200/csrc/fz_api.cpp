@@ -144,28 +144,74 @@ int make_field_maps(fz_handle* h) {
 }
 
 // Per-axis cPML coefficient table, restated from functions3D.cuh:689-723 (evaluated once here in
-// FP64 instead of powf/expf/logf per cell and stage).
+// FP64 instead of powf/expf/logf per cell and stage), with the profile constants taken from
+// fz_params. The entries are carried as values with their derivatives with respect to
+// (pml_R0, pml_kappa_max, pml_alpha_max), which the adjoint uses for the cPML gradient.
+struct D3 {
+  double v, g[3];
+};
+D3 dconst(double v) { return D3{v, {0.0, 0.0, 0.0}}; }
+D3 operator+(D3 a, D3 b) { return D3{a.v + b.v, {a.g[0] + b.g[0], a.g[1] + b.g[1], a.g[2] + b.g[2]}}; }
+D3 operator-(D3 a, D3 b) { return D3{a.v - b.v, {a.g[0] - b.g[0], a.g[1] - b.g[1], a.g[2] - b.g[2]}}; }
+D3 operator*(D3 a, D3 b) {
+  D3 r{a.v * b.v, {}};
+  for (int q = 0; q < 3; q++) r.g[q] = a.g[q] * b.v + a.v * b.g[q];
+  return r;
+}
+D3 operator/(D3 a, D3 b) {
+  D3 r{a.v / b.v, {}};
+  for (int q = 0; q < 3; q++) r.g[q] = (a.g[q] * b.v - a.v * b.g[q]) / (b.v * b.v);
+  return r;
+}
+D3 dexp(D3 a) {
+  D3 r{std::exp(a.v), {}};
+  for (int q = 0; q < 3; q++) r.g[q] = r.v * a.g[q];
+  return r;
+}
+}  // namespace
+
+namespace fzi {
+void pml_entry(const fz_params& p, int N, int lo, int hi, int i, PmlEntry* out) {
+  const int d = p.pml_cells, ng = GHOST;
+  const double m = p.pml_order;
+  // pref = (m+1) c ln(1/R0) / (2 d h); d pref / d R0 = -(m+1) c / (2 d h R0)
+  const D3 pref{0.5 * p.c * (m + 1.0) * std::log(1.0 / p.pml_R0) / ((double)d * p.h),
+                {-0.5 * p.c * (m + 1.0) / ((double)d * p.h * p.pml_R0), 0.0, 0.0}};
+  const D3 kappa_max{p.pml_kappa_max, {0.0, 1.0, 0.0}};
+  const D3 alpha_max{p.pml_alpha_max, {0.0, 0.0, 1.0}};
+  const D3 alpha_min = dconst(0.1) * alpha_max;
+  const double xm = std::min(1.0, std::max(0.0, ((double)(ng + d) - i) / d));
+  const double xp = std::min(1.0, std::max(0.0, (i - ((double)(N - 1 - ng) - d)) / d));
+  const D3 sig = dconst(lo) * pref * dconst(std::pow(xm, m)) + dconst(hi) * pref * dconst(std::pow(xp, m));
+  const double dep = lo * xm + hi * xp;
+  const D3 kap = dconst(1.0) + (kappa_max - dconst(1.0)) * dconst(std::pow(dep, m));
+  const D3 alp = alpha_min + (alpha_max - alpha_min) * dconst(1.0 - dep);
+  const bool in = (lo && i >= ng && i < ng + d) || (hi && i >= N - ng - d && i <= N - 1 - ng);
+  out->tile = in ? ((i < ng + d) ? (i - ng) : (i - (N - ng - d) + d)) : -1;
+  const D3 kinv1 = dconst(1.0) / kap - dconst(1.0);
+  const D3 b = dexp(dconst(0.0) - (alp + sig / kap) * dconst(p.dt));
+  const D3 ca = (sig.v > 0.0) ? (sig / (kap * (sig + kap * alp))) * (b - dconst(1.0)) : dconst(0.0);
+  const D3* e[3] = {&kinv1, &b, &ca};
+  for (int q = 0; q < 3; q++) {
+    out->v[q] = e[q]->v;
+    for (int r = 0; r < 3; r++) out->d[q][r] = e[q]->g[r];
+  }
+}
+}  // namespace fzi
+
+namespace {
+
 template <class R>
 std::vector<fz::PmlCoef<R>> pml_table(int N, int lo, int hi, const fz_params& p) {
-  const int d = p.pml_cells, ng = GHOST;
-  const double lnR0 = std::log(1.0 / 1e-7), m = 2.0;
-  const double kappa_max = 5.0, alpha_max = M_PI * 20.0, alpha_min = 0.1 * alpha_max;
-  const double pref = 0.5 * p.c * (m + 1.0) * lnR0 / ((double)d * p.h);
   std::vector<fz::PmlCoef<R>> t((size_t)N);
   for (int i = 0; i < N; i++) {
-    const double xm = std::min(1.0, std::max(0.0, ((double)(ng + d) - i) / d));
-    const double xp = std::min(1.0, std::max(0.0, (i - ((double)(N - 1 - ng) - d)) / d));
-    const double sig = lo * pref * std::pow(xm, m) + hi * pref * std::pow(xp, m);
-    const double dep = lo * xm + hi * xp;
-    const double kap = 1.0 + (kappa_max - 1.0) * std::pow(dep, m);
-    const double alp = alpha_min + (alpha_max - alpha_min) * (1.0 - dep);
-    const bool in = (lo && i >= ng && i < ng + d) || (hi && i >= N - ng - d && i <= N - 1 - ng);
+    fzi::PmlEntry e;
+    fzi::pml_entry(p, N, lo, hi, i, &e);
     fz::PmlCoef<R> c;
-    c.tile = in ? ((i < ng + d) ? (i - ng) : (i - (N - ng - d) + d)) : -1;
-    c.kinv1 = (R)(1.0 / kap - 1.0);
-    const double b = std::exp(-(alp + sig / kap) * p.dt);
-    c.b = (R)b;
-    c.ca = (R)((sig > 0.0) ? (sig / (kap * (sig + kap * alp))) * (b - 1.0) : 0.0);
+    c.tile = e.tile;
+    c.kinv1 = (R)e.v[0];
+    c.b = (R)e.v[1];
+    c.ca = (R)e.v[2];
     t[(size_t)i] = c;
   }
   return t;
@@ -756,6 +802,10 @@ int fz_params_init(fz_params* p) {
   p->rho = (double)1.225f;
   p->dt = 0.5 * p->h / p->c;
   p->tol_cells = 3.0;
+  p->pml_R0 = 1e-7;  // functions3D.cuh:692-719
+  p->pml_kappa_max = 5.0;
+  p->pml_alpha_max = M_PI * 20.0;
+  p->pml_order = 2.0;
   return FZ_OK;
 }
 
@@ -772,6 +822,10 @@ int fz_create(const fz_params* p, fz_handle** out) {
       (p->precision != FZ_FP32 && p->precision != FZ_FP64) || !(p->tol_cells > 1.0))
     return fzi::set_global_error(FZ_EINVAL, "fz_create: invalid parameter (h, c, rho, dt > 0; pml_cells >= 1; "
                                             "precision FZ_FP32/FZ_FP64; tol_cells > 1)");
+  if (!(p->pml_R0 > 0 && p->pml_R0 < 1) || !(p->pml_kappa_max >= 1) || !(p->pml_alpha_max >= 0) ||
+      !(p->pml_order > 0))
+    return fzi::set_global_error(FZ_EINVAL, "fz_create: invalid cPML profile (0 < pml_R0 < 1, pml_kappa_max >= 1, "
+                                            "pml_alpha_max >= 0, pml_order > 0)");
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess || ndev <= 0)

@@ -123,6 +123,15 @@ namespace fzi {
 int set_error(fz_handle* h, int code, const std::string& msg);
 int set_global_error(int code, const std::string& msg);
 int cuda_fail(fz_handle* h, cudaError_t e, const char* what);
+// one cPML table entry of an axis of N cells (lo / hi: faces enabled): the psi tile index (-1
+// outside the layer), the values (1/kappa - 1, b, ca) and d[value][param], the derivatives with
+// respect to (pml_R0, pml_kappa_max, pml_alpha_max)
+struct PmlEntry {
+  int tile;
+  double v[3];
+  double d[3][3];
+};
+void pml_entry(const fz_params& p, int N, int lo, int hi, int i, PmlEntry* out);
 // finalises the handle's setup (materials, sources, receivers, launch geometry); idempotent
 int prepare(fz_handle* h);
 // enqueues one time step on the handle's stream (or into the capture the stream takes part in)

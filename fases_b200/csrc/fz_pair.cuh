@@ -48,4 +48,77 @@ __device__ __forceinline__ typename Pair<R>::T psplat(R x) {
   return pmk(x, x);
 }
 
+// ------------------------------------------------------------------------------------------
+// WENO-Z reconstruction at one cell centre (Borges, Carmona, Costa & Don 2008, q = 1), the scheme
+// of functions3D.cuh:763-1001 with the tables of main3D.cu:834-843 and eps = 1e-10 (main3D.cu:770).
+//
+// The reference evaluates V-(i+1/2) (idx = 1) and V+(i-1/2) (idx = 0) of a cell in two separate
+// calls; both use the same three smoothness indicators and the same factors (1 + tau/(beta+eps)),
+// and differ only in the linear weights d (mirrored) and the candidate rows. This evaluates them
+// together, written on first differences a..d of the five-point stencil:
+//   candidates:  u_i + delta_r,   V = u_i + sum_r w_r delta_r,   w_r = d_r q_r / sum d q
+//   12/13 beta_r = (second difference)^2 + 3/13 (one-sided first-derivative term)^2
+// (the 12/13 scaling is absorbed into eps).
+// ------------------------------------------------------------------------------------------
+template <class R>
+__device__ __forceinline__ void weno_core(typename Pair<R>::T a, typename Pair<R>::T b, typename Pair<R>::T c,
+                                          typename Pair<R>::T d, typename Pair<R>::T D2, typename Pair<R>::T D1,
+                                          typename Pair<R>::T D0, typename Pair<R>::T q0, typename Pair<R>::T& vm,
+                                          typename Pair<R>::T& vp) {
+  typedef typename Pair<R>::T P;
+  const P E2 = pfma(b, psplat<R>(R(2)), D2);   // u_{i-2} - 4u_{i-1} + 3u_i
+  const P E1 = padd(b, c);                     // -(u_{i-1} - u_{i+1})
+  const P E0 = pfma(c, psplat<R>(R(-2)), D0);  // 3u_i - 4u_{i+1} + u_{i+2} (sign)
+  // 12/13 (beta_r + eps) = D_r^2 + 3/13 E_r^2 + 12/13 eps
+  const P k313 = psplat<R>(R(3.0 / 13.0));
+  const P eps = psplat<R>(R(1e-10 * 12.0 / 13.0));
+  const P B0 = pfma(D0, D0, pfma(pmul(E0, k313), E0, eps));
+  const P B1 = pfma(D1, D1, pfma(pmul(E1, k313), E1, eps));
+  const P B2 = pfma(D2, D2, pfma(pmul(E2, k313), E2, eps));
+  const P tau = pabs(psub(B0, B2));
+  const P one = psplat<R>(R(1));
+  const P q0w = pfma(tau, prcp(B0), one);
+  const P q1w = pfma(tau, prcp(B1), one);
+  const P q2w = pfma(tau, prcp(B2), one);
+  // normalisers: V- uses d = (3/10, 3/5, 1/10), V+ the mirrored (1/10, 3/5, 3/10)
+  const P t1 = pmul(q1w, psplat<R>(R(0.6)));
+  const P Sm = pfma(q0w, psplat<R>(R(0.3)), pfma(q2w, psplat<R>(R(0.1)), t1));
+  const P Sp = pfma(q0w, psplat<R>(R(0.1)), pfma(q2w, psplat<R>(R(0.3)), t1));
+  // d_r * delta_r for both faces, written on the first and second differences:
+  //   em0 = 0.15 c - 0.05 D0      ep0 = -0.05 c + D0/30
+  //   em1 = 0.15 E1 + 0.05 D1     ep1 = -0.15 E1 + 0.05 D1
+  //   em2 = 0.05 b + D2/30        ep2 = -0.15 b - 0.05 D2
+  const P h1 = pmul(D1, psplat<R>(R(0.05)));
+  const P em0 = pfma(c, psplat<R>(R(0.15)), pmul(D0, psplat<R>(R(-0.05))));
+  const P ep0 = pfma(c, psplat<R>(R(-0.05)), pmul(D0, psplat<R>(R(1.0 / 30.0))));
+  const P em1 = pfma(E1, psplat<R>(R(0.15)), h1);
+  const P ep1 = pfma(E1, psplat<R>(R(-0.15)), h1);
+  const P em2 = pfma(b, psplat<R>(R(0.05)), pmul(D2, psplat<R>(R(1.0 / 30.0))));
+  const P ep2 = pfma(b, psplat<R>(R(-0.15)), pmul(D2, psplat<R>(R(-0.05))));
+  const P Nm = pfma(q2w, em2, pfma(q1w, em1, pmul(q0w, em0)));
+  const P Np = pfma(q2w, ep2, pfma(q1w, ep1, pmul(q0w, ep0)));
+  vm = pfma(Nm, prcp(Sm), q0);
+  vp = pfma(Np, prcp(Sp), q0);
+}
+
+template <class R>
+__device__ __forceinline__ void weno_center(typename Pair<R>::T qm2, typename Pair<R>::T qm1,
+                                            typename Pair<R>::T q0, typename Pair<R>::T qp1,
+                                            typename Pair<R>::T qp2, typename Pair<R>::T& vm,
+                                            typename Pair<R>::T& vp) {
+  typedef typename Pair<R>::T P;
+  const P a = psub(qm1, qm2), b = psub(q0, qm1), c = psub(qp1, q0), d = psub(qp2, qp1);
+  weno_core<R>(a, b, c, d, psub(b, a), psub(c, b), psub(d, c), q0, vm, vp);
+}
+
+// Godunov (exact Riemann) flux of linear acoustics for a (pressure, normal velocity) pair
+// (functions3D.cuh:56-78):  F_p = 1/2 (rho c^2 (q+ + q-) - c (p+ - p-)),
+//                           F_q = 1/2 ((p+ + p-)/rho - c (q+ - q-)).
+template <class R>
+__device__ __forceinline__ typename Pair<R>::T godunov(typename Pair<R>::T vm, typename Pair<R>::T vp,
+                                                       typename Pair<R>::T kA, typename Pair<R>::T kC) {
+  const typename Pair<R>::T sum = padd(vm, vp), dif = psub(vp, vm);
+  return pfma(dif, kC, pmul(pswap(sum), kA));
+}
+
 }  // namespace fz

@@ -19,11 +19,13 @@ def _dptr(a):
 
 
 def params(h=0.02, c=None, rho=None, dt=None, cfl=0.5, pml=(0, 0, 0, 0, 0, 0), pml_cells=20,
-           precision="fp32", device=0, tol_cells=3.0, two_d=False, batch=1):
+           precision="fp32", device=0, tol_cells=3.0, two_d=False, batch=1, pml_R0=None, pml_kappa_max=None,
+           pml_alpha_max=None, pml_order=None):
     """Solver parameters. c/rho default to the reference's 20 degC air (main3D.cu:450-456);
     dt = cfl*h/c (main3D.cu:729-730). pml = (U, D, R, L, F, B) face keys (main3D.cu:155-160).
     batch > 1 steps that many independent field sets (one per source position) over the same
-    room in the same launches."""
+    room in the same launches. pml_R0 / pml_kappa_max / pml_alpha_max / pml_order override the
+    reference's cPML profile constants (1e-7, 5, 20 pi, 2; functions3D.cuh:689-723)."""
     p = FzParams()
     check(lib().fz_params_init(C.byref(p)))
     p.precision = _abi.FZ_FP64 if precision == "fp64" else _abi.FZ_FP32
@@ -40,6 +42,10 @@ def params(h=0.02, c=None, rho=None, dt=None, cfl=0.5, pml=(0, 0, 0, 0, 0, 0), p
     p.tol_cells = float(tol_cells)
     p.two_d = 1 if two_d else 0
     p.batch = int(batch)
+    for name, v in (("pml_R0", pml_R0), ("pml_kappa_max", pml_kappa_max), ("pml_alpha_max", pml_alpha_max),
+                    ("pml_order", pml_order)):
+        if v is not None:
+            setattr(p, name, float(v))
     return p
 
 
@@ -58,6 +64,9 @@ class Solver:
         self.batch = max(1, int(prm.batch)) if prm is not None else 1
         self._nrec = 0
         self._cap = 0
+        self._nsrc = 0
+        self._n_us = 0
+        self._src_opt = 0
 
     # -- lifetime --------------------------------------------------------------------------
     def close(self):
@@ -115,6 +124,9 @@ class Solver:
         self._chk(lib().fz_set_sources(self._h, cells.shape[0], cells.ctypes.data_as(C.POINTER(C.c_int32)),
                                        _dptr(sval), int(src_opt), _dptr(fr), _dptr(us),
                                        0 if us is None else us.size))
+        self._nsrc = cells.shape[0]
+        self._n_us = 0 if us is None else us.size
+        self._src_opt = int(src_opt)
 
     def set_source_members(self, member):
         """Batched solves: the batch member (0 .. batch-1, or -1 for all) of each source of the last
@@ -252,11 +264,16 @@ class Solver:
         self._chk(lib().fz_material_layout(self._h, C.byref(n), C.byref(k), C.byref(l)))
         return n.value, k.value, l.value
 
-    def misfit_gradient(self, target, nsteps=None, segment_steps=250):
-        """J = sum (IR - target)^2 over nsteps steps from the current (step-0) state and dJ/d(ADE
-        coefficients) by the discrete adjoint. target: [n_rec, >= nsteps]. Returns a dict with J,
-        the gradient split per coefficient (arrays [nMat], [nMat, K] or [nMat, L]), the raw
-        [nMat, 1 + 2K + 4L] array and the forward / backward device times in ms."""
+    def misfit_gradient(self, target, nsteps=None, segment_steps=250, sources=False, pml=False, initial=False,
+                        cotangent=False):
+        """J = sum (IR - target)^2 over nsteps steps from the current (step-0) state and its gradient
+        by the discrete adjoint; with cotangent=True, `target` is a cotangent g of the traces, J =
+        sum g IR and the gradients are the vector-Jacobian products sum g dIR/dtheta. target:
+        [n_rec, >= nsteps]. Returns a dict with J, the ADE-coefficient gradient split per coefficient
+        (arrays [nMat], [nMat, K] or [nMat, L]) and as the raw [nMat, 1 + 2K + 4L] array, the
+        forward / backward device times in ms, and on request: sources -> "sval" [nsrc] (dJ/dsval)
+        and "wave" [nsrc, n_us] (dJ/du_s per source, PCS / Ricker waveforms); pml -> "pml" {R0,
+        kappa_max, alpha_max}; initial -> "initial" (p, u, v, w) gradients, each [Nz, Ny, Nx]."""
         target = np.ascontiguousarray(target, dtype=np.float64)
         if target.ndim != 2 or target.shape[0] != self._nrec:
             raise ValueError("target must be [n_rec, n_steps]")
@@ -266,12 +283,35 @@ class Solver:
         grad = np.zeros((nm, P), np.float64)
         J = C.c_double()
         ms = (C.c_double * 2)()
-        self._chk(lib().fz_misfit_gradient(self._h, nsteps, int(segment_steps), _dptr(target), target.shape[1],
-                                           C.byref(J), _dptr(grad), grad.size, ms))
+        g = _abi.FzGradients()
+        g.cotangent = 1 if cotangent else 0
+        g.materials, g.materials_cap = _dptr(grad), grad.size
+        keep = {}
+        if sources:
+            n_us = 0 if self._src_opt == 2 else self._n_us
+            keep["sval"] = np.zeros(self._nsrc, np.float64)
+            keep["wave"] = np.zeros((self._nsrc, n_us), np.float64)
+            g.source_sval, g.source_sval_cap = _dptr(keep["sval"]), keep["sval"].size
+            g.source_wave, g.source_wave_cap = _dptr(keep["wave"]), keep["wave"].size
+        if pml:
+            keep["pml"] = np.zeros(4, np.float64)
+            g.pml, g.pml_cap = _dptr(keep["pml"]), 4
+        if initial:
+            keep["initial"] = np.zeros((4,) + tuple(self.shape), np.float64)
+            g.initial, g.initial_cap = _dptr(keep["initial"]), keep["initial"].size
+        self._chk(lib().fz_misfit_gradient_ex(self._h, nsteps, int(segment_steps), _dptr(target), target.shape[1],
+                                              C.byref(J), C.byref(g), ms))
         o = 1 + 2 * K
-        return {"J": J.value, "raw": grad, "Rinf": grad[:, 0], "A": grad[:, 1:1 + K], "zeta": grad[:, 1 + K:o],
-                "B": grad[:, o:o + L], "C": grad[:, o + L:o + 2 * L], "alpha": grad[:, o + 2 * L:o + 3 * L],
-                "beta": grad[:, o + 3 * L:o + 4 * L], "forward_ms": ms[0], "backward_ms": ms[1]}
+        out = {"J": J.value, "raw": grad, "Rinf": grad[:, 0], "A": grad[:, 1:1 + K], "zeta": grad[:, 1 + K:o],
+               "B": grad[:, o:o + L], "C": grad[:, o + L:o + 2 * L], "alpha": grad[:, o + 2 * L:o + 3 * L],
+               "beta": grad[:, o + 3 * L:o + 4 * L], "forward_ms": ms[0], "backward_ms": ms[1]}
+        if sources:
+            out["sval"], out["wave"] = keep["sval"], keep["wave"]
+        if pml:
+            out["pml"] = {"R0": keep["pml"][0], "kappa_max": keep["pml"][1], "alpha_max": keep["pml"][2]}
+        if initial:
+            out["initial"] = tuple(keep["initial"][f] for f in range(4))
+        return out
 
     def energy(self):
         e = C.c_double()

@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define FZ_ABI_VERSION 1
+#define FZ_ABI_VERSION 2
 
 /* status codes */
 #define FZ_OK 0
@@ -81,10 +81,18 @@ typedef struct fz_params {
                           (main3D.cu:1278, driven per source by common/gui.py). Host-side arrays of
                           fz_set_fields / fz_get_fields hold batch grids one after another; receiver
                           traces are [batch][n_rec][n_steps]. */
+  /* cPML profile (functions3D.cuh:689-723; the reference's constants are the defaults):
+   * sigma = (m+1) c ln(1/R0) / (2 d h) x^m, kappa = 1 + (kappa_max - 1) x^m,
+   * alpha = alpha_max (0.1 + 0.9 (1 - x)), x = depth / d, m = pml_order. */
+  double pml_R0;        /* target reflection (1e-7) */
+  double pml_kappa_max; /* (5) */
+  double pml_alpha_max; /* (20 pi) */
+  double pml_order;     /* m (2) */
 } fz_params;
 
 /* Fills p with the reference defaults: FP32, device 0, 20 PML cells, no PML faces, h = 0.02,
- * T = 20 degC -> c = sqrt(1.4*287.05*293.15), rho = 1.225, CFL 0.5, tol = 3h. */
+ * T = 20 degC -> c = sqrt(1.4*287.05*293.15), rho = 1.225, CFL 0.5, tol = 3h, cPML R0 = 1e-7,
+ * kappa_max = 5, alpha_max = 20 pi, order 2. */
 int fz_params_init(fz_params* p);
 
 /* Creates a solver on p->device. Replaces main3D.cu:235-293 (device probe) and the allocation
@@ -230,6 +238,33 @@ void fz_group_destroy(fz_group* g);
  * absorption and never differentiates the solver). */
 int fz_misfit_gradient(fz_handle* h, int64_t nsteps, int32_t segment_steps, const double* target,
                        int64_t target_steps, double* J, double* grad, int64_t grad_cap, double* ms);
+
+/* Outputs of fz_misfit_gradient_ex; every pointer may be NULL (not computed), each *_cap is its
+ * element count and must hold the size given. */
+typedef struct fz_gradients {
+  int32_t cotangent;     /* 0: J = sum (IR - target)^2 as fz_misfit_gradient. 1: target holds a
+                            cotangent g[r][n] of the receiver traces; J = sum g IR and every
+                            gradient is the vector-Jacobian product sum g dIR/dtheta */
+  double* materials;     /* [nMat][1 + 2K + 4L], as fz_misfit_gradient's grad */
+  int64_t materials_cap;
+  double* source_sval;   /* [nsrc]: d J / d sval[q] (fz_set_sources' source strengths) */
+  int64_t source_sval_cap;
+  double* source_wave;   /* [nsrc][n_us]: d J / d u_s[nn] through source q (PCS / Ricker waveforms;
+                            summing over q gives the gradient of the shared waveform) */
+  int64_t source_wave_cap;
+  double* pml;           /* [4]: d J / d (pml_R0, pml_kappa_max, pml_alpha_max) and 0 for pml_order */
+  int64_t pml_cap;
+  double* initial;       /* [4][Nx*Ny*Nz]: d J / d (p, u, v, w) of the step-0 state in the reference
+                            layout; 0 at cells no kernel writes (solid interior) */
+  int64_t initial_cap;
+} fz_gradients;
+
+/* fz_misfit_gradient with the gradients of fz_gradients: the ADE coefficients, the source
+ * strengths and waveform samples, the cPML profile parameters and the initial fields, from one
+ * forward pass with checkpoints and one reverse sweep. Same conditions, schedule and memory as
+ * fz_misfit_gradient, plus one psi-tile set per segment step when the cPML gradient is asked for. */
+int fz_misfit_gradient_ex(fz_handle* h, int64_t nsteps, int32_t segment_steps, const double* target,
+                          int64_t target_steps, double* J, fz_gradients* out, double* ms);
 
 /* Material table layout after setup: number of materials (>= 1) and the real-pole / complex-pair
  * counts K, L (each >= 1, zero-padded as read_fit_file pads, common/filterABC.h:52-89). */

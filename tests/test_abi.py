@@ -31,7 +31,7 @@ def test_binding_table_covers_header():
 def test_params_struct_layout_matches_header():
     p = _abi.FzParams()
     assert _abi.lib().fz_params_init(ctypes.byref(p)) == 0
-    assert p.abi_version == 1 and p.pml_cells == 20 and abs(p.tol_cells - 3.0) < 1e-15
+    assert p.abi_version == 2 and p.pml_cells == 20 and abs(p.tol_cells - 3.0) < 1e-15
     # c at 20 degC in the reference's float arithmetic (main3D.cu:450-456)
     T = np.float32(20.0) + np.float32(273.15)
     c = np.sqrt(np.float32(1.4) * np.float32(287.05) * T, dtype=np.float32)
