@@ -308,11 +308,13 @@ def run_batched(args):
     room = 192 ** 3
     single = _batched_solver(b, "fp32", steps_a + 20, cells[:1], us, 1.0 / pk)
     single.run(20)
+    depth_single, _ = single.autotune()  # both arms on their own tuned tile depth
     ms_single = single.run_timed(steps_a)
     ir_single = single.ir()
     single.close()
     bat = _batched_solver(b, "fp32", steps_a + 20, cells, us, 1.0 / pk, batch=nsrc, members=np.arange(nsrc))
     bat.run(20)
+    depth_batch, _ = bat.autotune()
     ms_batch = bat.run_timed(steps_a)
     ir_batch = bat.ir()
     bat.close()
@@ -324,6 +326,7 @@ def run_batched(args):
         "per_source_speedup": per_src_batch / per_src_single, "steps": steps_a,
         "ms_per_step_batch": ms_batch / steps_a, "ms_per_step_single": ms_single / steps_a,
         "member0_bitwise_equal_single": bool(np.array_equal(ir_batch[0], ir_single)),
+        "tile_depth": {"single": depth_single, "batch": depth_batch, "chosen_by": "fz_autotune"},
         "config": {"workload": "192^3 shoebox, 5 rigid obstacles, 6 ADE walls (2 real + 2 complex poles), "
                                "20-cell cPML on one face, 64 seeded PCS source positions, 8 receivers, FP32",
                    "sources": nsrc, "room_cells": room}}
@@ -345,8 +348,10 @@ def run_batched(args):
         cells_b += r[0] * r[1] * r[2]
     ms_seq = 0.0
     for solo, _ in solvers:
+        solo.autotune()  # each room alone on its own tuned tile depth
         ms_seq += solo.run_timed(steps_b)
     grp = Group([g for _, g in solvers])
+    depth_grp, _ = grp.autotune()
     ms_grp = grp.run_timed(steps_b)
     same = all(np.array_equal(solo.ir(), g.ir()) for solo, g in solvers)
     grp.close()
@@ -358,6 +363,7 @@ def run_batched(args):
         "value": cells_b * steps_b / (ms_grp / 1e3) / 1e9, "unit": UNIT,
         "sequential_value": cells_b * steps_b / (ms_seq / 1e3) / 1e9, "per_room_speedup": ms_seq / ms_grp,
         "steps": steps_b, "ms_group": ms_grp, "ms_sequential": ms_seq, "members_bitwise_equal_solo": same,
+        "tile_depth_group": depth_grp,
         "config": {"workload": "32 shoeboxes, edges uniform in [64, 160] cells (seed 45), 2 rigid obstacles, "
                                "6 ADE walls, cPML face, PCS source, 4 receivers each, FP32",
                    "rooms": rooms, "room_cells_total": cells_b}}
@@ -423,6 +429,8 @@ def main():
     s = make_solver(b, args.precision, nsteps_total + 31, device=local)
     info = s.info()
     s.run(args.warmup)
+    depth, _ = s.autotune()  # tile depth of the stage kernels, timed on this room
+    depth_heuristic = s.kz_chunk()[1]
     barrier(pg)
     # the timed steps: CUDA graphs of 10 steps, as fz_run issues them
     with Clocks(local) as clk:
@@ -473,6 +481,7 @@ def main():
     e.set_materials(m["Rinf"], m["A"], m["zeta"], m["B"], m["Cc"], m["alpha"], m["beta"])
     e.set_receivers(b["receivers"], ne)
     e.set_fields(p=b["p0"])
+    e.autotune()
     e.run(ne)
     ir = e.ir()
     vel = e.vel()
@@ -483,7 +492,7 @@ def main():
     d2h = ir.nbytes + vel.nbytes
     e2e = {"value": world * room_cells * ne / t_e2e / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d / ne,
            "d2h_bytes_per_step": d2h / ne, "steps": ne, "seconds": t_e2e,
-           "timer": "host wall clock around create, geometry/material/field upload, run, IR/VEL readback"}
+           "timer": "host wall clock around create, geometry/material/field upload, autotune, run, IR/VEL readback"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -503,7 +512,9 @@ def main():
                        "room_cells": room_cells, "padded_cells": int(np.prod(info["dims"])),
                        "band_cells": info["n_band"], "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (3 field sets of 4 x 183 MB)",
-                       "value_per_padded_cell": value * np.prod(info["dims"]) / room_cells},
+                       "value_per_padded_cell": value * np.prod(info["dims"]) / room_cells,
+                       "tile": {"columns": [32, 16], "depth": depth, "heuristic_depth": depth_heuristic,
+                                "chosen_by": "fz_autotune"}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": "k_stage (fused WENO-Z/Godunov/RK/cPML/source), 131/3 B per room cell per launch",

@@ -118,6 +118,10 @@ SIGNATURES = {
     "fz_state_load": (C.c_int, [_P, _P, _i64]),
     "fz_misfit_gradient": (C.c_int, [_P, _i64, _i32, _dp, _i64, _dp, _dp, _i64, _dp]),
     "fz_misfit_gradient_ex": (C.c_int, [_P, _i64, _i32, _dp, _i64, _dp, C.POINTER(FzGradients), _dp]),
+    "fz_autotune": (C.c_int, [_P, _i32, _ip, _dp]),
+    "fz_group_autotune": (C.c_int, [_P, _i32, _ip, _dp]),
+    "fz_set_kz_chunk": (C.c_int, [_P, _i32]),
+    "fz_get_kz_chunk": (C.c_int, [_P, _ip, _ip]),
     "fz_material_layout": (C.c_int, [_P, _ip, _ip, _ip]),
     "fz_group_create": (C.c_int, [C.POINTER(_P), _i32, C.POINTER(_P)]),
     "fz_group_run": (C.c_int, [_P, _i64]),

@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libfz.so")
 SOURCES = ["fz_kernels.cu", "fz_adjoint.cu", "fz_geometry.cu", "fz_api.cpp", "fz_project.cpp", "fz_group.cpp",
-           "fz_adjoint.cpp", "fz_noalloc.cu"]
+           "fz_adjoint.cpp", "fz_noalloc.cu", "fz_tune.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

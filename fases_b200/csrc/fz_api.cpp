@@ -451,11 +451,9 @@ int finalize(fz_handle* h) {
       best = nk;
     }
   }
-  h->kz_chunk = (nzi + best - 1) / best;
-  int nkz = (nzi + h->kz_chunk - 1) / h->kz_chunk;
-  h->zchunks = nkz;
-  h->stage_grid = dim3((unsigned)ntx, (unsigned)nty, (unsigned)(nkz * h->nb));
+  h->kz_heuristic = (nzi + best - 1) / best;
   h->finalized = true;
+  fzi::set_kz_chunk(h, h->kz_chunk > 0 ? h->kz_chunk : 0);
   return FZ_OK;
 }
 
@@ -564,23 +562,28 @@ struct Timer {
   }
 };
 
+template <class R>
+cudaError_t enqueue_stage_kernel(fz_handle* h, int st) {
+  const int in_set = (st == 0) ? h->i0 : (st == 1) ? h->i1 : h->i2;
+  fz::StageMaps m;
+  m.p = h->halo_map[in_set][0];
+  m.u = h->halo_map[in_set][1];
+  m.v = h->halo_map[in_set][2];
+  m.bp = h->own_map[h->i0][0];
+  m.bu = h->own_map[h->i0][1];
+  m.bv = h->own_map[h->i0][2];
+  m.bw = h->own_map[h->i0][3];
+  m.cls = h->cls_map;
+  return fz::launch_stage<R>(st, h->prm.two_d != 0, stage_args<R>(h, st), m, h->stage_grid, h->stream);
+}
+
 // Stage st of the current step: the stage kernel, then the immersed band (main3D.cu:1286-1306).
 template <class R>
 cudaError_t enqueue_stage(fz_handle* h, int st) {
   cudaError_t e;
   {
     Timer t(h, st);
-    const int in_set = (st == 0) ? h->i0 : (st == 1) ? h->i1 : h->i2;
-    fz::StageMaps m;
-    m.p = h->halo_map[in_set][0];
-    m.u = h->halo_map[in_set][1];
-    m.v = h->halo_map[in_set][2];
-    m.bp = h->own_map[h->i0][0];
-    m.bu = h->own_map[h->i0][1];
-    m.bv = h->own_map[h->i0][2];
-    m.bw = h->own_map[h->i0][3];
-    m.cls = h->cls_map;
-    e = fz::launch_stage<R>(st, h->prm.two_d != 0, stage_args<R>(h, st), m, h->stage_grid, h->stream);
+    e = enqueue_stage_kernel<R>(h, st);
     if (e != cudaSuccess) return e;
   }
   if (h->nB > 0) {
@@ -662,6 +665,8 @@ template <class R>
 int load_geometry(fz_handle* h, const float* S, const uint8_t* oid, int Nx, int Ny, int Nz) {
   free_device(h);
   h->finalized = false;
+  h->kz_chunk = 0;  // a new grid starts from the heuristic tile depth
+  h->stage_grid = dim3(0, 0, 0);
   h->Nx = Nx; h->Ny = Ny; h->Nz = Nz;
   h->Sx = ((int64_t)Nx + XOFF + 31) / 32 * 32;
   h->plane = h->Sx * Ny;
@@ -779,6 +784,27 @@ int prepare(fz_handle* h) {
 cudaError_t enqueue(fz_handle* h) { return h->fp64 ? enqueue_step<double>(h) : enqueue_step<float>(h); }
 cudaError_t enqueue_stage(fz_handle* h, int st) {
   return h->fp64 ? ::enqueue_stage<double>(h, st) : ::enqueue_stage<float>(h, st);
+}
+cudaError_t enqueue_stage_kernel(fz_handle* h, int st) {
+  return h->fp64 ? ::enqueue_stage_kernel<double>(h, st) : ::enqueue_stage_kernel<float>(h, st);
+}
+void set_kz_chunk(fz_handle* h, int kz_chunk) {
+  const int nzi = h->Nz - 2 * GHOST;
+  const int c = std::max(1, std::min(nzi, kz_chunk > 0 ? kz_chunk : h->kz_heuristic));
+  const int ntx = (h->Nx - 2 * GHOST + fz::TX - 1) / fz::TX;
+  const int nty = (h->Ny - 2 * GHOST + fz::TY - 1) / fz::TY;
+  const dim3 grid((unsigned)ntx, (unsigned)nty, (unsigned)(((nzi + c - 1) / c) * h->nb));
+  const bool same = (c == h->kz_chunk) && grid.x == h->stage_grid.x && grid.y == h->stage_grid.y &&
+                    grid.z == h->stage_grid.z;
+  h->kz_chunk = c;
+  h->zchunks = (nzi + c - 1) / c;
+  h->stage_grid = grid;
+  if (same) return;
+  for (auto& g : h->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
 }
 cudaError_t enqueue_finish(fz_handle* h) { return h->fp64 ? ::enqueue_finish<double>(h) : ::enqueue_finish<float>(h); }
 }  // namespace fzi

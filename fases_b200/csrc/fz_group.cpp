@@ -159,6 +159,26 @@ int fz_group_run(fz_group* g, int64_t nsteps) {
   return FZ_OK;
 }
 
+int fz_group_autotune(fz_group* g, int32_t reps, int32_t* kz_chunk, double* ms_per_step) {
+  if (!g) return fzi::set_global_error(FZ_EINVAL, "fz_group_autotune: NULL group");
+  int rc = fz_group_sync(g, 0);
+  if (rc != FZ_OK) return rc;
+  cudaSetDevice(g->device);
+  // one depth for every member (clamped to each room's planes), or 0: each member's own heuristic
+  int nzmax = 1;
+  for (fz_handle* h : g->m) nzmax = std::max(nzmax, h->Nz - 2 * fz::GHOST);
+  std::vector<int> cand{0};
+  for (int c : {4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256})
+    if (c <= nzmax) cand.push_back(c);
+  int best = 0;
+  rc = fzi::tune(g->m, g->stream, cand, reps, &best, ms_per_step);
+  for (auto& kv : g->graphs) cudaGraphExecDestroy(kv.second);  // captured with the old launch shape
+  g->graphs.clear();
+  if (rc != FZ_OK) return rc;
+  if (kz_chunk) *kz_chunk = best;
+  return FZ_OK;
+}
+
 int fz_group_sync(fz_group* g, int64_t timeout_ms) {
   if (!g) return fzi::set_global_error(FZ_EINVAL, "fz_group_sync: NULL group");
   if (timeout_ms <= 0) timeout_ms = 600000;

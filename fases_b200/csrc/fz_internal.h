@@ -102,6 +102,7 @@ struct fz_handle {
   int64_t steps_enqueued = 0;
   bool finalized = false;
   int kz_chunk = 0;
+  int kz_heuristic = 0;  // the wave-filling choice of prepare (fz_set_kz_chunk(h, 0) returns to it)
   int zchunks = 1;  // z chunks per member
   dim3 stage_grid;
 
@@ -139,4 +140,16 @@ cudaError_t enqueue(fz_handle* h);
 // the parts of one step: stage st (stage kernel + band), then receivers and buffer rotation
 cudaError_t enqueue_stage(fz_handle* h, int st);
 cudaError_t enqueue_finish(fz_handle* h);
+// the stage kernel of stage st alone (no band), on the handle's stream: the autotuner's trial
+cudaError_t enqueue_stage_kernel(fz_handle* h, int st);
+// tile depth of the stage kernels (z planes per CTA; 0 = the wave-filling heuristic); drops the
+// handle's captured graphs
+void set_kz_chunk(fz_handle* h, int kz_chunk);
+// Times the stage kernels of every handle in hs (launched on their own streams, forked from and
+// joined to `ts`) for each candidate tile depth (0 = each handle's heuristic; others are clamped
+// to a handle's planes) and leaves every handle on the fastest; the state is left as it was.
+int tune(const std::vector<fz_handle*>& hs, cudaStream_t ts, const std::vector<int>& candidates, int reps,
+         int* best, double* ms_per_step);
+// the tile depths worth timing for one handle: the heuristic and the best-filling alternatives
+std::vector<int> kz_candidates(fz_handle* h);
 }  // namespace fzi

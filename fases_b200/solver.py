@@ -200,6 +200,24 @@ class Solver:
     def sync(self, timeout_ms=0):
         self._chk(lib().fz_sync(self._h, int(timeout_ms)))
 
+    def autotune(self, reps=3):
+        """Times the stage kernels for the heuristic tile depth (z planes per CTA) and the
+        alternatives worth trying, keeps the fastest and returns (depth, stage ms per step); the
+        solve does not advance and its results do not depend on the depth."""
+        k, ms = C.c_int32(), C.c_double()
+        self._chk(lib().fz_autotune(self._h, int(reps), C.byref(k), C.byref(ms)))
+        return k.value, ms.value
+
+    def set_kz_chunk(self, depth):
+        """Tile depth of the stage kernels (0 = the wave-filling heuristic), e.g. from a cache."""
+        self._chk(lib().fz_set_kz_chunk(self._h, int(depth)))
+
+    def kz_chunk(self):
+        """(current tile depth, heuristic tile depth)."""
+        k, hk = C.c_int32(), C.c_int32()
+        self._chk(lib().fz_get_kz_chunk(self._h, C.byref(k), C.byref(hk)))
+        return k.value, hk.value
+
     def save_state(self, path=None):
         """The solver's complete state (checkpoint) as a uint8 array, also written to `path` if given."""
         n = C.c_int64()
@@ -380,6 +398,13 @@ class Group:
         ms = C.c_double()
         check(lib().fz_group_run_timed(self._g, int(nsteps), C.byref(ms)))
         return ms.value
+
+    def autotune(self, reps=3):
+        """One tile depth for every member, timed with the members' stage kernels side by side
+        (0 = each member's own heuristic); returns (depth, stage ms per step of the group)."""
+        k, ms = C.c_int32(), C.c_double()
+        check(lib().fz_group_autotune(self._g, int(reps), C.byref(k), C.byref(ms)))
+        return k.value, ms.value
 
     def sync(self, timeout_ms=0):
         check(lib().fz_group_sync(self._g, int(timeout_ms)))

@@ -221,6 +221,21 @@ int fz_group_run_timed(fz_group* g, int64_t nsteps, double* ms);
 int fz_group_sync(fz_group* g, int64_t timeout_ms);
 void fz_group_destroy(fz_group* g);
 
+/* Launch-shape autotuner. A stage-kernel CTA covers 32 x 16 columns by kz_chunk planes along z;
+ * the depth sets how many CTAs a stage launches and how whole waves of SMs fill. fz_autotune times
+ * the three stage kernels on this room for the heuristic depth and up to eight alternatives
+ * (reps steps' worth each, after one warm-up) and keeps the fastest; the state is left as it was
+ * (the call does not advance the solve). kz_chunk gets the chosen depth, ms_per_step the stage
+ * kernels' time per step. fz_group_autotune does the same for all members at once, timing their
+ * kernels side by side with one depth for every member (clamped to each room; 0 = each member's
+ * heuristic). Results do not depend on the depth (each CTA recomputes its boundary centres).
+ * The reference launches fixed TP(32,4,4) blocks (main3D.cu:1280-1306). */
+int fz_autotune(fz_handle* h, int32_t reps, int32_t* kz_chunk, double* ms_per_step);
+int fz_group_autotune(fz_group* g, int32_t reps, int32_t* kz_chunk, double* ms_per_step);
+/* Sets the depth directly (0 = the heuristic), e.g. from a cache of earlier tuning results. */
+int fz_set_kz_chunk(fz_handle* h, int32_t kz_chunk);
+int fz_get_kz_chunk(fz_handle* h, int32_t* kz_chunk, int32_t* heuristic);
+
 /* Gradient of the receiver misfit J = sum_r sum_{n < nsteps} (IR_r[n] - target[r][n])^2 (IR_r[n] = p
  * at receiver r after step n+1, FP64) with respect to every ADE coefficient of every material, by
  * the discrete adjoint of the stepping scheme (WENO-Z weights linearised, Godunov flux, RK stages,
