@@ -524,6 +524,7 @@ int fz_misfit_gradient_ex(fz_handle* h, int64_t nsteps, int32_t segment_steps, c
       return fzi::set_error(h, FZ_EINVAL, "fz_misfit_gradient: a source sits in a cell the stage kernels skip");
   }
   cudaSetDevice(h->device);
+  segment_steps = (int32_t)std::min<int64_t>(segment_steps, nsteps);  // no storage for steps never run
   return h->fp64 ? misfit_gradient<double>(h, nsteps, segment_steps, target, target_steps, J, *out, ms)
                  : misfit_gradient<float>(h, nsteps, segment_steps, target, target_steps, J, *out, ms);
 }
