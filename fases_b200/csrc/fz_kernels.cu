@@ -405,17 +405,48 @@ struct Vec4<double> {
 
 // STAGE selects the ADE stage coefficients (a, b, c) = (0,1,1), (3,1,4), (1,2,3)
 // (main3D.cu:1290, 1298, 1306): left = (a middle + b (right + dt L(right))) / c.
-template <class R, int STAGE>
-__global__ void __launch_bounds__(256, 4) k_band(const BandArgs<R> B) {
+// KM, LM > 0: at most KM real poles and LM complex pairs. Every load that does not depend on the
+// probe (the cell's own fields, the ADE states of the stage) is then issued at the top, beside the
+// probe gathers, so one thread keeps ~50 loads in flight; KM = LM = 0 is the general form with
+// the state loads inside the pole loops.
+template <class R, int STAGE, int KM, int LM>
+__global__ void __launch_bounds__(256, (sizeof(R) == 4 && KM > 0 && KM <= 2) ? 4 : 3) k_band(const BandArgs<R> B) {
   typedef typename Vec4<R>::T V4;
   const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= B.nB) return;
-  const int4 rc = B.rec[b];
+  const int4 rc = __ldg(B.rec + b);
   const int64_t cell = (int64_t)(((uint64_t)(uint32_t)rc.y << 32) | (uint32_t)rc.x);
   const int64_t q = cell + rc.z;
   const int m = rc.w;
+  const int64_t nB = B.nB;
   const V4 g4 = reinterpret_cast<const V4*>(B.geo)[b];
   const V4 n4 = reinterpret_cast<const V4*>(B.nrm)[b];
+  // the cell's own stage output (written by the stage kernel, blended here by this thread only)
+  R po0 = R(0), uo0 = R(0), vo0 = R(0), wo0 = R(0);
+  if (KM > 0) {
+    po0 = B.po[cell];
+    uo0 = B.uo[cell];
+    vo0 = B.vo[cell];
+    wo0 = B.wo[cell];
+  }
+  double rK[KM > 0 ? KM : 1], mK[KM > 0 ? KM : 1], r1L[LM > 0 ? LM : 1], r2L[LM > 0 ? LM : 1];
+  double m1L[LM > 0 ? LM : 1], m2L[LM > 0 ? LM : 1];
+#pragma unroll
+  for (int k = 0; k < KM; ++k)
+    if (k < B.K) {
+      rK[k] = __ldg(B.phR + (int64_t)k * nB + b);
+      if (STAGE > 0) mK[k] = __ldg(B.phM + (int64_t)k * nB + b);
+    }
+#pragma unroll
+  for (int l = 0; l < LM; ++l)
+    if (l < B.L) {
+      r1L[l] = __ldg(B.s1R + (int64_t)l * nB + b);
+      r2L[l] = __ldg(B.s2R + (int64_t)l * nB + b);
+      if (STAGE > 0) {
+        m1L[l] = __ldg(B.s1M + (int64_t)l * nB + b);
+        m2L[l] = __ldg(B.s2M + (int64_t)l * nB + b);
+      }
+    }
   const R sx = g4.x, sy = g4.y, sz = g4.z, chi = g4.w;
   const R nx = n4.x, ny = n4.y, nz = n4.z;
   const R pD = trilin<R>(B.pi, q, B.Sx, B.plane, sx, sy, sz);
@@ -428,46 +459,67 @@ __global__ void __launch_bounds__(256, 4) k_band(const BandArgs<R> B) {
   constexpr double a_ssp = (STAGE == 0) ? 0.0 : (STAGE == 1) ? 3.0 : 1.0;
   constexpr double b_ssp = (STAGE == 2) ? 2.0 : 1.0;
   constexpr double inv_c = (STAGE == 0) ? 1.0 : (STAGE == 1) ? 0.25 : 1.0 / 3.0;
-  const int64_t nB = B.nB;
   double sumA = 0.0, sumBC = 0.0;
-  for (int k = 0; k < B.K; ++k) {
+  // one real pole / complex pair of the ADE stage recursion
+  auto real_pole = [&](int k, double r, double mid) {
     const int mi = m * B.K + k;
-    const int64_t si = (int64_t)k * nB + b;
-    const double r = B.phR[si];
-    const double Lphi = wout - B.zeta[mi] * r;
+    const double Lphi = wout - __ldg(B.zeta + mi) * r;
     double v = b_ssp * (r + B.dt * Lphi);
-    if (STAGE > 0) v += a_ssp * B.phM[si];
+    if (STAGE > 0) v += a_ssp * mid;
     v *= inv_c;
-    B.phL[si] = v;
-    sumA += B.A[mi] * v;
-  }
-  for (int l = 0; l < B.L; ++l) {
+    B.phL[(int64_t)k * nB + b] = v;
+    sumA += __ldg(B.A + mi) * v;
+  };
+  auto pole_pair = [&](int l, double r1, double r2, double m1, double m2) {
     const int mi = m * B.L + l;
-    const int64_t si = (int64_t)l * nB + b;
-    const double r1 = B.s1R[si], r2 = B.s2R[si];
-    const double L1 = wout - (B.alpha[mi] * r1 + B.beta[mi] * r2);
-    const double L2 = B.beta[mi] * r1 - B.alpha[mi] * r2;
+    const double al = __ldg(B.alpha + mi), be = __ldg(B.beta + mi);
+    const double L1 = wout - (al * r1 + be * r2);
+    const double L2 = be * r1 - al * r2;
     double n1 = b_ssp * (r1 + B.dt * L1);
     double n2 = b_ssp * (r2 + B.dt * L2);
     if (STAGE > 0) {
-      n1 += a_ssp * B.s1M[si];
-      n2 += a_ssp * B.s2M[si];
+      n1 += a_ssp * m1;
+      n2 += a_ssp * m2;
     }
     n1 *= inv_c;
     n2 *= inv_c;
+    const int64_t si = (int64_t)l * nB + b;
     B.s1L[si] = n1;
     B.s2L[si] = n2;
-    sumBC += B.B[mi] * n1 + B.C[mi] * n2;
+    sumBC += __ldg(B.B + mi) * n1 + __ldg(B.C + mi) * n2;
+  };
+  if constexpr (KM > 0) {
+#pragma unroll
+    for (int k = 0; k < KM; ++k)
+      if (k < B.K) real_pole(k, rK[k], STAGE > 0 ? mK[k] : 0.0);
+#pragma unroll
+    for (int l = 0; l < LM; ++l)
+      if (l < B.L) pole_pair(l, r1L[l], r2L[l], STAGE > 0 ? m1L[l] : 0.0, STAGE > 0 ? m2L[l] : 0.0);
+  } else {
+    for (int k = 0; k < B.K; ++k) {
+      const int64_t si = (int64_t)k * nB + b;
+      real_pole(k, B.phR[si], STAGE > 0 ? B.phM[si] : 0.0);
+    }
+    for (int l = 0; l < B.L; ++l) {
+      const int64_t si = (int64_t)l * nB + b;
+      pole_pair(l, B.s1R[si], B.s2R[si], STAGE > 0 ? B.s1M[si] : 0.0, STAGE > 0 ? B.s2M[si] : 0.0);
+    }
   }
-  const double win = B.Rinf[m] * wout + sumA + sumBC;  // incoming characteristic
+  const double win = __ldg(B.Rinf + m) * wout + sumA + sumBC;  // incoming characteristic
   const R pb = (R)(0.5 * (win + wout));
   const R unb = (R)((wout - win) / (2.0 * B.Z0));
   const R ub = unb * nx + utx, vb = unb * ny + uty, wb = unb * nz + utz;
   const R omc = R(1) - chi;
-  B.uo[cell] = omc * B.uo[cell] + chi * ub;
-  B.vo[cell] = omc * B.vo[cell] + chi * vb;
-  B.wo[cell] = omc * B.wo[cell] + chi * wb;
-  B.po[cell] = omc * B.po[cell] + chi * pb;
+  if (KM == 0) {
+    po0 = B.po[cell];
+    uo0 = B.uo[cell];
+    vo0 = B.vo[cell];
+    wo0 = B.wo[cell];
+  }
+  B.uo[cell] = omc * uo0 + chi * ub;
+  B.vo[cell] = omc * vo0 + chi * vb;
+  B.wo[cell] = omc * wo0 + chi * wb;
+  B.po[cell] = omc * po0 + chi * pb;
 }
 
 // Receiver gather after the last stage of a step (main3D.cu:1399-1414), into a device buffer;
@@ -626,12 +678,23 @@ cudaError_t launch_band(int stage, const BandArgs<R>& a, cudaStream_t s) {
   if (a.nB <= 0) return cudaSuccess;
   const int bs = 256;
   const int64_t nb = (a.nB + bs - 1) / bs;
-  if (stage == 0)
-    k_band<R, 0><<<(unsigned)nb, bs, 0, s>>>(a);
-  else if (stage == 1)
-    k_band<R, 1><<<(unsigned)nb, bs, 0, s>>>(a);
-  else
-    k_band<R, 2><<<(unsigned)nb, bs, 0, s>>>(a);
+  // pole counts of up to 2 (4) real poles and complex pairs take the fixed-size form
+  const int fit = (a.K <= 2 && a.L <= 2) ? 2 : (a.K <= 4 && a.L <= 4) ? 4 : 0;
+#define FZ_BAND_LAUNCH(ST)                                                    \
+  if (fit == 2)                                                               \
+    k_band<R, ST, 2, 2><<<(unsigned)nb, bs, 0, s>>>(a);                       \
+  else if (fit == 4)                                                          \
+    k_band<R, ST, 4, 4><<<(unsigned)nb, bs, 0, s>>>(a);                       \
+  else                                                                        \
+    k_band<R, ST, 0, 0><<<(unsigned)nb, bs, 0, s>>>(a);
+  if (stage == 0) {
+    FZ_BAND_LAUNCH(0)
+  } else if (stage == 1) {
+    FZ_BAND_LAUNCH(1)
+  } else {
+    FZ_BAND_LAUNCH(2)
+  }
+#undef FZ_BAND_LAUNCH
   return cudaGetLastError();
 }
 
