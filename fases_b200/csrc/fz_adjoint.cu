@@ -15,98 +15,89 @@ namespace fz {
 
 namespace {
 
-template <class R>
-struct WenoTables {
-  // candidate rows (main3D.cu:834-837), beta second-term rows (839-841), linear weights (843)
-  static __device__ __forceinline__ R crl(int row, int l) {
-    const R t[4][3] = {{R(11.0 / 6.0), R(-7.0 / 6.0), R(1.0 / 3.0)},
-                       {R(1.0 / 3.0), R(5.0 / 6.0), R(-1.0 / 6.0)},
-                       {R(-1.0 / 6.0), R(5.0 / 6.0), R(1.0 / 3.0)},
-                       {R(1.0 / 3.0), R(-7.0 / 6.0), R(11.0 / 6.0)}};
-    return t[row][l];
-  }
-  static __device__ __forceinline__ R brl(int r, int l) {
-    const R t[3][3] = {{R(3), R(-4), R(1)}, {R(1), R(0), R(-1)}, {R(1), R(-4), R(3)}};
-    return t[r][l];
-  }
-  static __device__ __forceinline__ R dd(int i) {
-    const R t[3] = {R(0.3), R(0.6), R(0.1)};
-    return t[i];
-  }
-};
-
 // Reverse mode of one WENO-Z cell centre for a pair of variables (pressure and the velocity
 // component along the sweep): u[0..4] are the values at c-2 .. c+2; the centre gives V-(c+1/2)
-// (side 1) and V+(c-1/2) (side 0) from one set of smoothness indicators. g[0..4] += lam_m dV-/du +
-// lam_p dV+/du. Reciprocals as in the forward kernels (one MUFU op in FP32).
+// (lam_m, its adjoint) and V+(c-1/2) (lam_p) from one set of smoothness indicators, as the
+// stepping kernels' weno_core computes them (first differences a..d, second differences D_r,
+// E_r, 12/13-scaled indicators B_r, q_r = 1 + tau/B_r, normalisers Sm, Sp). g[0..4] += lam_m
+// dV-/du + lam_p dV+/du. The forward part is recomputed; reciprocals are differentiated as exact
+// 1/x. tau = |B0 - B2| takes the subgradient sign(0) = 0.
 template <class R>
 __device__ __forceinline__ void weno_centre_rev(const typename Pair<R>::T u[5], typename Pair<R>::T lam_m,
                                                 typename Pair<R>::T lam_p, typename Pair<R>::T g[5]) {
   typedef typename Pair<R>::T P;
-  typedef WenoTables<R> T;
-  const P eps = psplat<R>(R(1e-10));
-  P b1[3], b2[3], tib[3], ib[3];
-  P lbeta[3];
-#pragma unroll
-  for (int r = 0; r < 3; r++) {
-    b1[r] = pfma(u[3 - r], psplat<R>(R(-2)), padd(u[2 - r], u[4 - r]));
-    b2[r] = pfma(psplat<R>(T::brl(r, 0)), u[2 - r],
-                 pfma(psplat<R>(T::brl(r, 1)), u[3 - r], pmul(psplat<R>(T::brl(r, 2)), u[4 - r])));
-  }
-  P beta[3];
-#pragma unroll
-  for (int r = 0; r < 3; r++) {
-    beta[r] = pfma(pmul(b1[r], psplat<R>(R(13.0 / 12.0))), b1[r], pmul(pmul(b2[r], psplat<R>(R(0.25))), b2[r]));
-    ib[r] = prcp(padd(beta[r], eps));
-    lbeta[r] = psplat<R>(R(0));
-  }
-  const P diff = psub(beta[0], beta[2]);
+  auto K = [](double x) { return psplat<R>(R(x)); };
+  // ---- forward (weno_core)
+  const P a = psub(u[1], u[0]), b = psub(u[2], u[1]), c = psub(u[3], u[2]), d = psub(u[4], u[3]);
+  const P D2 = psub(b, a), D1 = psub(c, b), D0 = psub(d, c);
+  const P E2 = pfma(b, K(2.0), D2), E1 = padd(b, c), E0 = pfma(c, K(-2.0), D0);
+  const P k313 = K(3.0 / 13.0), eps = K(1e-10 * 12.0 / 13.0);
+  const P B0 = pfma(D0, D0, pfma(pmul(E0, k313), E0, eps));
+  const P B1 = pfma(D1, D1, pfma(pmul(E1, k313), E1, eps));
+  const P B2 = pfma(D2, D2, pfma(pmul(E2, k313), E2, eps));
+  const P diff = psub(B0, B2);
   const P tau = pabs(diff);
-#pragma unroll
-  for (int r = 0; r < 3; r++) tib[r] = pmul(tau, ib[r]);
-  P ltau = psplat<R>(R(0));
-#pragma unroll
-  for (int side = 0; side < 2; side++) {
-    const P lam = side ? lam_m : lam_p;
-    P cand[3], alpha[3];
-    P S = psplat<R>(R(0)), num = psplat<R>(R(0));
-#pragma unroll
-    for (int r = 0; r < 3; r++) {
-      cand[r] = pfma(psplat<R>(T::crl(r + side, 0)), u[2 - r],
-                     pfma(psplat<R>(T::crl(r + side, 1)), u[3 - r], pmul(psplat<R>(T::crl(r + side, 2)), u[4 - r])));
-      const P d = psplat<R>(T::dd(side ? r : 2 - r));
-      alpha[r] = pfma(d, tib[r], d);
-      S = padd(S, alpha[r]);
-      num = pfma(alpha[r], cand[r], num);
-    }
-    const P iS = prcp(S);
-    const P V = pmul(num, iS);
-    const P sl = pmul(iS, lam);
-#pragma unroll
-    for (int r = 0; r < 3; r++) {
-      const P lc = pmul(alpha[r], sl);
-      g[2 - r] = pfma(psplat<R>(T::crl(r + side, 0)), lc, g[2 - r]);
-      g[3 - r] = pfma(psplat<R>(T::crl(r + side, 1)), lc, g[3 - r]);
-      g[4 - r] = pfma(psplat<R>(T::crl(r + side, 2)), lc, g[4 - r]);
-      // t = d ib (cand - V) lam / S: d alpha / d tau and d alpha / d beta share it
-      const P t = pmul(pmul(psplat<R>(T::dd(side ? r : 2 - r)), ib[r]), pmul(psub(cand[r], V), sl));
-      ltau = padd(ltau, t);
-      lbeta[r] = psub(lbeta[r], pmul(t, tib[r]));
-    }
-  }
-  // tau = |beta0 - beta2|: subgradient sign(0) = 0
+  const P rB0 = prcp(B0), rB1 = prcp(B1), rB2 = prcp(B2);
+  const P one = K(1.0);
+  const P q0 = pfma(tau, rB0, one), q1 = pfma(tau, rB1, one), q2 = pfma(tau, rB2, one);
+  const P t1 = pmul(q1, K(0.6));
+  const P Sm = pfma(q0, K(0.3), pfma(q2, K(0.1), t1));
+  const P Sp = pfma(q0, K(0.1), pfma(q2, K(0.3), t1));
+  const P h1 = pmul(D1, K(0.05));
+  const P em0 = pfma(c, K(0.15), pmul(D0, K(-0.05)));
+  const P ep0 = pfma(c, K(-0.05), pmul(D0, K(1.0 / 30.0)));
+  const P em1 = pfma(E1, K(0.15), h1);
+  const P ep1 = pfma(E1, K(-0.15), h1);
+  const P em2 = pfma(b, K(0.05), pmul(D2, K(1.0 / 30.0)));
+  const P ep2 = pfma(b, K(-0.15), pmul(D2, K(-0.05)));
+  const P Nm = pfma(q2, em2, pfma(q1, em1, pmul(q0, em0)));
+  const P Np = pfma(q2, ep2, pfma(q1, ep1, pmul(q0, ep0)));
+  const P rSm = prcp(Sm), rSp = prcp(Sp);
+  // ---- reverse: vm = q0c + Nm / Sm, vp = q0c + Np / Sp
+  const P tm = pmul(lam_m, rSm), tp = pmul(lam_p, rSp);  // adjoints of Nm, Np
+  const P lSm = pmul(tm, pmul(Nm, rSm)), lSp = pmul(tp, pmul(Np, rSp));  // minus the adjoints of Sm, Sp
+  // adjoints of q_r (with the Sm, Sp signs folded in)
+  const P lq0 = pfma(tp, ep0, pfma(tm, em0, pfma(lSm, K(-0.3), pmul(lSp, K(-0.1)))));
+  const P lq1 = pfma(tp, ep1, pfma(tm, em1, pmul(padd(lSm, lSp), K(-0.6))));
+  const P lq2 = pfma(tp, ep2, pfma(tm, em2, pfma(lSm, K(-0.1), pmul(lSp, K(-0.3)))));
+  // adjoints of the first and second differences through em_r, ep_r (d/d em_r = tm q_r, d/d ep_r = tp q_r)
+  P lc = pmul(q0, pfma(tm, K(0.15), pmul(tp, K(-0.05))));
+  P lD0 = pmul(q0, pfma(tm, K(-0.05), pmul(tp, K(1.0 / 30.0))));
+  P lE1 = pmul(pmul(q1, K(0.15)), psub(tm, tp));
+  P lD1 = pmul(pmul(q1, K(0.05)), padd(tm, tp));
+  P lb = pmul(q2, pfma(tm, K(0.05), pmul(tp, K(-0.15))));
+  P lD2 = pmul(q2, pfma(tm, K(1.0 / 30.0), pmul(tp, K(-0.05))));
+  // q_r = 1 + tau rB_r: d/dtau = rB_r, d/dB_r = -tau rB_r^2 = -(q_r - 1) rB_r
+  const P ltau = pfma(lq2, rB2, pfma(lq1, rB1, pmul(lq0, rB0)));
   const P sl = pmk(diff.x > R(0) ? ltau.x : (diff.x < R(0) ? -ltau.x : R(0)),
                    diff.y > R(0) ? ltau.y : (diff.y < R(0) ? -ltau.y : R(0)));
-  lbeta[0] = padd(lbeta[0], sl);
-  lbeta[2] = psub(lbeta[2], sl);
-#pragma unroll
-  for (int r = 0; r < 3; r++) {
-    const P l1 = pmul(pmul(b1[r], psplat<R>(R(13.0 / 6.0))), lbeta[r]);
-    const P l2 = pmul(pmul(b2[r], psplat<R>(R(0.5))), lbeta[r]);
-    g[2 - r] = padd(g[2 - r], pfma(psplat<R>(T::brl(r, 0)), l2, l1));
-    g[3 - r] = padd(g[3 - r], pfma(psplat<R>(T::brl(r, 1)), l2, pmul(psplat<R>(R(-2)), l1)));
-    g[4 - r] = padd(g[4 - r], pfma(psplat<R>(T::brl(r, 2)), l2, l1));
-  }
+  // twice the adjoints of B_r (B_r = D_r^2 + 3/13 E_r^2 + eps)
+  const P m2 = K(-2.0);
+  const P lB0 = pfma(pmul(lq0, psub(q0, one)), pmul(rB0, m2), padd(sl, sl));
+  const P lB1 = pmul(pmul(lq1, psub(q1, one)), pmul(rB1, m2));
+  const P lB2 = psub(pmul(pmul(lq2, psub(q2, one)), pmul(rB2, m2)), padd(sl, sl));
+  lD0 = pfma(D0, lB0, lD0);
+  lD1 = pfma(D1, lB1, lD1);
+  lD2 = pfma(D2, lB2, lD2);
+  const P lE0 = pmul(pmul(E0, k313), lB0);
+  lE1 = pfma(pmul(E1, k313), lB1, lE1);
+  const P lE2 = pmul(pmul(E2, k313), lB2);
+  // E2 = 2b + D2, E1 = b + c, E0 = -2c + D0
+  lb = pfma(lE2, K(2.0), padd(lb, lE1));
+  lD2 = padd(lD2, lE2);
+  lc = pfma(lE0, K(-2.0), padd(lc, lE1));
+  lD0 = padd(lD0, lE0);
+  // D2 = b - a, D1 = c - b, D0 = d - c
+  lb = psub(padd(lb, lD2), lD1);
+  lc = psub(padd(lc, lD1), lD0);
+  const P la = pmul(lD2, K(-1.0));
+  const P ld = lD0;
+  // a = u1 - u0, b = u2 - u1, c = u3 - u2, d = u4 - u3; u2 is also the value both faces start from
+  g[0] = psub(g[0], la);
+  g[1] = padd(g[1], psub(la, lb));
+  g[2] = padd(g[2], padd(psub(lb, lc), padd(lam_m, lam_p)));
+  g[3] = padd(g[3], psub(lc, ld));
+  g[4] = padd(g[4], ld);
 }
 
 // Adjoint of the Godunov flux of a face: the adjoints of its left state (from the face's
