@@ -150,6 +150,25 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
   double* d_gpml = (double*)ar.take((size_t)3 * 6 * d * 8);
   if (!d_gpml) return fzi::set_error(h, FZ_ENOMEM, "fz_misfit_gradient: arena layout overflow");
 
+  // the handle's own field arrays by set, put back after every recompute
+  void* own[3][4];
+  for (int q = 0; q < 3; q++)
+    for (int f = 0; f < 4; f++) own[q][f] = h->U[q][f];
+  auto unbind = [&]() -> int {
+    for (int q = 0; q < 3; q++) {
+      const int rc = fzi::bind_field_set(h, q, own[q]);
+      if (rc != FZ_OK) return rc;
+    }
+    return FZ_OK;
+  };
+#define FZ_ARC(call)                \
+  do {                              \
+    const int rc__ = (call);        \
+    if (rc__ != FZ_OK) {            \
+      unbind();                     \
+      return rc__;                  \
+    }                               \
+  } while (0)
   auto save = [&](const State& st) -> cudaError_t {
     cudaError_t e = cudaSuccess;
     for (int f = 0; f < 4 && e == cudaSuccess; f++)
@@ -301,34 +320,48 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
   };
 
   FZ_ACUDA(h, cudaEventRecord(ev[2], s), "event record");
+  // cells no kernel writes read zero in every stored stage input, as in the handle's own sets
+  for (int q = 0; q < 3; q++)
+    for (void* p : S[q]) FZ_ACUDA(h, cudaMemsetAsync(p, 0, fb, s), "memset");
   for (int64_t q = nseg - 1; q >= 0; q--) {
     const int len = (int)std::min<int64_t>(seg, nsteps - q * seg);
     FZ_ACUDA(h, restore(ck[(size_t)q], q * seg), "restore");
-    // recompute the segment, storing stage inputs and ADE sets
-    for (int t = 0; t < len; t++) {
+    // recompute the segment with the stage kernels writing straight into the segment storage
+    // (field sets bound to the stored arrays): the step input is S[0][t], stage 0 writes S[1][t],
+    // stage 1 S[2][t], stage 2 the next step's S[0][t+1]; ADE sets are copied
+    {
       cudaError_t e = cudaSuccess;
       for (int f = 0; f < 4 && e == cudaSuccess; f++)
-        e = cudaMemcpyAsync(S[0][(size_t)t * 4 + f], h->U[h->i0][f], fb, cudaMemcpyDeviceToDevice, s);
+        e = cudaMemcpyAsync(S[0][f], h->U[h->i0][f], fb, cudaMemcpyDeviceToDevice, s);
+      if (e != cudaSuccess) return fzi::cuda_fail(h, e, "adjoint recompute");
+    }
+    FZ_ARC(fzi::bind_field_set(h, h->i0, &S[0][0]));
+    for (int t = 0; t < len; t++) {
+      cudaError_t e = cudaSuccess;
       for (int a = 0; a < 3 && e == cudaSuccess; a++)
         if (ade_b[a]) e = cudaMemcpyAsync(Ad[0][a][(size_t)t], h->d_ade[h->ph_old][a], ade_b[a], cudaMemcpyDeviceToDevice, s);
       for (int a = 0; a < 3 && e == cudaSuccess && want_pml; a++)
         if (psi_b[a]) e = cudaMemcpyAsync(Ps[a][(size_t)t], h->d_psi[a], psi_b[a], cudaMemcpyDeviceToDevice, s);
+      FZ_ARC(fzi::bind_field_set(h, h->i1, &S[1][(size_t)t * 4]));
       if (e == cudaSuccess) e = fzi::enqueue_stage(h, 0);
-      for (int f = 0; f < 4 && e == cudaSuccess; f++)
-        e = cudaMemcpyAsync(S[1][(size_t)t * 4 + f], h->U[h->i1][f], fb, cudaMemcpyDeviceToDevice, s);
       for (int a = 0; a < 3 && e == cudaSuccess; a++)
         if (ade_b[a]) e = cudaMemcpyAsync(Ad[1][a][(size_t)t], h->d_ade[h->ph_cur][a], ade_b[a], cudaMemcpyDeviceToDevice, s);
+      FZ_ARC(fzi::bind_field_set(h, h->i2, &S[2][(size_t)t * 4]));
       if (e == cudaSuccess) e = fzi::enqueue_stage(h, 1);
-      for (int f = 0; f < 4 && e == cudaSuccess; f++)
-        e = cudaMemcpyAsync(S[2][(size_t)t * 4 + f], h->U[h->i2][f], fb, cudaMemcpyDeviceToDevice, s);
       for (int a = 0; a < 3 && e == cudaSuccess; a++)
         if (ade_b[a]) e = cudaMemcpyAsync(Ad[2][a][(size_t)t], h->d_ade[h->ph_nu][a], ade_b[a], cudaMemcpyDeviceToDevice, s);
+      // the last step's output is the next segment's checkpoint, not stored: a free own set takes it
+      FZ_ARC(fzi::bind_field_set(h, h->i1, (t + 1 < len) ? &S[0][(size_t)(t + 1) * 4] : own[0]));
       if (e == cudaSuccess) e = fzi::enqueue_stage(h, 2);
       for (int a = 0; a < 3 && e == cudaSuccess; a++)
         if (ade_b[a]) e = cudaMemcpyAsync(Ad[3][a][(size_t)t], h->d_ade[h->ph_cur][a], ade_b[a], cudaMemcpyDeviceToDevice, s);
       if (e == cudaSuccess) e = fzi::enqueue_finish(h);
-      if (e != cudaSuccess) return fzi::cuda_fail(h, e, "adjoint recompute");
+      if (e != cudaSuccess) {
+        unbind();
+        return fzi::cuda_fail(h, e, "adjoint recompute");
+      }
     }
+    FZ_ARC(unbind());
     // reverse sweep
     for (int t = len - 1; t >= 0; t--) {
       const int64_t n = q * seg + t;
@@ -412,6 +445,7 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
       ps = 1 - ps;
     }
   }
+#undef FZ_ARC
   FZ_ACUDA(h, fz::launch_adj_grad_reduce(h->d_brec, d_gcell, nB, Pn, nMat, d_grad, s), "gradient reduce");
   FZ_ACUDA(h, cudaEventRecord(ev[3], s), "event record");
   FZ_ACUDA(h, cudaStreamSynchronize(s), "adjoint sync");

@@ -607,17 +607,21 @@ __global__ void __launch_bounds__(256) k_adj_probe_scatter(const AdjBandArgs<R> 
   }
 }
 
-// grad[m][e] = sum of gcell[e][b] over the band cells b of material m; one block per coefficient
-// slot e, per-material bins in shared memory.
+// grad[m][e] += sum of gcell[e][b] over the band cells b of material m (grad zeroed before): blocks
+// (coefficient slot e, chunk of band cells), per-material bins in shared memory, one global atomic
+// per bin and block.
+constexpr int GRAD_CHUNK = 256 * 32;
 __global__ void __launch_bounds__(256) k_adj_grad_reduce(const int4* rec, const double* gcell, int64_t nB, int P,
                                                          int nMat, double* grad) {
   extern __shared__ double bins[];
   const int e = blockIdx.x;
   for (int m = threadIdx.x; m < nMat; m += blockDim.x) bins[m] = 0.0;
   __syncthreads();
-  for (int64_t b = threadIdx.x; b < nB; b += blockDim.x) atomicAdd(&bins[rec[b].w], gcell[(int64_t)e * nB + b]);
+  const int64_t b0 = (int64_t)blockIdx.y * GRAD_CHUNK, b1 = min(nB, b0 + (int64_t)GRAD_CHUNK);
+  for (int64_t b = b0 + threadIdx.x; b < b1; b += blockDim.x) atomicAdd(&bins[rec[b].w], gcell[(int64_t)e * nB + b]);
   __syncthreads();
-  for (int m = threadIdx.x; m < nMat; m += blockDim.x) grad[(int64_t)m * P + e] = bins[m];
+  for (int m = threadIdx.x; m < nMat; m += blockDim.x)
+    if (bins[m] != 0.0) atomicAdd(&grad[(int64_t)m * P + e], bins[m]);
 }
 
 template <class R>
@@ -749,8 +753,10 @@ cudaError_t launch_adj_band(int stage, const AdjBandArgs<R>& a, cudaStream_t s) 
 
 cudaError_t launch_adj_grad_reduce(const int4* rec, const double* gcell, int64_t nB, int P, int nMat, double* grad,
                                    cudaStream_t s) {
-  if (nB <= 0) return cudaMemsetAsync(grad, 0, (size_t)nMat * P * sizeof(double), s);
-  k_adj_grad_reduce<<<(unsigned)P, 256, (size_t)nMat * sizeof(double), s>>>(rec, gcell, nB, P, nMat, grad);
+  cudaError_t e = cudaMemsetAsync(grad, 0, (size_t)nMat * P * sizeof(double), s);
+  if (e != cudaSuccess || nB <= 0) return e;
+  const dim3 grid((unsigned)P, (unsigned)((nB + GRAD_CHUNK - 1) / GRAD_CHUNK));
+  k_adj_grad_reduce<<<grid, 256, (size_t)nMat * sizeof(double), s>>>(rec, gcell, nB, P, nMat, grad);
   return cudaGetLastError();
 }
 

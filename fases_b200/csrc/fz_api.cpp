@@ -785,6 +785,19 @@ cudaError_t enqueue(fz_handle* h) { return h->fp64 ? enqueue_step<double>(h) : e
 cudaError_t enqueue_stage(fz_handle* h, int st) {
   return h->fp64 ? ::enqueue_stage<double>(h, st) : ::enqueue_stage<float>(h, st);
 }
+int bind_field_set(fz_handle* h, int set, void* const* f) {
+  const CUtensorMapDataType t = h->fp64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  for (int q = 0; q < 4; q++) h->U[set][q] = f[q];
+  for (int q = 0; q < 3; q++) {
+    const int rc = make_map(h, &h->halo_map[set][q], h->U[set][q], h->rsize, t, fz::PW, fz::PH);
+    if (rc != FZ_OK) return rc;
+  }
+  for (int q = 0; q < 4; q++) {
+    const int rc = make_map(h, &h->own_map[set][q], h->U[set][q], h->rsize, t, fz::TX, fz::TY);
+    if (rc != FZ_OK) return rc;
+  }
+  return FZ_OK;
+}
 cudaError_t enqueue_stage_kernel(fz_handle* h, int st) {
   return h->fp64 ? ::enqueue_stage_kernel<double>(h, st) : ::enqueue_stage_kernel<float>(h, st);
 }

@@ -140,6 +140,9 @@ cudaError_t enqueue(fz_handle* h);
 // the parts of one step: stage st (stage kernel + band), then receivers and buffer rotation
 cudaError_t enqueue_stage(fz_handle* h, int st);
 cudaError_t enqueue_finish(fz_handle* h);
+// points field set `set` at the four arrays f (same size and layout as the handle's own) and
+// re-encodes its TMA maps; kernels already launched keep the maps they were launched with
+int bind_field_set(fz_handle* h, int set, void* const* f);
 // the stage kernel of stage st alone (no band), on the handle's stream: the autotuner's trial
 cudaError_t enqueue_stage_kernel(fz_handle* h, int st);
 // tile depth of the stage kernels (z planes per CTA; 0 = the wave-filling heuristic); drops the
