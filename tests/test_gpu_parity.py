@@ -84,3 +84,39 @@ def test_energy_matches_oracle():
     s = run_gpu(cfg, "fp64")
     o = run_oracle(cfg)
     assert abs(s.energy() - o.energy()) <= 1e-10 * abs(o.energy())
+
+
+@pytest.mark.parametrize("K,L", [(3, 4), (5, 6), (0, 3)])
+def test_pole_counts_beyond_two(K, L):
+    # the band kernel keeps up to 2 (and up to 4) real poles and complex pairs in fixed-size
+    # register arrays and takes a general loop above that: each form against the oracle, FP64 and FP32
+    cfg = small_room(seed=40 + K, K=K, L=L, steps=60)
+    o = run_oracle(cfg)
+    ir_o, _ = o.ir()
+    s64 = run_gpu(cfg, "fp64")
+    assert rel_l2(s64.ir(), ir_o) < TOL_FP64
+    for a, b in zip(s64.fields(), o.fields()):
+        assert rel_l2(a, b) < TOL_FP64
+    s32 = run_gpu(cfg, "fp32")
+    ir_g = s32.ir()
+    errs = [rel_l2(ir_g[r], ir_o[r]) for r in range(ir_o.shape[0])]
+    assert max(errs) < TOL_FP32_IR, errs
+
+
+def test_free_field_without_band_cells():
+    # all air (no wall, no material: the band list is empty), cPML on every face, a pulse and a
+    # PCS source; FP64 against the oracle and the receivers' traces
+    from types import SimpleNamespace
+    cfg = small_room(seed=9, room=(30, 28, 26), pml=(1, 1, 1, 1, 1, 1), pml_cells=5, obstacle=False, steps=50)
+    shape = cfg["scene"].S.shape
+    S = np.full(shape, 1.0, np.float32)
+    oid = np.full(shape, 0xFF, np.uint8)
+    cfg["scene"] = SimpleNamespace(S=S, oid=oid, shape=shape)
+    cfg["materials"] = {k: np.asarray(v)[:1] for k, v in cfg["materials"].items()}
+    s = run_gpu(cfg, "fp64")
+    assert s.info()["n_band"] == 0
+    o = run_oracle(cfg)
+    ir_o, _ = o.ir()
+    assert rel_l2(s.ir(), ir_o) < TOL_FP64
+    for a, b in zip(s.fields(), o.fields()):
+        assert rel_l2(a, b) < TOL_FP64
