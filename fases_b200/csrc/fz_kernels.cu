@@ -551,8 +551,23 @@ template <class R>
 __global__ void k_count_nonfinite(const R* __restrict__ p, const R* __restrict__ u, const R* __restrict__ v,
                                   const R* __restrict__ w, int64_t n, unsigned long long* count) {
   unsigned long long k = 0;
-  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x)
-    k += (!isfinite(p[c])) + (!isfinite(u[c])) + (!isfinite(v[c])) + (!isfinite(w[c]));
+  // four cells per thread and pass, their sixteen loads issued together
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t c0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c0 < n; c0 += 4 * stride) {
+    R x[4][4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int64_t c = c0 + q * stride;
+      const bool in = c < n;
+      x[q][0] = in ? p[c] : R(0);
+      x[q][1] = in ? u[c] : R(0);
+      x[q][2] = in ? v[c] : R(0);
+      x[q][3] = in ? w[c] : R(0);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      k += (!isfinite(x[q][0])) + (!isfinite(x[q][1])) + (!isfinite(x[q][2])) + (!isfinite(x[q][3]));
+  }
   for (int o = 16; o > 0; o >>= 1) k += __shfl_down_sync(0xffffffffu, k, o);
   if ((threadIdx.x & 31) == 0 && k) atomicAdd(count, k);
 }
@@ -607,10 +622,24 @@ template <class R>
 __global__ void k_energy(const R* __restrict__ p, const R* __restrict__ u, const R* __restrict__ v,
                          const R* __restrict__ w, int64_t n, double inv_rc2, double rho, double* out) {
   double s = 0.0;
-  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
-       c += (int64_t)gridDim.x * blockDim.x) {
-    const double pp = p[c], uu = u[c], vv = v[c], ww = w[c];
-    s += pp * pp * inv_rc2 + rho * (uu * uu + vv * vv + ww * ww);
+  // four cells per thread and pass, their sixteen loads issued together
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t c0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c0 < n; c0 += 4 * stride) {
+    R x[4][4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int64_t c = c0 + q * stride;
+      const bool in = c < n;
+      x[q][0] = in ? p[c] : R(0);
+      x[q][1] = in ? u[c] : R(0);
+      x[q][2] = in ? v[c] : R(0);
+      x[q][3] = in ? w[c] : R(0);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const double pp = x[q][0], uu = x[q][1], vv = x[q][2], ww = x[q][3];
+      s += pp * pp * inv_rc2 + rho * (uu * uu + vv * vv + ww * ww);
+    }
   }
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
   __shared__ double red[32];
@@ -708,7 +737,7 @@ cudaError_t launch_receivers(const R* p, const R* u, const R* v, const R* w, con
 template <class R>
 cudaError_t launch_count_nonfinite(const R* p, const R* u, const R* v, const R* w, int64_t n,
                                    unsigned long long* count, int nsm, cudaStream_t s) {
-  k_count_nonfinite<R><<<nsm * 4, 256, 0, s>>>(p, u, v, w, n, count);
+  k_count_nonfinite<R><<<nsm * 8, 256, 0, s>>>(p, u, v, w, n, count);
   return cudaGetLastError();
 }
 
@@ -723,7 +752,7 @@ cudaError_t launch_slices(const R* p, const R* u, const R* v, const R* w, int Nx
 template <class R>
 cudaError_t launch_energy(const R* p, const R* u, const R* v, const R* w, int64_t n, double inv_rc2,
                           double rho, double* out, int nsm, cudaStream_t s) {
-  k_energy<R><<<nsm * 4, 256, 0, s>>>(p, u, v, w, n, inv_rc2, rho, out);
+  k_energy<R><<<nsm * 8, 256, 0, s>>>(p, u, v, w, n, inv_rc2, rho, out);
   return cudaGetLastError();
 }
 
