@@ -208,6 +208,7 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
   } evg{ev};
 
   // ---- forward with checkpoints
+  nvtxRangePushA("adjoint: forward with checkpoints");
   FZ_ACUDA(h, cudaEventRecord(ev[0], s), "event record");
   for (int64_t q = 0; q < nseg; q++) {
     FZ_ACUDA(h, save(ck[(size_t)q]), "checkpoint");
@@ -216,6 +217,7 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
   }
   FZ_ACUDA(h, save(ck[(size_t)nseg]), "checkpoint");
   FZ_ACUDA(h, cudaEventRecord(ev[1], s), "event record");
+  nvtxRangePop();
   int rc = fz_sync(h, 0);
   if (rc != FZ_OK) return rc;
 
@@ -363,6 +365,7 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
     }
     FZ_ARC(unbind());
     // reverse sweep
+    fz_range sweep_range("adjoint: reverse sweep of a segment");
     for (int t = len - 1; t >= 0; t--) {
       const int64_t n = q * seg + t;
       for (int qq : {jO, j1, j2})
@@ -539,6 +542,7 @@ int fz_misfit_gradient(fz_handle* h, int64_t nsteps, int32_t segment_steps, cons
 
 int fz_misfit_gradient_ex(fz_handle* h, int64_t nsteps, int32_t segment_steps, const double* target,
                           int64_t target_steps, double* J, fz_gradients* out, double* ms) {
+  fz_range nvtx_range("fz_misfit_gradient");
   if (!h) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
   if (nsteps < 1 || segment_steps < 1 || !target || !out || target_steps < nsteps)
     return fzi::set_error(h, FZ_EINVAL, "fz_misfit_gradient: nsteps >= 1, segment_steps >= 1, target of "

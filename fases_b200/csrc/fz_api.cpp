@@ -1146,6 +1146,7 @@ int fz_state_bytes(fz_handle* h, int64_t* bytes) {
 }
 
 int fz_state_save(fz_handle* h, void* buf, int64_t cap) {
+  fz_range nvtx_range("fz_state_save");
   int64_t need = 0;
   int rc = fz_state_bytes(h, &need);
   if (rc != FZ_OK) return rc;
@@ -1166,6 +1167,7 @@ int fz_state_save(fz_handle* h, void* buf, int64_t cap) {
 }
 
 int fz_state_load(fz_handle* h, const void* buf, int64_t len) {
+  fz_range nvtx_range("fz_state_load");
   int64_t need = 0;
   int rc = fz_state_bytes(h, &need);
   if (rc != FZ_OK) return rc;
@@ -1214,6 +1216,7 @@ int fz_check_health(fz_handle* h, int64_t* nonfinite) {
 }
 
 int fz_run(fz_handle* h, int64_t nsteps) {
+  fz_range nvtx_range("fz_run");
   if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
   if (nsteps < 0) return set_error(h, FZ_EINVAL, "fz_run: negative step count");
   cudaSetDevice(h->device);
@@ -1221,6 +1224,7 @@ int fz_run(fz_handle* h, int64_t nsteps) {
 }
 
 int fz_run_progress(fz_handle* h, int64_t nsteps, int32_t every_percent, fz_progress_fn cb, void* user) {
+  fz_range nvtx_range("fz_run_progress");
   if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
   if (nsteps < 0 || every_percent < 1 || every_percent > 100)
     return set_error(h, FZ_EINVAL, "fz_run_progress: nsteps >= 0 and every_percent in [1, 100]");

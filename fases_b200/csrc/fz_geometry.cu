@@ -547,6 +547,7 @@ int fz_scene_dims(const char* obj_path, double h, int32_t* dims, double* L) {
 
 int fz_build_scene(const char* obj_path, double h, double tol_cells, int32_t device, float* S, uint8_t* oid,
                    int64_t cap) {
+  fz_range nvtx_range("fz_build_scene");
   if (!obj_path || !(h > 0) || !(tol_cells > 0) || !S || !oid)
     return fzi::set_global_error(FZ_EINVAL, "fz_build_scene: bad arguments");
   int d[3];

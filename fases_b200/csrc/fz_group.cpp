@@ -124,6 +124,7 @@ int fz_group_create(fz_handle* const* members, int32_t n, fz_group** out) {
 }
 
 int fz_group_run(fz_group* g, int64_t nsteps) {
+  fz_range nvtx_range("fz_group_run");
   if (!g || nsteps < 0) return fzi::set_global_error(FZ_EINVAL, "fz_group_run: bad arguments");
   cudaSetDevice(g->device);
   for (fz_handle* h : g->m)

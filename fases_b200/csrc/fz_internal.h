@@ -5,8 +5,18 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/fz.h"
 #include "fz_device.cuh"
+
+// NVTX range over a scope (host timeline markers for nsys / ncu; no cost without a tool attached)
+struct fz_range {
+  explicit fz_range(const char* name) { nvtxRangePushA(name); }
+  ~fz_range() { nvtxRangePop(); }
+  fz_range(const fz_range&) = delete;
+  fz_range& operator=(const fz_range&) = delete;
+};
 
 struct fz_timing_rec {
   int kind;

@@ -290,6 +290,7 @@ int fz_write_outputs(fz_handle* h, const char* output_dir, int32_t src_idx, cons
 
 int fz_load_project(const char* scene_path, const char* config_path, const char* src_path, const char* rec_path,
                     int32_t precision, int32_t device, fz_handle** out, int64_t* n_steps_out) {
+  fz_range nvtx_range("fz_load_project");
   if (!scene_path || !config_path || !src_path || !rec_path || !out)
     return set_global_error(FZ_EINVAL, "fz_load_project: NULL argument");
   *out = nullptr;

@@ -191,6 +191,7 @@ int tune(const std::vector<fz_handle*>& hs, cudaStream_t ts, const std::vector<i
 extern "C" {
 
 int fz_autotune(fz_handle* h, int32_t reps, int32_t* kz_chunk, double* ms_per_step) {
+  fz_range nvtx_range("fz_autotune");
   if (!h) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
   if (!h->have_geometry) return fzi::set_error(h, FZ_ESTATE, "fz_autotune before fz_load_geometry_raw");
   int rc = fzi::prepare(h);
