@@ -8,7 +8,9 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libfz.so")
+# FZ_BOUNDS_CHECK=1 loads the bounds-checked build (every computed index of the stepping kernels
+# checked against its array; an out-of-range one sets an error bit and is skipped)
+LIB_PATH = os.path.join(HERE, "libfz_checked.so" if os.environ.get("FZ_BOUNDS_CHECK") == "1" else "libfz.so")
 
 FZ_OK = 0
 FZ_EINVAL = -1
@@ -20,6 +22,7 @@ FZ_ESTATE = -6
 FZ_ETIMEOUT = -7
 FZ_ENONFINITE = -8
 FZ_ENODEV = -9
+FZ_EBOUNDS = -10
 FZ_FP32 = 0
 FZ_FP64 = 1
 FZ_SRC_PCS = 0
@@ -31,7 +34,7 @@ FZ_NOALLOC_MAX_CELLS = 4096 * 16384
 ERROR_NAMES = {
     FZ_EINVAL: "FZ_EINVAL", FZ_ENOMEM: "FZ_ENOMEM", FZ_ECUDA: "FZ_ECUDA", FZ_EIO: "FZ_EIO",
     FZ_EPARSE: "FZ_EPARSE", FZ_ESTATE: "FZ_ESTATE", FZ_ETIMEOUT: "FZ_ETIMEOUT",
-    FZ_ENONFINITE: "FZ_ENONFINITE", FZ_ENODEV: "FZ_ENODEV",
+    FZ_ENONFINITE: "FZ_ENONFINITE", FZ_ENODEV: "FZ_ENODEV", FZ_EBOUNDS: "FZ_EBOUNDS",
 }
 
 

@@ -504,6 +504,16 @@ fz::StageArgs<R> stage_args(fz_handle* h, int stage) {
   a.half_dt = (R)(0.5 * p.dt);
   a.step = h->d_step;
   a.err = h->d_err;
+  a.nfield = h->ncell_dev * h->nb;
+  {
+    const int64_t d2 = 2 * (int64_t)p.pml_cells;
+    a.npsi[0] = h->d_psi[0] ? d2 * h->Ny * h->Nz * h->nb : 0;
+    a.npsi[1] = h->d_psi[1] ? (int64_t)h->Nx * d2 * h->Nz * h->nb : 0;
+    a.npsi[2] = h->d_psi[2] ? (int64_t)h->Nx * h->Ny * d2 * h->nb : 0;
+    a.npc[0] = h->Nx;
+    a.npc[1] = h->Ny;
+    a.npc[2] = (int64_t)h->Nz * h->nb;
+  }
   return a;
 }
 
@@ -522,6 +532,8 @@ fz::BandArgs<R> band_args(fz_handle* h, int stage) {
   b.pi = in[0]; b.ui = in[1]; b.vi = in[2]; b.wi = in[3];
   b.po = out[0]; b.uo = out[1]; b.vo = out[2]; b.wo = out[3];
   b.Sx = h->Sx; b.plane = h->plane;
+  b.err = h->d_err;
+  b.nfield = h->ncell_dev * h->nb;
   b.Z0 = h->prm.rho * h->prm.c;
   b.dt = h->prm.dt;
   // ADE state roles (left, middle, right) of the stage, main3D.cu:1290-1306
@@ -603,7 +615,7 @@ cudaError_t enqueue_finish(fz_handle* h) {
     Timer t(h, 4);
     R* const* u1 = (R* const*)h->U[h->i1];
     e = fz::launch_receivers<R>(u1[0], u1[1], u1[2], u1[3], h->d_rec_cell, h->nrec * h->nb, h->d_ir, h->d_vel,
-                                h->rec_cap, h->d_step, h->d_err, h->stream);
+                                h->rec_cap, h->d_step, h->d_err, h->ncell_dev * h->nb, h->stream);
     if (e != cudaSuccess) return e;
     if (h->sl_on) {
       e = fz::launch_slices<R>(u1[0], u1[1], u1[2], u1[3], h->Nx, h->Ny, h->Nz, h->Sx, h->sl_i, h->sl_j, h->sl_k,
@@ -1284,6 +1296,9 @@ int fz_sync(fz_handle* h, int64_t timeout_ms) {
       if (kerr & fz::KERR_NONFINITE)
         return set_error(h, FZ_ENONFINITE, "a receiver sampled NaN or Inf: the solution blew up (check the "
                                                "materials' passivity, the CFL number and the initial fields)");
+      if (kerr & fz::KERR_BOUNDS)
+        return set_error(h, FZ_EBOUNDS, "the bounds-checked build caught an index outside its array (error word " +
+                                             std::to_string(kerr) + ")");
       if (kerr != 0) return set_error(h, FZ_ECUDA, "device error word " + std::to_string(kerr));
       return FZ_OK;
     }

@@ -99,11 +99,36 @@ struct StageArgs {
   R half_dt;
   const int64_t* step;  // device step counter n
   int32_t* err;         // set to a nonzero FZ_KERR_* code when a bounded wait gives up
+  // array sizes for the bounds-checked build: elements of one field array (all members), of the
+  // psi tiles per axis, of the cPML tables per axis
+  int64_t nfield;
+  int64_t npsi[3];
+  int64_t npc[3];
 };
 
 // Kernel error codes written to the handle's device error word.
 constexpr int32_t KERR_TMA_TIMEOUT = 1;
 constexpr int32_t KERR_NONFINITE = 2;  // a receiver sampled NaN or Inf (the solution blew up)
+constexpr int32_t KERR_BOUNDS = 4;     // the bounds-checked build caught an index outside its array
+
+// Index check of the bounds-checked build (compiled with -DFZ_BOUNDS_CHECK): an index outside
+// [0, n) sets KERR_BOUNDS in the error word and the access is skipped. In the normal build the
+// check is the constant true and costs nothing.
+#if defined(__CUDACC__)
+__device__ __forceinline__ bool fz_inb(int32_t* err, int64_t i, int64_t n) {
+#ifdef FZ_BOUNDS_CHECK
+  if (i < 0 || i >= n) {
+    atomicOr(err, KERR_BOUNDS);
+    return false;
+  }
+#else
+  (void)err;
+  (void)i;
+  (void)n;
+#endif
+  return true;
+}
+#endif
 
 // TMA descriptors of one stage launch: the stage-input fields p, u, v as halo tiles
 // (PW x PH x 1), the base state U0 as own tiles (TX x TY x 1; stages 1 and 2) and the class bytes
@@ -149,6 +174,8 @@ struct BandArgs {
   double* s2L;
   const double* s2M;
   const double* s2R;
+  int32_t* err;    // device error word (bounds-checked build)
+  int64_t nfield;  // elements of one field array (bounds-checked build)
 };
 
 }  // namespace fz

@@ -187,6 +187,7 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
   auto ld_pw = [&](int kk) -> P {
     if (!col_ok) return psplat<R>(R(0));
     const int64_t g = col + plane * kk;
+    if (!fz_inb(A.err, g, A.nfield)) return psplat<R>(R(0));
     return pmk(A.pi[g], A.wi[g]);
   };
 
@@ -282,7 +283,7 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
       issue(it + 2);
     }
 
-    if (valid && (cls & (CLS_UPDATE | CLS_SOURCE))) {
+    if (valid && (cls & (CLS_UPDATE | CLS_SOURCE)) && fz_inb(A.err, gk, A.nfield)) {
       const int64_t g = gk;
       if (cls & CLS_UPDATE) {
         // ---- face fluxes of this cell; flux differences (times h): .x pressure, .y velocity
@@ -320,34 +321,40 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
           vn = third * bv + two3 * (v_in + A.dt_h * Ly.y);
           wn = third * bw + two3 * (w_in + A.dt_h * Lz.y);
         }
-        if (pml_xy || (A.pml_on && A.pcz[k].tile >= 0)) {
+        if (pml_xy || (A.pml_on && fz_inb(A.err, k, A.npc[2]) && A.pcz[k].tile >= 0)) {
           // cPML (functions3D.cuh:725-755): field += w dt ((1/kappa - 1) D + psi), psi frozen
           // within the step and advanced once, in stage 2, by recursive convolution.
           const PmlCoef<R> cx = A.pcx[i], cy = A.pcy[j], cz = A.pcz[k];
           const int64_t d2 = A.pml_d2;
           if (cx.tile >= 0) {
             const int64_t X = cx.tile + d2 * ((int64_t)j + (int64_t)A.Ny * k);
+            if (fz_inb(A.err, X, A.npsi[0])) {
             const P ps = A.psix[X];
             const R Dp = Lx.x * A.inv_h, Du = Lx.y * A.inv_h;
             pn += A.wdt * (cx.kinv1 * Dp + ps.x);
             un += A.wdt * (cx.kinv1 * Du + ps.y);
             if (STAGE == 2) A.psix[X] = pmk(cx.b * ps.x + cx.ca * Dp, cx.b * ps.y + cx.ca * Du);
+            }
           }
           if (cy.tile >= 0) {
             const int64_t Y = (int64_t)i + (int64_t)A.Nx * ((int64_t)cy.tile + d2 * k);
+            if (fz_inb(A.err, Y, A.npsi[1])) {
             const P ps = A.psiy[Y];
             const R Dp = Ly.x * A.inv_h, Dv = Ly.y * A.inv_h;
             pn += A.wdt * (cy.kinv1 * Dp + ps.x);
             vn += A.wdt * (cy.kinv1 * Dv + ps.y);
             if (STAGE == 2) A.psiy[Y] = pmk(cy.b * ps.x + cy.ca * Dp, cy.b * ps.y + cy.ca * Dv);
+            }
           }
           if (cz.tile >= 0) {
             const int64_t Z = (int64_t)i + (int64_t)A.Nx * ((int64_t)j + (int64_t)A.Ny * cz.tile);
+            if (fz_inb(A.err, Z, A.npsi[2])) {
             const P ps = A.psiz[Z];
             const R Dp = Lz.x * A.inv_h, Dw = Lz.y * A.inv_h;
             pn += A.wdt * (cz.kinv1 * Dp + ps.x);
             wn += A.wdt * (cz.kinv1 * Dw + ps.y);
             if (STAGE == 2) A.psiz[Z] = pmk(cz.b * ps.x + cz.ca * Dp, cz.b * ps.y + cz.ca * Dw);
+            }
           }
         }
         if (cls & CLS_SOURCE) pn += source_sum(A, g);
@@ -419,6 +426,9 @@ __global__ void __launch_bounds__(256, (sizeof(R) == 4 && KM > 0 && KM <= 2) ? 4
   const int64_t q = cell + rc.z;
   const int m = rc.w;
   const int64_t nB = B.nB;
+  if (!fz_inb(B.err, cell, B.nfield) || !fz_inb(B.err, q, B.nfield) ||
+      !fz_inb(B.err, q + B.plane + B.Sx + 1, B.nfield))
+    return;
   const V4 g4 = reinterpret_cast<const V4*>(B.geo)[b];
   const V4 n4 = reinterpret_cast<const V4*>(B.nrm)[b];
   // the cell's own stage output (written by the stage kernel, blended here by this thread only)
@@ -527,10 +537,11 @@ __global__ void __launch_bounds__(256, (sizeof(R) == 4 && KM > 0 && KM <= 2) ? 4
 template <class R>
 __global__ void k_receivers(const R* __restrict__ p, const R* __restrict__ u, const R* __restrict__ v,
                             const R* __restrict__ w, const int64_t* __restrict__ rcell, int nrec,
-                            double* ir, double* vel, int64_t cap, int64_t* step, int32_t* err) {
+                            double* ir, double* vel, int64_t cap, int64_t* step, int32_t* err, int64_t nfield) {
   const int64_t n = *step;
   for (int r = threadIdx.x; r < nrec; r += blockDim.x) {
     const int64_t c = rcell[r];
+    if (!fz_inb(err, c, nfield)) continue;
     const double pp = (double)p[c], uu = (double)u[c], vv = (double)v[c], ww = (double)w[c];
     // health word: a blown-up solution reaches the receivers (their samples are read anyway)
     if (!isfinite(pp) || !isfinite(uu) || !isfinite(vv) || !isfinite(ww)) atomicOr(err, KERR_NONFINITE);
@@ -729,8 +740,9 @@ cudaError_t launch_band(int stage, const BandArgs<R>& a, cudaStream_t s) {
 
 template <class R>
 cudaError_t launch_receivers(const R* p, const R* u, const R* v, const R* w, const int64_t* rcell, int nrec,
-                             double* ir, double* vel, int64_t cap, int64_t* step, int32_t* err, cudaStream_t s) {
-  k_receivers<R><<<1, 256, 0, s>>>(p, u, v, w, rcell, nrec, ir, vel, cap, step, err);
+                             double* ir, double* vel, int64_t cap, int64_t* step, int32_t* err, int64_t nfield,
+                             cudaStream_t s) {
+  k_receivers<R><<<1, 256, 0, s>>>(p, u, v, w, rcell, nrec, ir, vel, cap, step, err, nfield);
   return cudaGetLastError();
 }
 
@@ -764,7 +776,7 @@ cudaError_t launch_energy(const R* p, const R* u, const R* v, const R* w, int64_
   template cudaError_t launch_band<R>(int, const BandArgs<R>&, cudaStream_t);                      \
   template cudaError_t launch_receivers<R>(const R*, const R*, const R*, const R*, const int64_t*, \
                                            int, double*, double*, int64_t, int64_t*, int32_t*,     \
-                                           cudaStream_t);                                          \
+                                           int64_t, cudaStream_t);                                 \
   template cudaError_t launch_count_nonfinite<R>(const R*, const R*, const R*, const R*, int64_t,  \
                                                  unsigned long long*, int, cudaStream_t);         \
   template cudaError_t launch_slices<R>(const R*, const R*, const R*, const R*, int, int, int, int64_t, int, int, \

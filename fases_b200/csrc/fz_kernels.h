@@ -21,7 +21,7 @@ cudaError_t launch_band(int stage, const BandArgs<R>& a, cudaStream_t s);
 template <class R>
 cudaError_t launch_receivers(const R* p, const R* u, const R* v, const R* w, const int64_t* rcell,
                              int nrec, double* ir, double* vel, int64_t cap, int64_t* step, int32_t* err,
-                             cudaStream_t s);
+                             int64_t nfield, cudaStream_t s);
 template <class R>
 cudaError_t launch_count_nonfinite(const R* p, const R* u, const R* v, const R* w, int64_t n,
                                    unsigned long long* count, int nsm, cudaStream_t s);

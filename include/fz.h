@@ -44,6 +44,7 @@ extern "C" {
 #define FZ_ETIMEOUT -7     /* a bounded device wait gave up */
 #define FZ_ENONFINITE -8   /* health check found NaN/Inf in the state */
 #define FZ_ENODEV -9       /* no usable CUDA device */
+#define FZ_EBOUNDS -10     /* the bounds-checked build (libfz_checked.so) caught an out-of-range index */
 
 /* precision modes */
 #define FZ_FP32 0  /* FP32 field state; FP64 ADE state, receiver samples and energy (default) */
