@@ -262,6 +262,9 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
   sa.firho = (R)(0.5 / p.rho);
   sa.pml_on = h->pml_on ? 1 : 0;
   sa.pml_d2 = (int)d2;
+  sa.err = h->d_err;
+  sa.nfield = N;
+  for (int a = 0; a < 3; a++) sa.npsi[a] = (int64_t)(psi_b[a] / sizeof(P));
   sa.pcx = (const fz::PmlCoef<R>*)h->d_pml_coef[0];
   sa.pcy = (const fz::PmlCoef<R>*)h->d_pml_coef[1];
   sa.pcz = (const fz::PmlCoef<R>*)h->d_pml_coef[2];
@@ -312,6 +315,8 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
     ba.beta = m;
   }
   ba.gcell = d_gcell;
+  ba.err = h->d_err;
+  ba.nfield = N;
   ba.probe = d_probe;
 
   // buffer roles: A = adjoint of the step's output, B/D = of the stage-2/stage-1 inputs, C = of U0
@@ -423,6 +428,9 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
             pa.inv_h = sa.inv_h; pa.frc2 = sa.frc2; pa.firho = sa.firho; pa.fc = sa.fc;
             pa.wdt = w * p.dt;
             pa.g = d_gpml + (size_t)a * 6 * d;
+            pa.err = h->d_err;
+            pa.nfield = N;
+            pa.npsi = (int64_t)(psi_b[a] / sizeof(P));
             FZ_ACUDA(h, fz::launch_adj_pml_grad<R>(pa, h->nsm, s), "adjoint cPML gradient");
           }
         set_in(sa, in_st[st]);

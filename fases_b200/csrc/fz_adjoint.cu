@@ -161,9 +161,12 @@ __device__ __forceinline__ void adj_g_local(const AdjStageArgs<R>& A, int d, int
     coef += A.wdt * pc.kinv1 * A.inv_h;
     if (A.stage == 2) {
       const P* lpsi = (d == 0) ? A.lpsix : (d == 1) ? A.lpsiy : A.lpsiz;
-      const P l = lpsi[psi_index(A, d, i, j, k, pc.tile)];
-      gp = pc.ca * A.inv_h * l.x;
-      gv = pc.ca * A.inv_h * l.y;
+      const int64_t x = psi_index(A, d, i, j, k, pc.tile);
+      if (fz_inb(A.err, x, A.npsi[d])) {
+        const P l = lpsi[x];
+        gp = pc.ca * A.inv_h * l.x;
+        gv = pc.ca * A.inv_h * l.y;
+      }
     }
   }
   gp += coef * lp;
@@ -221,8 +224,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_adj_stage(const AdjStageArgs<R>
   auto prefetch = [&](int k) {
 #pragma unroll
     for (int q = 0; q < NE; q++) {
-      const bool ok = rin[q] && k < Nz;
       const int64_t g = roff[q] + plane * (int64_t)k;
+      const bool ok = rin[q] && k < Nz && fz_inb(A.err, g, A.nfield);
       pre[q][0] = ok ? A.pi[g] : R(0);
       pre[q][1] = ok ? A.ui[g] : R(0);
       pre[q][2] = ok ? A.vi[g] : R(0);
@@ -244,7 +247,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_adj_stage(const AdjStageArgs<R>
       }
     }
   };
-  auto ldz = [&](const R* f, int k) -> R { return (col_in && k >= 0 && k < Nz) ? f[col + plane * k] : R(0); };
+  auto ldz = [&](const R* f, int k) -> R {
+    return (col_in && k >= 0 && k < Nz && fz_inb(A.err, col + plane * k, A.nfield)) ? f[col + plane * k] : R(0);
+  };
 
   // z queues at centre plane kc: values at kc-2 .. kc+2, weights at kc-1 .. kc+1, contribution
   // windows for planes kc-2 .. kc+2
@@ -275,7 +280,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_adj_stage(const AdjStageArgs<R>
   const PmlCoef<R> pci = sPx[tx + 3], pcj = sPy[ty + 3];
   auto gz_cell = [&](int k) -> P {
     R gp = R(0), gv = R(0);
-    if (col_in && k >= 0 && k < Nz) {
+    if (col_in && k >= 0 && k < Nz && fz_inb(A.err, col + plane * (int64_t)k, A.nfield)) {
       const int64_t c = col + plane * (int64_t)k;
       adj_g_local(A, 2, i, j, k, A.cls[c], A.lp[c], A.lw[c], sPz[k - kb + 3], gp, gv);
     }
@@ -297,13 +302,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_adj_stage(const AdjStageArgs<R>
     // ---- loads for later in this iteration and for the next plane
     zq[4] = pmk(ldz(A.pi, kc + 2), ldz(A.wi, kc + 2));
     const int kz1 = kc + 1;
-    const bool z1 = col_in && kz1 >= 0 && kz1 < Nz;
     const int64_t cz1 = col + plane * (int64_t)kz1;
+    const bool z1 = col_in && kz1 >= 0 && kz1 < Nz && fz_inb(A.err, cz1, A.nfield);
     const uint8_t cls_z1 = z1 ? A.cls[cz1] : (uint8_t)0;
     const R lpz1 = z1 ? A.lp[cz1] : R(0), lwz1 = z1 ? A.lw[cz1] : R(0);
     const int kf = kc - 2;
-    const bool fl = (kf >= kb) && valid;
     const int64_t cf = col + plane * (int64_t)kf;
+    const bool fl = (kf >= kb) && valid && fz_inb(A.err, cf, A.nfield);
     const uint8_t cls_f = fl ? A.cls[cf] : (uint8_t)0;
     R Lf[4] = {R(0), R(0), R(0), R(0)};
     R Pf[4] = {R(0), R(0), R(0), R(0)};  // the accumulator this stage adds to (input or U0 adjoint)
@@ -441,6 +446,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_adj_stage(const AdjStageArgs<R>
           for (int d = 0; d < 3; d++) {
             if (pc[d].tile < 0) continue;
             const int64_t x = psi_index(A, d, i, j, kf, pc[d].tile);
+            if (!fz_inb(A.err, x, A.npsi[d])) continue;
             P l;
             if (A.stage == 2) {  // psi^{n+1} = b psi^n + ca D: carry b, then psi^n's own uses
               const P o = lin[d][x];
@@ -502,6 +508,9 @@ __global__ void __launch_bounds__(256) k_adj_band(const AdjBandArgs<R> B) {
   const int64_t q = cell + rc.z;
   const int m = rc.w;
   const int64_t nB = B.nB;
+  if (!fz_inb(B.err, cell, B.nfield) || !fz_inb(B.err, q, B.nfield) ||
+      !fz_inb(B.err, q + B.plane + B.Sx + 1, B.nfield))
+    return;
   double* gc = B.gcell + b;
   auto gadd = [&](int e, double v) { gc[(int64_t)e * nB] += v; };
   const R sx = B.geo[4 * b + 0], sy = B.geo[4 * b + 1], sz = B.geo[4 * b + 2], chi = B.geo[4 * b + 3];
@@ -589,6 +598,7 @@ __global__ void __launch_bounds__(256) k_adj_probe_scatter(const AdjBandArgs<R> 
   const int4 rc = B.rec[b];
   const int64_t cell = (int64_t)(((uint64_t)(uint32_t)rc.y << 32) | (uint32_t)rc.x);
   const int64_t q = cell + rc.z;
+  if (!fz_inb(B.err, q, B.nfield) || !fz_inb(B.err, q + B.plane + B.Sx + 1, B.nfield)) return;
   const R sx = B.geo[4 * b + 0], sy = B.geo[4 * b + 1], sz = B.geo[4 * b + 2];
   const int64_t nB = B.nB, Sx = B.Sx, pl = B.plane;
   const R lpD = B.probe[b], luD = B.probe[nB + b], lvD = B.probe[2 * nB + b], lwD = B.probe[3 * nB + b];
@@ -675,6 +685,7 @@ __global__ void __launch_bounds__(256) k_adj_pml_grad(const AdjPmlArgs<R> A) {
     const int j = (A.axis == 1) ? ca : GHOST + (int)a1;
     const int k = (A.axis == 2) ? ca : GHOST + (int)a2;
     const int64_t g = XOFF + i + A.Sx * ((int64_t)j + (int64_t)A.Ny * k);
+    if (!fz_inb(A.err, g - 3 * st, A.nfield) || !fz_inb(A.err, g + 3 * st, A.nfield)) continue;
     if (!(A.cls[g] & CLS_UPDATE)) continue;
     P q[7];
 #pragma unroll
@@ -690,6 +701,7 @@ __global__ void __launch_bounds__(256) k_adj_pml_grad(const AdjPmlArgs<R> A) {
       const int64_t X = (A.axis == 0)   ? tile + (int64_t)d2 * ((int64_t)j + (int64_t)A.Ny * k)
                         : (A.axis == 1) ? i + (int64_t)A.Nx * ((int64_t)tile + (int64_t)d2 * k)
                                         : i + (int64_t)A.Nx * ((int64_t)j + (int64_t)A.Ny * tile);
+      if (!fz_inb(A.err, X, A.npsi)) continue;
       const P lps = A.lpsi[X], ps = A.psin[X];
       atomicAdd(&gs[3 * tile + 1], (double)lps.x * (double)ps.x + (double)lps.y * (double)ps.y);
       atomicAdd(&gs[3 * tile + 2], (double)lps.x * (double)Dp + (double)lps.y * (double)Dv);

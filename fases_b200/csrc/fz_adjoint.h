@@ -56,6 +56,10 @@ struct AdjStageArgs {
   int32_t kz_chunk;  // z planes per CTA of the fused stage adjoint
   int32_t acc_in;    // 1: add to the input adjoint (it holds U0's adjoint already), 0: store it
   int32_t acc_base;  // 1: add to U0's adjoint, 0: store it (stages 1 and 2)
+  // bounds-checked build: device error word, elements of one field array and of the psi tiles
+  int32_t* err;
+  int64_t nfield;
+  int64_t npsi[3];
 };
 
 // Adjoint of the immersed band of one stage (functions3D.cuh:426-565), with the gradient of the
@@ -111,6 +115,8 @@ struct AdjBandArgs {
   double* gs2R;
   double* gcell;  // [1 + 2K + 4L][nB]: per band cell, d J / d (Rinf, A[K], zeta[K], B[L], C[L],
                   // alpha[L], beta[L]) of its material, accumulated over stages and steps
+  int32_t* err;     // bounds-checked build: device error word, elements of one field array
+  int64_t nfield;
 };
 
 // Gradient with respect to the cPML table entries (1/kappa - 1, b, ca) of one axis from one stage.
@@ -136,6 +142,8 @@ struct AdjPmlArgs {
   R inv_h, frc2, firho, fc;
   double wdt;
   double* g;
+  int32_t* err;  // bounds-checked build: device error word, elements of a field array and psi tile
+  int64_t nfield, npsi;
 };
 template <class R>
 cudaError_t launch_adj_pml_grad(const AdjPmlArgs<R>& a, int nsm, cudaStream_t s);

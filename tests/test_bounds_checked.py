@@ -1,11 +1,12 @@
 """The bounds-checked build (libfz_checked.so, compiled with -DFZ_BOUNDS_CHECK; loaded when
-FZ_BOUNDS_CHECK=1): every computed global index of the stage, band and receiver kernels is checked
-against its array and an out-of-range one would set an error bit (FZ_EBOUNDS at the next sync)
-instead of being accessed. compute-sanitizer is not available for this purpose, so this build
-stands in for its memcheck on the stepping kernels. The same solves -- cPML on every face, an
-obstacle band, PCS source, receivers; a batch of three; a planar room; FP32 and FP64 -- run in a
-child process on the checked build must finish without an error and reproduce the normal build's
-traces bit for bit."""
+FZ_BOUNDS_CHECK=1): every computed global index of the stepping kernels (stage, band, receivers)
+and of the adjoint kernels is checked against its array, and an out-of-range one would set an
+error bit (FZ_EBOUNDS at the next sync) instead of being accessed. compute-sanitizer is not
+available for this purpose, so this build stands in for its memcheck. The same solves -- cPML on
+every face, an obstacle band, PCS source, receivers; a batch of three; ragged tiles; FP32 and
+FP64 -- and a gradient with every output (materials, sources, cPML, initial fields) run in a child
+process on the checked build must finish without an error and reproduce the normal build's traces
+bit for bit (the gradient to 1e-5: its atomics sum in a varying order)."""
 import ctypes
 import json
 import os
@@ -39,6 +40,14 @@ b = tb._solver(cfg, "fp32", batch=3, members=np.arange(3))
 b.run(21)
 out["batch"] = b.ir().tolist()
 b.close()
+from tests import test_adjoint_params as ap
+cfg = ap._cfg()
+tgt = ap._target(cfg)
+s = ap._solver(cfg, precision="fp32")
+g = s.misfit_gradient(tgt, segment_steps=16, sources=True, pml=True, initial=True)
+s.close()
+out["grad"] = [g["raw"].ravel().tolist(), g["sval"].tolist(), [g["pml"][k] for k in ("R0", "kappa_max", "alpha_max")],
+               g["initial"][0].ravel().tolist()]
 print(json.dumps(out))
 '''
 
@@ -69,4 +78,9 @@ def test_checked_build_runs_clean_and_matches():
     b = _run(False)
     assert a.keys() == b.keys()
     for k in a:
-        assert np.array_equal(np.asarray(a[k]), np.asarray(b[k])), k
+        if k == "grad":  # the adjoint's atomics sum in an order that varies from run to run
+            for x, y in zip(a[k], b[k]):
+                x, y = np.asarray(x), np.asarray(y)
+                assert np.linalg.norm(x - y) <= 1e-5 * np.linalg.norm(y), k
+        else:
+            assert np.array_equal(np.asarray(a[k]), np.asarray(b[k])), k
