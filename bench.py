@@ -11,8 +11,8 @@ flush is needed between steps.
 
 --impl reference times the CPU restatement of the reference update loop (the reference has no
 CPU solver of its own; its CUDA solver has no library interface) on bounded z-slab samples of
-the same room. Multi-GPU: independent replicas, one per rank (the north star is one GPU per
-solve; a 2nd GPU solves its own room), max time over ranks.
+the same room. Multi-GPU: independent replicas, one per rank (one solve runs on one GPU; a
+second GPU solves its own room), max time over ranks.
 """
 import argparse
 import json

@@ -180,7 +180,9 @@ def prune(dest):
 
 
 if __name__ == "__main__":
-    out_root = os.path.abspath(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden"))
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_golden.py OUTPUT_DIR")
+    out_root = os.path.abspath(sys.argv[1])
     rc_all = 0
     for case in CASES:
         dest = os.path.join(out_root, case)

@@ -1,7 +1,7 @@
 """Same project, same B200: the reference solver `fases3D` (built from its own sources for sm_100a
 by oracle/build_ref.sh) against this stepper driven through fz_load_project on the reference's own
 scene cache. Checks that the receiver traces agree and that this stepper is faster, and writes both
-timings to gpurun_out/reference_speed.json when that folder exists.
+timings to $FZ_RESULTS_DIR/reference_speed.json when that variable names a folder.
 
 Room (default 5 x 4 x 2 m at h = 0.02 m = 250 x 200 x 100 cells, 5 obstacles, one cPML face,
 PCS source, 8 receivers) can be scaled with FZ_REFSPEED_ROOM="Lx Ly Lz" (metres)."""
@@ -88,8 +88,8 @@ def test_this_stepper_beats_the_reference_on_the_same_project(tmp_path):
         "speedup_loop": t_ref_loop / t_fz_wall, "speedup_device": t_ref_loop / t_fz_dev, "ir_rel_l2_vs_reference": errs,
     }
     print(json.dumps(result))
-    outdir = os.path.join(ROOT, "gpurun_out")
-    if os.path.isdir(outdir):
+    outdir = os.environ.get("FZ_RESULTS_DIR", "")
+    if outdir and os.path.isdir(outdir):
         with open(os.path.join(outdir, "reference_speed.json"), "w") as f:
             json.dump(result, f, indent=1)
     assert max(errs) < 5e-5, errs
