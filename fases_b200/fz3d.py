@@ -1,6 +1,6 @@
 """Command-line drop-in for the FVM part of `fases3D` (3D-solver/core/main3D.cu:26-1449):
 
-    python -m fases_b200.fz3d <scene.obj> <config.txt> <src.txt> <rec.txt> [--fp64] [--estimate]
+    python -m fases_b200.fz3d <scene.obj> <config.txt> <src.txt> <rec.txt> [--fp64] [--estimate] [--no-autotune]
 
 Reads the same project files through libfz.so (fz_load_project), runs the Nt time steps of the
 configuration on the GPU, prints the integer progress lines the GUI parses ("NN%" every 5 %,
@@ -96,13 +96,16 @@ def estimate(scene, config, precision="fp32", device=0):
 def main(argv=None):
     argv = list(sys.argv[1:] if argv is None else argv)
     if len(argv) < 4:
-        print("Usage: fz3d <scene> <config> <src> <rec> [--fp64]")
+        print("Usage: fz3d <scene> <config> <src> <rec> [--fp64] [--estimate] [--no-autotune]")
         return 1
     precision = "fp64" if "--fp64" in argv else "fp32"
     scene, config, src, rec = argv[:4]
     if "--estimate" in argv:
         return estimate(scene, config, precision)
     s, nt = Solver.from_project(scene, config, src, rec, precision=precision)
+    if nt >= 200 and "--no-autotune" not in argv:
+        depth, _ = s.autotune()  # a few stage launches; pays for itself on runs of this length
+        print(f"[OK] stage tile depth {depth} planes (autotuned)", flush=True)
     print(f"[OK] Will now start {nt} iterations", flush=True)
     t0 = time.perf_counter()
     s.run_progress(nt, lambda done, total: print("%d%%" % int(100.0 * done / total + 0.5), flush=True), 5)
