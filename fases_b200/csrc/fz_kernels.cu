@@ -287,11 +287,9 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
       const int64_t g = gk;
       if (cls & CLS_UPDATE) {
         // ---- face fluxes of this cell; flux differences (times h): .x pressure, .y velocity
-        const P Fx_lo = godunov<R>(XCm[ty * (TX + 2) + tx], xp, kA, kC);
-        const P Fx_hi = godunov<R>(xm, XCp[ty * (TX + 2) + tx + 2], kA, kC);
-        const P Fy_lo = godunov<R>(YCm[ty * TX + tx], yp, kA, kC);
-        const P Fy_hi = godunov<R>(ym, YCp[(ty + 2) * TX + tx], kA, kC);
-        const P Lx = psub(Fx_lo, Fx_hi), Ly = psub(Fy_lo, Fy_hi), Lz = psub(Fz_lo, Fz_hi);
+        const P Lx = godunov_diff<R>(XCm[ty * (TX + 2) + tx], xp, xm, XCp[ty * (TX + 2) + tx + 2], kA, kC);
+        const P Ly = godunov_diff<R>(YCm[ty * TX + tx], yp, ym, YCp[(ty + 2) * TX + tx], kA, kC);
+        const P Lz = psub(Fz_lo, Fz_hi);
         const R Lp = Lx.x + Ly.x + Lz.x;
         const int c0 = (ty + HY) * PW + (tx + HX);
         const R p_in = DIM2 ? Tp[c0] : qb.x, w_in = DIM2 ? A.wi[g] : qb.y;

@@ -121,4 +121,17 @@ __device__ __forceinline__ typename Pair<R>::T godunov(typename Pair<R>::T vm, t
   return pfma(dif, kC, pmul(pswap(sum), kA));
 }
 
+// Difference of the Godunov fluxes through the low and the high face of a cell, F(lo) - F(hi),
+// from the face states (left state of a face = V- of the centre below it, right state = V+ of the
+// centre above): the flux is linear in the states, so the difference is taken on the sums and
+// differences first and swapped and scaled once.
+template <class R>
+__device__ __forceinline__ typename Pair<R>::T godunov_diff(typename Pair<R>::T vm_lo, typename Pair<R>::T vp_lo,
+                                                            typename Pair<R>::T vm_hi, typename Pair<R>::T vp_hi,
+                                                            typename Pair<R>::T kA, typename Pair<R>::T kC) {
+  const typename Pair<R>::T S = psub(padd(vm_lo, vp_lo), padd(vm_hi, vp_hi));
+  const typename Pair<R>::T D = psub(psub(vp_lo, vm_lo), psub(vp_hi, vm_hi));
+  return pfma(D, kC, pmul(pswap(S), kA));
+}
+
 }  // namespace fz
