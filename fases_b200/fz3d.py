@@ -1,6 +1,7 @@
 """Command-line drop-in for the FVM part of `fases3D` (3D-solver/core/main3D.cu:26-1449):
 
-    python -m fases_b200.fz3d <scene.obj> <config.txt> <src.txt> <rec.txt> [--fp64] [--estimate] [--no-autotune]
+    python -m fases_b200.fz3d <scene.obj> <config.txt> <src.txt> <rec.txt> [--fp64] [--estimate]
+                              [--keep-other-sources] [--no-autotune]
 
 Reads the same project files through libfz.so (fz_load_project), runs the Nt time steps of the
 configuration on the GPU, prints the integer progress lines the GUI parses ("NN%" every 5 %,
@@ -40,6 +41,48 @@ def _src_index(config_path):
         except ValueError:
             continue
     return int(vals[17]) if len(vals) > 17 else 0
+
+
+_SLICE_FILES = ("pressureX.bin", "pressureY.bin", "pressureZ.bin", "Iy_X.bin", "Iz_X.bin", "Ix_Y.bin", "Iz_Y.bin",
+                "Ix_Z.bin", "Iy_Z.bin", "header.txt", "pre_header.txt")
+
+
+def purge_outputs(out_dir, src_idx, keep_other_sources=False):
+    """Removes the stale outputs of earlier runs before a run, as fases3D does (main3D.cu:170-216):
+    the animation slices, header.txt and pre_header.txt, and every IR/VEL/HIR/HRT/ARR*.bin (their
+    names vary with receivers, sources and bands, and a changed dt leaves bins of another length);
+    with keep_other_sources (--keep-other-sources, the auralization runs 2..N) only the bins of
+    this source are removed. S.bin / oid.bin stay: they are the scene cache."""
+    if not os.path.isdir(out_dir):
+        return []
+    removed = []
+    for fn in _SLICE_FILES:
+        p = os.path.join(out_dir, fn)
+        if os.path.exists(p):
+            os.remove(p)
+            removed.append(fn)
+
+    def file_src(name):  # PREFIX<rec>_<src>[_band].bin -> <src>
+        u = name.find("_")
+        if u < 0:
+            return -1
+        rest = name[u + 1:]
+        e = min([i for i in (rest.find("_"), rest.find(".")) if i >= 0] or [len(rest)])
+        try:
+            return int(rest[:e])
+        except ValueError:
+            return -1
+
+    for fn in sorted(os.listdir(out_dir)):
+        if not fn.endswith(".bin") or len(fn) <= 4:
+            continue
+        if not any(fn.startswith(pfx) for pfx in ("HIR", "HRT", "IR", "ARR", "VEL")):
+            continue
+        if keep_other_sources and file_src(fn) != src_idx:
+            continue
+        os.remove(os.path.join(out_dir, fn))
+        removed.append(fn)
+    return removed
 
 
 def _config_values(config_path):
@@ -96,12 +139,17 @@ def estimate(scene, config, precision="fp32", device=0):
 def main(argv=None):
     argv = list(sys.argv[1:] if argv is None else argv)
     if len(argv) < 4:
-        print("Usage: fz3d <scene> <config> <src> <rec> [--fp64] [--estimate] [--no-autotune]")
+        print("Usage: fz3d <scene> <config> <src> <rec> [--fp64] [--estimate] [--keep-other-sources] [--no-autotune]")
         return 1
     precision = "fp64" if "--fp64" in argv else "fp32"
     scene, config, src, rec = argv[:4]
     if "--estimate" in argv:
         return estimate(scene, config, precision)
+    if "--ga-only" in argv or "--dump-rays" in argv:
+        print("[!] --ga-only / --dump-rays run the geometric-acoustics part (image sources, ray tracing), "
+              "which this solver does not implement", flush=True)
+        return 2
+    purge_outputs(_project_output_dir(config), _src_index(config), "--keep-other-sources" in argv)
     s, nt = Solver.from_project(scene, config, src, rec, precision=precision)
     if nt >= 200 and "--no-autotune" not in argv:
         depth, _ = s.autotune()  # a few stage launches; pays for itself on runs of this length

@@ -63,3 +63,28 @@ def test_cli_runs_a_project_without_cache(tmp_path):
     mem = [ln for ln in e.stdout.splitlines() if ln.startswith("[MEM]")]
     assert mem and "voxels=%d" % (nx * ny * nz) in mem[0]
     assert "[OK] estimate: V =" in e.stdout
+
+
+def test_stale_outputs_are_purged_like_the_reference(tmp_path):
+    # main3D.cu:170-216: slices and headers go, every IR/VEL/HIR/HRT/ARR bin goes; with
+    # --keep-other-sources only this source's bins go; the scene cache stays
+    from fases_b200.fz3d import purge_outputs
+    out = tmp_path / "output"
+    out.mkdir()
+    names = ["IR0_0.bin", "IR1_0.bin", "IR0_1.bin", "VEL0_1.bin", "HIR0_1_125.bin", "HRT2_0_250.bin", "ARR1_1.bin",
+             "pressureX.bin", "Iy_X.bin", "header.txt", "pre_header.txt", "S.bin", "oid.bin", "scene_cache.txt",
+             "notes.txt"]
+    for n in names:
+        (out / n).write_bytes(b"x")
+    purge_outputs(str(out), 1, keep_other_sources=True)
+    left = sorted(p.name for p in out.iterdir())
+    assert left == sorted(["IR0_0.bin", "IR1_0.bin", "HRT2_0_250.bin", "S.bin", "oid.bin", "scene_cache.txt",
+                           "notes.txt"])
+    purge_outputs(str(out), 1)
+    left = sorted(p.name for p in out.iterdir())
+    assert left == ["S.bin", "notes.txt", "oid.bin", "scene_cache.txt"]
+
+
+def test_geometric_acoustics_flags_are_refused():
+    from fases_b200.fz3d import main
+    assert main(["a.obj", "c.txt", "s.txt", "r.txt", "--ga-only"]) == 2
