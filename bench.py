@@ -439,8 +439,9 @@ def main():
     s = make_solver(b, args.precision, nsteps_total + 31, device=local)
     info = s.info()
     s.run(args.warmup)
-    depth, _ = s.autotune()  # tile depth of the stage kernels, timed on this room
+    depth, _ = s.autotune()  # z chunks of the stage kernels, timed on this room
     depth_heuristic = s.kz_chunk()[1]
+    zsched = s.z_schedule()
     barrier(pg)
     # the timed steps: CUDA graphs of 10 steps, as fz_run issues them
     with Clocks(local) as clk:
@@ -524,7 +525,7 @@ def main():
                        "l2": "inputs larger than L2 (3 field sets of 4 x 183 MB)",
                        "value_per_padded_cell": value * np.prod(info["dims"]) / room_cells,
                        "tile": {"columns": [32, 16], "depth": depth, "heuristic_depth": depth_heuristic,
-                                "chosen_by": "fz_autotune"}},
+                                "z_chunks": zsched, "chosen_by": "fz_autotune"}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": "k_stage (fused WENO-Z/Godunov/RK/cPML/source), 131/3 B per room cell per launch",

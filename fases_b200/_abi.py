@@ -125,6 +125,8 @@ SIGNATURES = {
     "fz_group_autotune": (C.c_int, [_P, _i32, _ip, _dp]),
     "fz_set_kz_chunk": (C.c_int, [_P, _i32]),
     "fz_get_kz_chunk": (C.c_int, [_P, _ip, _ip]),
+    "fz_get_z_schedule": (C.c_int, [_P, _ip, _i32, _ip]),
+    "fz_set_z_schedule": (C.c_int, [_P, _ip, _i32]),
     "fz_material_layout": (C.c_int, [_P, _ip, _ip, _ip]),
     "fz_group_create": (C.c_int, [C.POINTER(_P), _i32, C.POINTER(_P)]),
     "fz_group_run": (C.c_int, [_P, _i64]),

@@ -432,6 +432,7 @@ int finalize(fz_handle* h) {
   int occ = 1;
   FZ_CUDA(h, fz::stage_occupancy<R>(&occ), "occupancy");
   occ = std::max(1, occ);
+  h->stage_occ = occ;
   const int ntx = (h->Nx - 2 * GHOST + fz::TX - 1) / fz::TX;
   const int nty = (h->Ny - 2 * GHOST + fz::TY - 1) / fz::TY;
   const int nzi = h->Nz - 2 * GHOST;
@@ -475,6 +476,8 @@ fz::StageArgs<R> stage_args(fz_handle* h, int stage) {
   a.Sx = h->Sx; a.plane = h->plane;
   a.kz_chunk = h->kz_chunk;
   a.zchunks = h->zchunks;
+  a.zoff[0] = 0;
+  for (int c = 0; c < h->zchunks && c < fz::FZ_MAX_ZCHUNKS; c++) a.zoff[c + 1] = a.zoff[c] + h->zsizes[(size_t)c];
   const fz_params& p = h->prm;
   a.dt_h = (R)(p.dt / p.h);
   a.frc2 = (R)(0.5 * p.rho * p.c * p.c);
@@ -813,23 +816,77 @@ int bind_field_set(fz_handle* h, int set, void* const* f) {
 cudaError_t enqueue_stage_kernel(fz_handle* h, int st) {
   return h->fp64 ? ::enqueue_stage_kernel<double>(h, st) : ::enqueue_stage_kernel<float>(h, st);
 }
-void set_kz_chunk(fz_handle* h, int kz_chunk) {
+int set_z_sizes(fz_handle* h, const std::vector<int>& sizes) {
   const int nzi = h->Nz - 2 * GHOST;
-  const int c = std::max(1, std::min(nzi, kz_chunk > 0 ? kz_chunk : h->kz_heuristic));
+  int sum = 0;
+  for (int c : sizes) {
+    if (c < 1) return set_error(h, FZ_EINVAL, "z chunk of fewer than one plane");
+    sum += c;
+  }
+  if (sizes.empty() || (int)sizes.size() > fz::FZ_MAX_ZCHUNKS || sum != nzi)
+    return set_error(h, FZ_EINVAL, "z chunks must cover the interior planes in at most " +
+                                       std::to_string(fz::FZ_MAX_ZCHUNKS) + " pieces");
   const int ntx = (h->Nx - 2 * GHOST + fz::TX - 1) / fz::TX;
   const int nty = (h->Ny - 2 * GHOST + fz::TY - 1) / fz::TY;
-  const dim3 grid((unsigned)ntx, (unsigned)nty, (unsigned)(((nzi + c - 1) / c) * h->nb));
-  const bool same = (c == h->kz_chunk) && grid.x == h->stage_grid.x && grid.y == h->stage_grid.y &&
+  const dim3 grid((unsigned)ntx, (unsigned)nty, (unsigned)(sizes.size() * h->nb));
+  const bool same = sizes == h->zsizes && grid.x == h->stage_grid.x && grid.y == h->stage_grid.y &&
                     grid.z == h->stage_grid.z;
-  h->kz_chunk = c;
-  h->zchunks = (nzi + c - 1) / c;
+  h->zsizes = sizes;
+  h->zchunks = (int)sizes.size();
+  h->kz_chunk = *std::max_element(sizes.begin(), sizes.end());
   h->stage_grid = grid;
-  if (same) return;
+  if (same) return FZ_OK;
   for (auto& g : h->graph)
     if (g) {
       cudaGraphExecDestroy(g);
       g = nullptr;
     }
+  return FZ_OK;
+}
+
+void set_kz_chunk(fz_handle* h, int kz_chunk) {
+  const int nzi = h->Nz - 2 * GHOST;
+  int c = std::max(1, std::min(nzi, kz_chunk > 0 ? kz_chunk : h->kz_heuristic));
+  c = std::max(c, (nzi + fz::FZ_MAX_ZCHUNKS - 1) / fz::FZ_MAX_ZCHUNKS);
+  std::vector<int> sizes;
+  for (int z = 0; z < nzi; z += c) sizes.push_back(std::min(c, nzi - z));
+  set_z_sizes(h, sizes);
+}
+
+std::vector<int> guided_z_sizes(fz_handle* h, int depth) {
+  const int nzi = h->Nz - 2 * GHOST;
+  const int D = std::max(1, std::min(nzi, depth > 0 ? depth : h->kz_heuristic));
+  const int ntx = (h->Nx - 2 * GHOST + fz::TX - 1) / fz::TX;
+  const int nty = (h->Ny - 2 * GHOST + fz::TY - 1) / fz::TY;
+  const int rows = std::max(1, (h->nsm * h->stage_occ) / std::max(1, ntx * nty));  // chunk rows per wave
+  const int d2 = std::max(1, D / 2), d4 = std::max(1, D / 4);
+  const int tail2 = rows * d2, tail4 = rows * d4;
+  std::vector<int> sizes;
+  int left = nzi;
+  while (left > tail2 + tail4 && left > D) {
+    sizes.push_back(D);
+    left -= D;
+  }
+  while (left > tail4 && left > d2) {
+    sizes.push_back(d2);
+    left -= d2;
+  }
+  while (left > 0) {
+    const int c = std::min(d4, left);
+    sizes.push_back(c);
+    left -= c;
+  }
+  if (sizes.size() > 1 && 2 * sizes.back() < d4) {  // a sliver at the end joins the chunk before it
+    const int c = sizes.back();
+    sizes.pop_back();
+    sizes.back() += c;
+  }
+  if ((int)sizes.size() > fz::FZ_MAX_ZCHUNKS) {  // too fine: uniform chunks instead
+    sizes.clear();
+    const int c = std::max(D, (nzi + fz::FZ_MAX_ZCHUNKS - 1) / fz::FZ_MAX_ZCHUNKS);
+    for (int z = 0; z < nzi; z += c) sizes.push_back(std::min(c, nzi - z));
+  }
+  return sizes;
 }
 cudaError_t enqueue_finish(fz_handle* h) { return h->fp64 ? ::enqueue_finish<double>(h) : ::enqueue_finish<float>(h); }
 }  // namespace fzi

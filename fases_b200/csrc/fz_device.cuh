@@ -50,6 +50,8 @@ struct Pair<double> {
 };
 
 // Arguments of one stage launch.
+constexpr int FZ_MAX_ZCHUNKS = 256;  // z chunks per member a stage launch can have
+
 template <class R>
 struct StageArgs {
   typedef typename Pair<R>::T P;
@@ -69,8 +71,11 @@ struct StageArgs {
   int32_t Nx, Ny, Nz;
   int64_t Sx;     // row pitch (elements)
   int64_t plane;  // Sx * Ny
-  int32_t kz_chunk;
-  int32_t zchunks;  // z chunks per batch member: blockIdx.z = member * zchunks + chunk
+  int32_t kz_chunk;  // largest z chunk (planes per CTA)
+  int32_t zchunks;   // z chunks per batch member: blockIdx.z = member * zchunks + chunk
+  // chunk c of a member covers its interior planes [zoff[c], zoff[c+1]) (counted from the first
+  // interior plane); chunks may differ in length (long ones first, short ones for the last waves)
+  int32_t zoff[FZ_MAX_ZCHUNKS + 1];
   R dt_h;   // dt / h
   R frc2;   // 0.5 * rho * c^2
   R firho;  // 0.5 / rho

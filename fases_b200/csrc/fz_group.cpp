@@ -168,15 +168,15 @@ int fz_group_autotune(fz_group* g, int32_t reps, int32_t* kz_chunk, double* ms_p
   // one depth for every member (clamped to each room's planes), or 0: each member's own heuristic
   int nzmax = 1;
   for (fz_handle* h : g->m) nzmax = std::max(nzmax, h->Nz - 2 * fz::GHOST);
-  std::vector<int> cand{0};
+  std::vector<fzi::ZPlan> cand{{0, 0}};
   for (int c : {4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256})
-    if (c <= nzmax) cand.push_back(c);
-  int best = 0;
+    if (c <= nzmax) cand.push_back({c, 0});
+  fzi::ZPlan best{0, 0};
   rc = fzi::tune(g->m, g->stream, cand, reps, &best, ms_per_step);
   for (auto& kv : g->graphs) cudaGraphExecDestroy(kv.second);  // captured with the old launch shape
   g->graphs.clear();
   if (rc != FZ_OK) return rc;
-  if (kz_chunk) *kz_chunk = best;
+  if (kz_chunk) *kz_chunk = best.depth;
   return FZ_OK;
 }
 

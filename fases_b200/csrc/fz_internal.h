@@ -111,9 +111,11 @@ struct fz_handle {
   double* d_scratch = nullptr;
   int64_t steps_enqueued = 0;
   bool finalized = false;
-  int kz_chunk = 0;
+  int kz_chunk = 0;       // largest z chunk of the stage kernels
   int kz_heuristic = 0;  // the wave-filling choice of prepare (fz_set_kz_chunk(h, 0) returns to it)
-  int zchunks = 1;  // z chunks per member
+  int zchunks = 1;       // z chunks per member
+  std::vector<int> zsizes;  // their lengths in planes (sum = interior planes), longest first
+  int stage_occ = 1;        // stage-kernel CTAs per SM
   dim3 stage_grid;
 
   // graphs, keyed by buffer parity
@@ -158,11 +160,25 @@ cudaError_t enqueue_stage_kernel(fz_handle* h, int st);
 // tile depth of the stage kernels (z planes per CTA; 0 = the wave-filling heuristic); drops the
 // handle's captured graphs
 void set_kz_chunk(fz_handle* h, int kz_chunk);
+// z chunks of any lengths (summing to the interior planes, at most FZ_MAX_ZCHUNKS); drops graphs
+int set_z_sizes(fz_handle* h, const std::vector<int>& sizes);
+// a guided schedule: chunks of `depth` planes, then about one wave of CTAs at depth/2 and one at
+// depth/4, so the last waves are short
+std::vector<int> guided_z_sizes(fz_handle* h, int depth);
 // Times the stage kernels of every handle in hs (launched on their own streams, forked from and
 // joined to `ts`) for each candidate tile depth (0 = each handle's heuristic; others are clamped
 // to a handle's planes) and leaves every handle on the fastest; the state is left as it was.
-int tune(const std::vector<fz_handle*>& hs, cudaStream_t ts, const std::vector<int>& candidates, int reps,
-         int* best, double* ms_per_step);
-// the tile depths worth timing for one handle: the heuristic and the best-filling alternatives
-std::vector<int> kz_candidates(fz_handle* h);
+// A candidate launch shape: uniform z chunks of `depth` planes (0 = each handle's heuristic), or,
+// with guided set, the guided schedule of that depth.
+struct ZPlan {
+  int depth;
+  int guided;
+};
+int tune(const std::vector<fz_handle*>& hs, cudaStream_t ts, const std::vector<ZPlan>& candidates, int reps,
+         ZPlan* best, double* ms_per_step);
+// apply a candidate to one handle
+int apply_z_plan(fz_handle* h, const ZPlan& p);
+// the launch shapes worth timing for one handle: the heuristic, the best-filling uniform depths and
+// guided schedules of the best of them
+std::vector<ZPlan> kz_candidates(fz_handle* h);
 }  // namespace fzi

@@ -81,7 +81,7 @@ struct StageSmem {
 };
 
 // ------------------------------------------------------------------------------------------
-// Fused stage kernel. CTA = 32 x 16 columns marching in z over kz_chunk planes.
+// Fused stage kernel. CTA = 32 x 16 columns marching in z over one z chunk of planes.
 //  - x, y: plane k of p, u, v arrives by TMA into a ring of three shared-memory tiles (with a
 //    3-cell halo), issued two planes ahead, so global latency overlaps the arithmetic of the
 //    planes in between. Every x- and y-centre is evaluated once (the reference evaluates every
@@ -137,8 +137,9 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
   // batch members are stacked along z (member m owns planes [m Nz, (m+1) Nz)); the cPML z table,
   // the psi tiles and the class bytes are laid out per member the same way
   const int member = blockIdx.z / A.zchunks;
-  const int kb = GHOST + (blockIdx.z - member * A.zchunks) * A.kz_chunk + member * A.Nz;
-  const int ke = min(kb + A.kz_chunk, (member + 1) * A.Nz - GHOST);
+  const int chunk = blockIdx.z - member * A.zchunks;
+  const int kb = GHOST + member * A.Nz + A.zoff[chunk];
+  const int ke = min(GHOST + member * A.Nz + A.zoff[chunk + 1], (member + 1) * A.Nz - GHOST);
   if (kb >= ke) return;
   const int nplanes = ke - kb;
   const int64_t Sx = A.Sx, plane = A.plane;

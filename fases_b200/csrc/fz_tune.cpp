@@ -1,9 +1,10 @@
 // fz_tune.cpp -- launch-shape autotuner of the stage kernels. The tile of a stage-kernel CTA is
-// 32 x 16 columns by kz_chunk planes along z; the depth decides how many CTAs a stage launches
-// (and so how whole waves of the 148 SMs fill), and each CTA pays about 1.5 planes of start-up
-// work (two extra z centres, the TMA ring fill). prepare() picks the depth from a wave-filling
-// model; the tuner times the stage kernels of the real room for the depths worth trying and keeps
-// the fastest. For a group of rooms the depths are timed with every member's kernels running side
+// 32 x 16 columns by one z chunk of planes; the chunk lengths decide how many CTAs a stage
+// launches (and so how whole waves of the 148 SMs fill), and each CTA pays about 1.5 planes of
+// start-up work (two extra z centres, the TMA ring fill). prepare() picks a uniform depth from a
+// wave-filling model; the tuner times the stage kernels of the real room for the uniform depths
+// worth trying and for guided schedules (long chunks first, short ones for the last waves, so the
+// start-up cost stays low without a long tail) and keeps the fastest. For a group of rooms the depths are timed with every member's kernels running side
 // by side, as the group's graphs run them. The reference launches fixed TP(32,4,4) blocks
 // (3D-solver/core/main3D.cu:1280-1306) and has no tuner.
 //
@@ -80,13 +81,18 @@ int restore_state(fz_handle* h, Saved& sv) {
 
 namespace fzi {
 
-std::vector<int> kz_candidates(fz_handle* h) {
+int apply_z_plan(fz_handle* h, const ZPlan& p) {
+  if (p.guided) return set_z_sizes(h, guided_z_sizes(h, p.depth));
+  set_kz_chunk(h, p.depth);
+  return FZ_OK;
+}
+
+std::vector<ZPlan> kz_candidates(fz_handle* h) {
   const int nzi = h->Nz - 2 * GHOST;
-  std::vector<int> out{0};
+  std::vector<ZPlan> out{{0, 0}};
   if (nzi <= 1) return out;
   // every distinct depth ceil(nzi / nk) of at least 4 planes, ranked by the heuristic's model
-  int occ = 2;  // stage CTAs per SM in FP32 (one in FP64); only the ranking uses it
-  if (h->fp64) occ = 1;
+  const int occ = std::max(1, h->stage_occ);
   const int ntx = (h->Nx - 2 * GHOST + fz::TX - 1) / fz::TX;
   const int nty = (h->Ny - 2 * GHOST + fz::TY - 1) / fz::TY;
   const int64_t slots = (int64_t)h->nsm * occ;
@@ -105,12 +111,17 @@ std::vector<int> kz_candidates(fz_handle* h) {
     return a.first > b.first || (a.first == b.first && a.second > b.second);
   });
   for (size_t q = 0; q < ranked.size() && out.size() < 9; q++)
-    if (ranked[q].second != h->kz_heuristic) out.push_back(ranked[q].second);
+    if (ranked[q].second != h->kz_heuristic) out.push_back({ranked[q].second, 0});
+  // guided schedules: long chunks first, short ones for the last waves (single rooms; a batch's
+  // members run one after another in the grid, so its tail is one member's)
+  if (h->nb == 1)
+    for (int D : {h->kz_heuristic, nzi / 2, nzi / 3, nzi / 4, 64, 48, 32})
+      if (D >= 8 && D <= nzi) out.push_back({D, 1});
   return out;
 }
 
-int tune(const std::vector<fz_handle*>& hs, cudaStream_t ts, const std::vector<int>& candidates, int reps,
-         int* best, double* ms_per_step) {
+int tune(const std::vector<fz_handle*>& hs, cudaStream_t ts, const std::vector<ZPlan>& candidates, int reps,
+         ZPlan* best, double* ms_per_step) {
   if (hs.empty() || candidates.empty()) return set_global_error(FZ_EINVAL, "autotune: nothing to tune");
   reps = std::max(1, std::min(reps, 100));
   for (fz_handle* h : hs) {
@@ -145,10 +156,13 @@ int tune(const std::vector<fz_handle*>& hs, cudaStream_t ts, const std::vector<i
     }
     return x;
   };
-  int chosen = candidates[0];
+  ZPlan chosen = candidates[0];
   double best_ms = -1.0;
   for (size_t c = 0; c < candidates.size() && e == cudaSuccess; c++) {
-    for (fz_handle* h : hs) set_kz_chunk(h, candidates[c]);
+    for (fz_handle* h : hs) {
+      const int rc = apply_z_plan(h, candidates[c]);
+      if (rc != FZ_OK && e == cudaSuccess) e = cudaErrorInvalidValue;
+    }
     e = round(1);  // warm-up of this launch shape
     if (e == cudaSuccess) e = cudaEventRecord(a, ts);
     if (e == cudaSuccess) e = round(reps);
@@ -169,7 +183,7 @@ int tune(const std::vector<fz_handle*>& hs, cudaStream_t ts, const std::vector<i
   if (b) cudaEventDestroy(b);
   for (cudaEvent_t j : join)
     if (j) cudaEventDestroy(j);
-  for (fz_handle* h : hs) set_kz_chunk(h, chosen);
+  for (fz_handle* h : hs) apply_z_plan(h, chosen);
   int rc = FZ_OK;
   for (size_t q = 0; q < hs.size(); q++) {
     const int r = restore_state(hs[q], saved[q]);
@@ -197,7 +211,7 @@ int fz_autotune(fz_handle* h, int32_t reps, int32_t* kz_chunk, double* ms_per_st
   int rc = fzi::prepare(h);
   if (rc != FZ_OK) return rc;
   cudaSetDevice(h->device);
-  int best = 0;
+  fzi::ZPlan best{0, 0};
   rc = fzi::tune({h}, h->stream, fzi::kz_candidates(h), reps, &best, ms_per_step);
   if (rc != FZ_OK) return rc;
   if (kz_chunk) *kz_chunk = h->kz_chunk;
@@ -214,6 +228,28 @@ int fz_set_kz_chunk(fz_handle* h, int32_t kz_chunk) {
   if (rc != FZ_OK) return rc;
   fzi::set_kz_chunk(h, kz_chunk);
   return FZ_OK;
+}
+
+int fz_get_z_schedule(fz_handle* h, int32_t* sizes, int32_t cap, int32_t* n) {
+  if (!h) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  if (!h->have_geometry) return fzi::set_error(h, FZ_ESTATE, "fz_get_z_schedule before fz_load_geometry_raw");
+  const int rc = fzi::prepare(h);
+  if (rc != FZ_OK) return rc;
+  if (n) *n = h->zchunks;
+  if (sizes)
+    for (int c = 0; c < h->zchunks && c < cap; c++) sizes[c] = h->zsizes[(size_t)c];
+  return FZ_OK;
+}
+
+int fz_set_z_schedule(fz_handle* h, const int32_t* sizes, int32_t n) {
+  if (!h) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  if (!sizes || n < 1) return fzi::set_error(h, FZ_EINVAL, "fz_set_z_schedule: sizes[n >= 1] required");
+  if (!h->have_geometry) return fzi::set_error(h, FZ_ESTATE, "fz_set_z_schedule before fz_load_geometry_raw");
+  int rc = fzi::prepare(h);
+  if (rc != FZ_OK) return rc;
+  rc = fz_sync(h, 0);
+  if (rc != FZ_OK) return rc;
+  return fzi::set_z_sizes(h, std::vector<int>(sizes, sizes + n));
 }
 
 int fz_get_kz_chunk(fz_handle* h, int32_t* kz_chunk, int32_t* heuristic) {

@@ -212,6 +212,19 @@ class Solver:
         """Tile depth of the stage kernels (0 = the wave-filling heuristic), e.g. from a cache."""
         self._chk(lib().fz_set_kz_chunk(self._h, int(depth)))
 
+    def z_schedule(self):
+        """Lengths (planes) of the stage kernels' z chunks, longest first."""
+        n = C.c_int32()
+        self._chk(lib().fz_get_z_schedule(self._h, None, 0, C.byref(n)))
+        out = (C.c_int32 * max(1, n.value))()
+        self._chk(lib().fz_get_z_schedule(self._h, out, n.value, C.byref(n)))
+        return [out[q] for q in range(n.value)]
+
+    def set_z_schedule(self, sizes):
+        """Sets the z chunk lengths directly (summing to the interior planes), e.g. from z_schedule."""
+        arr = (C.c_int32 * len(sizes))(*[int(x) for x in sizes])
+        self._chk(lib().fz_set_z_schedule(self._h, arr, len(sizes)))
+
     def kz_chunk(self):
         """(current tile depth, heuristic tile depth)."""
         k, hk = C.c_int32(), C.c_int32()

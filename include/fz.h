@@ -222,20 +222,28 @@ int fz_group_run_timed(fz_group* g, int64_t nsteps, double* ms);
 int fz_group_sync(fz_group* g, int64_t timeout_ms);
 void fz_group_destroy(fz_group* g);
 
-/* Launch-shape autotuner. A stage-kernel CTA covers 32 x 16 columns by kz_chunk planes along z;
- * the depth sets how many CTAs a stage launches and how whole waves of SMs fill. fz_autotune times
- * the three stage kernels on this room for the heuristic depth and up to eight alternatives
+/* Launch-shape autotuner. A stage-kernel CTA covers 32 x 16 columns by one z chunk of planes;
+ * the chunk lengths set how many CTAs a stage launches and how whole waves of SMs fill. fz_autotune
+ * times the three stage kernels on this room for the heuristic depth, up to eight other uniform
+ * depths and (single rooms) guided schedules -- long chunks first, short ones for the last waves --
  * (reps steps' worth each, after one warm-up) and keeps the fastest; the state is left as it was
- * (the call does not advance the solve). kz_chunk gets the chosen depth, ms_per_step the stage
- * kernels' time per step. fz_group_autotune does the same for all members at once, timing their
- * kernels side by side with one depth for every member (clamped to each room; 0 = each member's
- * heuristic). Results do not depend on the depth (each CTA recomputes its boundary centres).
+ * (the call does not advance the solve). kz_chunk gets the chosen (longest) chunk, ms_per_step the
+ * stage kernels' time per step; fz_get_z_schedule lists the chunks. fz_group_autotune does the
+ * same for all members at once, timing their kernels side by side with one uniform depth for every
+ * member (clamped to each room; 0 = each member's heuristic). Results do not depend on the depth (each CTA recomputes its boundary centres).
  * The reference launches fixed TP(32,4,4) blocks (main3D.cu:1280-1306). */
 int fz_autotune(fz_handle* h, int32_t reps, int32_t* kz_chunk, double* ms_per_step);
 int fz_group_autotune(fz_group* g, int32_t reps, int32_t* kz_chunk, double* ms_per_step);
 /* Sets the depth directly (0 = the heuristic), e.g. from a cache of earlier tuning results. */
 int fz_set_kz_chunk(fz_handle* h, int32_t kz_chunk);
 int fz_get_kz_chunk(fz_handle* h, int32_t* kz_chunk, int32_t* heuristic);
+/* The z chunks the stage kernels use now (lengths in planes, longest first; the tuner may pick a
+ * guided schedule: long chunks first, short ones for the last waves). n gets their number; at most
+ * cap lengths are written to sizes (may be NULL). */
+int fz_get_z_schedule(fz_handle* h, int32_t* sizes, int32_t cap, int32_t* n);
+/* Sets the z chunks directly (n lengths >= 1 summing to the interior planes Nz - 6, n <= 256),
+ * e.g. a schedule fz_get_z_schedule reported for this room before. */
+int fz_set_z_schedule(fz_handle* h, const int32_t* sizes, int32_t n);
 
 /* Gradient of the receiver misfit J = sum_r sum_{n < nsteps} (IR_r[n] - target[r][n])^2 (IR_r[n] = p
  * at receiver r after step n+1, FP64) with respect to every ADE coefficient of every material, by

@@ -32,6 +32,7 @@ def test_tuner_entry_points_check_arguments():
     assert L.fz_autotune(None, 3, None, None) == _abi.FZ_EINVAL
     assert L.fz_group_autotune(None, 3, None, None) == _abi.FZ_EINVAL
     assert L.fz_set_kz_chunk(None, 4) == _abi.FZ_EINVAL
+    assert L.fz_set_z_schedule(None, None, 0) == _abi.FZ_EINVAL
 
 
 @pytest.mark.gpu
@@ -50,7 +51,12 @@ def test_tuning_mid_solve_changes_nothing(precision):
     s.run(11)
     s.set_kz_chunk(5)  # an odd depth that leaves a short last chunk
     assert s.kz_chunk()[0] == 5
-    s.run(16)
+    s.run(7)
+    nzi = s.shape[0] - 6
+    sched = [nzi - 3, 2, 1] if nzi > 3 else [nzi]  # chunks of unequal length, longest first
+    s.set_z_schedule(sched)
+    assert s.z_schedule() == sched
+    s.run(9)
     assert np.array_equal(s.ir(), ir_ref)
     for a, b in zip(s.fields(), f_ref):
         assert np.array_equal(a, b)
