@@ -30,7 +30,8 @@ def build(force: bool = False, verbose: bool = False, out: str = None, defines=(
     if not force and out == LIB and not _stale():
         return LIB
     cmd = ["nvcc", "-std=c++17", "-O3", *ARCH, "-lineinfo", "-shared",
-           "-Xcompiler", "-fPIC,-ffp-contract=off", "-I", os.path.join(HERE, "..", "include")]
+           "-Xcompiler", "-fPIC,-ffp-contract=off,-fopenmp", "-lgomp",
+           "-I", os.path.join(HERE, "..", "include")]
     if verbose:
         cmd += ["-Xptxas", "-v"]
     cmd += ["-D" + d for d in defines]

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <new>
 #include <string>
 #include <thread>
@@ -267,7 +268,17 @@ int build_band(fz_handle* h) {
   std::vector<int32_t> mat;
   h->band_cell_ref.clear();
   auto Sat = [&](int i, int j, int k) { return (double)S[ref_index(h, i, j, k)]; };
-  for (int k = GHOST; k < Nz - GHOST; k++)
+  // one list per z plane, built in parallel and joined in plane order (the build_boundary_map
+  // order of common/filterABC.h:95-108)
+  struct Plane {
+    std::vector<int64_t> cell, corner, ref;
+    std::vector<R> geo, nrm;
+    std::vector<int32_t> mat;
+  };
+  std::vector<Plane> planes((size_t)Nz);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int k = GHOST; k < Nz - GHOST; k++) {
+    Plane& P = planes[(size_t)k];
     for (int j = GHOST; j < Ny - GHOST; j++)
       for (int i = GHOST; i < Nx - GHOST; i++) {
         const int64_t rc = ref_index(h, i, j, k);
@@ -295,19 +306,28 @@ int build_band(fz_handle* h) {
           const double r = (s - hh) / (tol - hh);
           chi = 1.0 - r * r * (3.0 - 2.0 * r);
         }
-        cell.push_back(dev_index(h, i, j, k));
-        corner.push_back(dev_index(h, bi, bj, bk));
-        geo.push_back((R)(fx - bi));
-        geo.push_back((R)(fy - bj));
-        geo.push_back((R)(fzz - bk));
-        geo.push_back((R)chi);
-        nrm.push_back((R)nx);
-        nrm.push_back((R)ny);
-        nrm.push_back((R)nz);
-        nrm.push_back((R)0);
-        mat.push_back((int32_t)o - 1);
-        h->band_cell_ref.push_back(rc);
+        P.cell.push_back(dev_index(h, i, j, k));
+        P.corner.push_back(dev_index(h, bi, bj, bk));
+        P.geo.push_back((R)(fx - bi));
+        P.geo.push_back((R)(fy - bj));
+        P.geo.push_back((R)(fzz - bk));
+        P.geo.push_back((R)chi);
+        P.nrm.push_back((R)nx);
+        P.nrm.push_back((R)ny);
+        P.nrm.push_back((R)nz);
+        P.nrm.push_back((R)0);
+        P.mat.push_back((int32_t)o - 1);
+        P.ref.push_back(rc);
       }
+  }
+  for (const Plane& P : planes) {
+    cell.insert(cell.end(), P.cell.begin(), P.cell.end());
+    corner.insert(corner.end(), P.corner.begin(), P.corner.end());
+    geo.insert(geo.end(), P.geo.begin(), P.geo.end());
+    nrm.insert(nrm.end(), P.nrm.begin(), P.nrm.end());
+    mat.insert(mat.end(), P.mat.begin(), P.mat.end());
+    h->band_cell_ref.insert(h->band_cell_ref.end(), P.ref.begin(), P.ref.end());
+  }
   h->nB1 = (int64_t)cell.size();
   h->nB = h->nB1 * h->nb;
   h->band_mat = mat;
@@ -701,6 +721,7 @@ int load_geometry(fz_handle* h, const float* S, const uint8_t* oid, int Nx, int 
   h->cls_host.assign((size_t)h->ncell_dev, 0);
   int64_t nup = 0;
   const float hf = (float)h->prm.h;
+#pragma omp parallel for reduction(+ : nup) schedule(static)
   for (int k = GHOST; k < Nz - GHOST; k++)
     for (int j = GHOST; j < Ny - GHOST; j++)
       for (int i = GHOST; i < Nx - GHOST; i++)
@@ -746,7 +767,9 @@ int get_fields(fz_handle* h, double* p, double* u, double* v, double* w) {
       FZ_CUDA(h, cudaMemcpy2D(tmp.data(), rowb, src, (size_t)h->Sx * sizeof(R), rowb,
                               (size_t)h->Ny * h->Nz, cudaMemcpyDeviceToHost), "fields D2H");
       double* o = outs[f] + (size_t)m * N;
-      for (size_t c = 0; c < N; c++) o[c] = (double)tmp[c];
+      const R* t = tmp.data();
+#pragma omp parallel for schedule(static)
+      for (int64_t c = 0; c < (int64_t)N; c++) o[c] = (double)t[c];
     }
   }
   return FZ_OK;
@@ -756,7 +779,8 @@ template <class R>
 int set_fields(fz_handle* h, const double* p, const double* u, const double* v, const double* w) {
   const size_t rowb = (size_t)h->Nx * sizeof(R);
   const size_t N = (size_t)h->Nx * h->Ny * h->Nz;
-  std::vector<R> tmp(N);
+  std::unique_ptr<R[]> tmp(new (std::nothrow) R[N]);
+  if (!tmp) return set_error(h, FZ_ENOMEM, "fz_set_fields: out of host memory");
   const double* ins[4] = {p, u, v, w};
   for (int f = 0; f < 4; f++) {
     if (!ins[f]) {
@@ -766,8 +790,10 @@ int set_fields(fz_handle* h, const double* p, const double* u, const double* v, 
     for (int m = 0; m < h->nb; m++) {
       R* dst = (R*)h->U[h->i0][f] + XOFF + (size_t)m * h->ncell_dev;
       const double* in = ins[f] + (size_t)m * N;
-      for (size_t c = 0; c < N; c++) tmp[c] = (R)in[c];
-      FZ_CUDA(h, cudaMemcpy2D(dst, (size_t)h->Sx * sizeof(R), tmp.data(), rowb, rowb,
+      R* t = tmp.get();
+#pragma omp parallel for schedule(static)
+      for (int64_t c = 0; c < (int64_t)N; c++) t[c] = (R)in[c];
+      FZ_CUDA(h, cudaMemcpy2D(dst, (size_t)h->Sx * sizeof(R), tmp.get(), rowb, rowb,
                               (size_t)h->Ny * h->Nz, cudaMemcpyHostToDevice), "fields H2D");
     }
   }
