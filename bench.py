@@ -42,10 +42,12 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=12000, help="length of the end-to-end job")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    ap.add_argument("--config", default="plain3d", choices=["plain3d", "plain2d", "precision", "batched", "adjoint"],
+    ap.add_argument("--config", default="plain3d", choices=["plain3d", "plain2d", "precision", "batched", "adjoint",
+                                                            "legacy2d"],
                     help="plain3d: the headline room (default); plain2d: the 2D FP64 room; "
                          "precision: FP32 bulk vs all-FP64 on a 256^3 room; batched: 64 sources in one "
-                         "192^3 room and 32 rooms in one graph; adjoint: misfit gradient on a 256^3 room")
+                         "192^3 room and 32 rooms in one graph; adjoint: misfit gradient on a 256^3 room; "
+                         "legacy2d: the reference's 2D legacy scheme on an 803x815-node grid")
     return ap.parse_args()
 
 
@@ -237,6 +239,52 @@ def run_plain2d(args):
                          "sample": f"the full {steps}-step run, FP64, {t_cpu:.1f} s"}}), flush=True)
 
 
+def run_legacy2d(args):
+    """The 2D legacy scheme (include/fz_legacy2d.h) on a grid the size of the reference's shipped
+    2D project (2D-solver/input/scene/hybridTST.obj: 4.006 x 4.067 m at h = 5 mm, 803 x 815 nodes)
+    with two synthetic rectangular obstacles of two ADE materials (2 real poles, 1 complex pair),
+    sPML on the y faces, the raised-cosine plane wave, FP32 as the reference; the CPU restatement
+    (oracle, scalar) timed on a bounded number of steps of the same grid."""
+    from fases_b200.legacy2d import Legacy2D, plane_wave_fields, rect_scene
+    from oracle.oracle import legacy2d_run
+    Nx, Ny = 803, 815
+    s = Legacy2D(Nx, Ny, precision=args.precision)
+    P = s.params
+    S, oid = rect_scene(Nx, Ny, P.h, [((1.4, 0.3), (1.5, 2.6), 1), ((2.4, 2.0), (3.2, 2.3), 2)])
+    mats = {"Rinf": np.array([0.83, 0.7]),
+            "A": np.array([[171.9, -343.5], [120.0, 0.0]]), "zeta": np.array([[317.2, 3796.2], [900.0, 0.0]]),
+            "B": np.array([[-21.96], [15.0]]), "C": np.array([[-42.35], [-30.0]]),
+            "alpha": np.array([[39.14], [600.0]]), "beta": np.array([[348.0], [1800.0]])}
+    s.load_geometry(S, oid)
+    s.set_materials(mats["Rinf"], mats["A"], mats["zeta"], mats["B"], mats["C"], mats["alpha"], mats["beta"])
+    p0, u0, v0 = plane_wave_fields(Nx, Ny, P.h, 0.5, P.rho, P.c)
+    s.set_fields(p0, u0, v0)
+    steps = args.steps if args.steps != 300 else 2000
+    s.set_receiver(Nx // 2, Ny // 2, args.warmup + steps)
+    s.run(args.warmup)
+    ms = s.run_timed(steps)
+    ir = s.ir()
+    nodes = (Nx - 6) * (Ny - 6)
+    s.close()
+    nb = 20
+    t = time.perf_counter()
+    legacy2d_run(S, oid, P.h, P.dt, P.rho, P.c, P.eps, P.tol, (P.pml_n, P.pml_s, P.pml_e, P.pml_w), mats, p0, u0, v0,
+                 (Nx // 2, Ny // 2), nb, use_float=args.precision == "fp32")
+    t_cpu = time.perf_counter() - t
+    print(json.dumps({
+        "metric": "Gnode-updates/s, 2D legacy scheme (WENO-JS, sPML, bicubic ADE boundary)",
+        "value": nodes * steps / (ms / 1e3) / 1e9, "unit": "Gnode/s", "n_gpus": 1, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": ms / steps, "higher_is_better": True,
+        "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic (seeded)",
+        "config": {"workload": "2D legacy scheme, 803x815 nodes (4.0 x 4.07 m at h=5 mm), 2 rectangular ADE "
+                               "obstacles, sPML on y faces, raised-cosine plane wave, 1 receiver",
+                   "interior_nodes": nodes, "timer": "CUDA events on the solve's stream",
+                   "l2": "grid fits in L2 (3 buffers x 3 fields x 2.6 MB); no flush, as in a real run"},
+        "finite": bool(np.isfinite(ir).all()),
+        "cpu_baseline": {"value": nodes * nb / t_cpu / 1e9, "unit": "Gnode/s", "cores": 1, "kind": "port",
+                         "sample": f"{nb} steps of the same grid, scalar restatement, {t_cpu:.1f} s"}}), flush=True)
+
+
 def run_precision(args):
     """Config 3: 256^3 room with the config-2 material model; FP32 field state (FP64 ADE state,
     FP64 receiver samples) against all-FP64, per-receiver IR rel-L2 and energy drift."""
@@ -423,7 +471,8 @@ def main():
     args = parse()
     rank, world, local, pg = dist_setup(args.gpus)
     # the reference arm and the side configurations run on rank 0 only; the other ranks leave
-    side = {"plain2d": run_plain2d, "precision": run_precision, "batched": run_batched, "adjoint": run_adjoint}
+    side = {"plain2d": run_plain2d, "precision": run_precision, "batched": run_batched, "adjoint": run_adjoint,
+            "legacy2d": run_legacy2d}
     if args.impl == "reference" or args.config in side:
         if rank == 0:
             if args.impl == "reference":

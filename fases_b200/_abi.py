@@ -79,6 +79,17 @@ class FzGradients(C.Structure):
 PROGRESS_FN = C.CFUNCTYPE(C.c_int, C.c_int64, C.c_int64, C.c_void_p)
 
 
+class FzL2dParams(C.Structure):
+    """fz_l2d_params of include/fz_legacy2d.h."""
+    _fields_ = [
+        ("Nx", C.c_int32), ("Ny", C.c_int32),
+        ("h", C.c_double), ("dt", C.c_double), ("rho", C.c_double), ("c", C.c_double),
+        ("eps", C.c_double), ("tol", C.c_double),
+        ("pml_n", C.c_int32), ("pml_s", C.c_int32), ("pml_e", C.c_int32), ("pml_w", C.c_int32),
+        ("precision", C.c_int32), ("device", C.c_int32),
+    ]
+
+
 class FzError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"{ERROR_NAMES.get(code, code)}: {msg}")
@@ -94,7 +105,7 @@ _ip = C.POINTER(C.c_int32)
 _i64p = C.POINTER(C.c_int64)
 _u8p = C.POINTER(C.c_uint8)
 
-# name -> (restype, argtypes); the exported surface of include/fz.h
+# name -> (restype, argtypes); the exported surface of include/fz.h and include/fz_legacy2d.h
 SIGNATURES = {
     "fz_params_init": (C.c_int, [C.POINTER(FzParams)]),
     "fz_create": (C.c_int, [C.POINTER(FzParams), C.POINTER(_P)]),
@@ -149,6 +160,22 @@ SIGNATURES = {
     "fz_energy_noalloc": (C.c_int, [_P, _P, _P, _P, _i64, C.c_double, C.c_double, _P, _P]),
     "fz_last_error": (C.c_int, [_P, C.c_char_p, C.c_size_t]),
     "fz_global_error": (C.c_int, [C.c_char_p, C.c_size_t]),
+    # include/fz_legacy2d.h
+    "fz_l2d_params_init": (None, [C.POINTER(FzL2dParams)]),
+    "fz_l2d_create": (C.c_int, [C.POINTER(FzL2dParams), C.POINTER(_P)]),
+    "fz_l2d_destroy": (C.c_int, [_P]),
+    "fz_l2d_load_geometry": (C.c_int, [_P, _fp, _u8p]),
+    "fz_l2d_set_materials": (C.c_int, [_P, _i32, _i32, _i32, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
+    "fz_l2d_set_fields": (C.c_int, [_P, _dp, _dp, _dp]),
+    "fz_l2d_set_receiver": (C.c_int, [_P, _i32, _i32, _i64]),
+    "fz_l2d_run": (C.c_int, [_P, _i64]),
+    "fz_l2d_run_timed": (C.c_int, [_P, _i64, _dp]),
+    "fz_l2d_step_count": (C.c_int64, [_P]),
+    "fz_l2d_samples": (C.c_int64, [_P]),
+    "fz_l2d_get_ir": (C.c_int, [_P, _dp, _i64]),
+    "fz_l2d_get_fields": (C.c_int, [_P, _dp, _dp, _dp]),
+    "fz_l2d_band_cells": (C.c_int64, [_P]),
+    "fz_l2d_last_error": (C.c_int, [_P, C.c_char_p, C.c_size_t]),
 }
 
 _lib = None

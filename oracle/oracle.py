@@ -62,6 +62,9 @@ def _load():
         [C.c_double, C.c_int64, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.orc_waveform.argtypes = [C.c_int32, C.c_double, C.c_double, C.c_double, C.c_int64, C.c_double,
                                C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.orc_l2d_run.argtypes = [C.c_int32, C.c_int32, C.c_int32] + [C.c_double] * 6 + \
+        [C.POINTER(C.c_int32), C.POINTER(C.c_float), C.POINTER(C.c_uint8), C.c_int32, C.c_int32, C.c_int32] + \
+        [C.POINTER(C.c_double)] * 10 + [C.c_int32, C.c_int32, C.c_int64] + [C.POINTER(C.c_double)] * 4
     return L
 
 
@@ -190,3 +193,33 @@ def waveform(src_opt, glob_f, f_cutoff, dt, Nt, h, rho):
     lib().orc_waveform(int(src_opt), float(glob_f), float(f_cutoff), float(dt), int(Nt), float(h), float(rho),
                        _dp(us), _dp(pr), C.byref(pk))
     return us, pr, pk.value
+
+
+def legacy2d_run(S, oid, h, dt, rho, c, eps, tol, pml, mats, p0, u0, v0, rec, nsteps, use_float=False):
+    """The reference 2D legacy solver restated (oracle/fz_legacy2d_oracle.cpp): nsteps steps from
+    the fields p0, u0, v0 (Ny x Nx arrays, None = zeros) on the node grid of S / oid; pml = the
+    sPML keys (N, S, E, W). mats holds Rinf (nmat), A, zeta (nmat x K), B, C, alpha, beta
+    (nmat x L). Returns the receiver trace at rec = (i, j) and the final p, u, v."""
+    S = np.ascontiguousarray(S, np.float32)
+    oid = np.ascontiguousarray(oid, np.uint8)
+    Ny, Nx = S.shape
+    pml4 = (C.c_int32 * 4)(*[int(x) for x in pml])
+    Rinf = np.ascontiguousarray(mats["Rinf"], np.float64)
+    nmat = len(Rinf)
+    A = np.ascontiguousarray(mats["A"], np.float64).reshape(nmat, -1)
+    B = np.ascontiguousarray(mats["B"], np.float64).reshape(nmat, -1)
+    K, L = A.shape[1], B.shape[1]
+    arr = [Rinf, A, np.ascontiguousarray(mats["zeta"], np.float64).reshape(nmat, K), B,
+           np.ascontiguousarray(mats["C"], np.float64).reshape(nmat, L),
+           np.ascontiguousarray(mats["alpha"], np.float64).reshape(nmat, L),
+           np.ascontiguousarray(mats["beta"], np.float64).reshape(nmat, L)]
+    f0 = [None if f is None else np.ascontiguousarray(f, np.float64).reshape(Ny, Nx) for f in (p0, u0, v0)]
+    ir = np.zeros(max(nsteps, 1))
+    out = [np.zeros((Ny, Nx)) for _ in range(3)]
+    rc = lib().orc_l2d_run(int(use_float), Nx, Ny, h, dt, rho, c, eps, tol, pml4,
+                           S.ctypes.data_as(C.POINTER(C.c_float)), oid.ctypes.data_as(C.POINTER(C.c_uint8)),
+                           nmat, K, L, *[_dp(a) for a in arr], *[_dp(f) for f in f0], int(rec[0]), int(rec[1]),
+                           nsteps, _dp(ir), *[_dp(o) for o in out])
+    if rc != 0:
+        raise ValueError("orc_l2d_run: bad arguments")
+    return ir[:nsteps], out

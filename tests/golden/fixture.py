@@ -148,3 +148,65 @@ def run_oracle(fx, steps=None):
                rec_cells=fx["rec"], max_steps=steps)
     o.run(steps)
     return o
+
+
+def load_legacy2d(case_dir):
+    """Oracle inputs of a 2D legacy golden project (make_golden_legacy2d.py) plus the reference's
+    receiver trace, in the reference's float conventions (2D-solver/core/main.cu:38-82, 231-295,
+    378-404, 430-499; common/filterABC.h:31-90)."""
+    cfg = read_config(os.path.join(case_dir, "config", "config.txt"))
+    h, t_max = cfg[0], cfg[1]
+    c = np.sqrt(f32(1.4) * f32(287.05) * f32(cfg[3] + f32(273.15)), dtype=f32)
+    rho = f32(1.225)
+    dt = f32(cfg[4] * h / c)
+    Nt = int(t_max / dt) + 1
+    pml = tuple(int(cfg[6 + q]) for q in range(4))  # N, S, E, W
+    hdr = open(os.path.join(case_dir, "output", "pre_header.txt")).read().split()
+    Nx, Ny = int(hdr[0]), int(hdr[1])
+    S = np.fromfile(os.path.join(case_dir, "output", "S.bin"), np.float32, Nx * Ny).reshape(Ny, Nx)
+    oid = np.fromfile(os.path.join(case_dir, "output", "oid.bin"), np.uint8, Nx * Ny).reshape(Ny, Nx)
+    Km, Lm = [int(x) for x in open(os.path.join(case_dir, "config", "poles.txt")).read().split()[:2]]
+    Km, Lm = max(1, Km), max(1, Lm)
+    layers = [n for n in obj_layers(os.path.join(case_dir, "scene.obj")) if "boundary" not in n.lower()]
+    nm = len(layers)
+    mat = {"Rinf": np.zeros(nm), "A": np.zeros((nm, Km)), "zeta": np.zeros((nm, Km)), "B": np.zeros((nm, Lm)),
+           "C": np.zeros((nm, Lm)), "alpha": np.zeros((nm, Lm)), "beta": np.zeros((nm, Lm))}
+    for m, name in enumerate(layers):
+        Rinf, A, zeta, B, C_, al, be = read_fit(os.path.join(case_dir, "input", "fit", name + ".fit"))
+        mat["Rinf"][m] = Rinf
+        for key, vals in (("A", A), ("zeta", zeta), ("B", B), ("C", C_), ("alpha", al), ("beta", be)):
+            mat[key][m, :len(vals)] = vals
+    src_x = None
+    for line in open(os.path.join(case_dir, "input", "src", "src.txt")):
+        if line.strip() and not line.startswith("#"):
+            v = [f32(x) for x in line.split()]
+            if 0 <= int(v[0] / h) < Nx and 0 <= int(v[1] / h) < Ny:
+                src_x = v[0]
+    rec = (Nx // 2, Ny // 2)
+    for line in open(os.path.join(case_dir, "input", "rec", "rec.txt")):
+        if line.strip() and not line.startswith("#"):
+            v = [f32(x) for x in line.split()]
+            ij = (int(v[0] / h), int(v[1] / h))
+            if 0 <= ij[0] < Nx and 0 <= ij[1] < Ny:
+                rec = ij
+    # raised-cosine plane wave (main.cu:455-473; functions.cuh:555-559)
+    ww = f32(0.5) * f32(0.04)
+    xx = (np.arange(Nx, dtype=f32) + f32(0.5)) * h
+    xi = (xx - src_x) / ww
+    g = np.where(np.abs(xi) > f32(1), f32(0), f32(0.5) * (f32(1) + np.cos(f32(np.pi) * xi, dtype=f32))).astype(f32)
+    pI = (f32(0.1) * g).astype(f32)
+    uI = (pI / (rho * c)).astype(f32)
+    p0 = np.tile(pI.astype(np.float64), (Ny, 1))
+    u0 = np.tile(uI.astype(np.float64), (Ny, 1))
+    ir = np.fromfile(os.path.join(case_dir, "output", "IR.bin"), np.float32).astype(np.float64)
+    return {"S": S, "oid": oid, "h": float(h), "dt": float(dt), "c": float(c), "rho": float(rho),
+            "eps": float(f32(1e-7)), "tol": float(f32(3.0) * h), "pml": pml, "materials": mat, "Nt": Nt,
+            "p0": p0, "u0": u0, "rec": rec, "src_x": float(src_x), "ir": ir,
+            "config": os.path.join(case_dir, "config", "config.txt")}
+
+
+def run_legacy2d_oracle(fx, steps=None, use_float=False):
+    from oracle.oracle import legacy2d_run
+    steps = fx["Nt"] if steps is None else steps
+    return legacy2d_run(fx["S"], fx["oid"], fx["h"], fx["dt"], fx["rho"], fx["c"], fx["eps"], fx["tol"], fx["pml"],
+                        fx["materials"], fx["p0"], fx["u0"], None, fx["rec"], steps, use_float=use_float)

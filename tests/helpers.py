@@ -82,3 +82,52 @@ def rel_l2(a, b):
     b = np.asarray(b, float)
     den = np.linalg.norm(b)
     return float(np.linalg.norm(a - b) / den) if den > 0 else float(np.linalg.norm(a - b))
+
+
+def legacy2d_scene(Nx, Ny, h, rects, tol_cells=3.0):
+    """Node-based signed distance S and object ids oid of rectangular obstacles for the 2D legacy
+    scheme, by the conventions of 2D-solver/include/parsing.h:248-299, 404-466: nodes at
+    (i h, j h), S > 0 in the fluid, the outer boundary polygon contributes no distance (FLT_MAX
+    with no obstacle), oid = the nearest obstacle's layer (1-based) at interior nodes with
+    0 <= S <= tol and a nonzero central-difference gradient, 255 elsewhere.
+    rects: [((x0, y0), (x1, y1), layer), ...]."""
+    x = np.arange(Nx) * h
+    y = np.arange(Ny) * h
+    X, Y = np.meshgrid(x, y)
+    S = np.full((Ny, Nx), float(np.finfo(np.float32).max))
+    lay = np.zeros((Ny, Nx), np.int32)
+    for (x0, y0), (x1, y1), layer in rects:
+        cx, cy, hx, hy = (x0 + x1) / 2, (y0 + y1) / 2, (x1 - x0) / 2, (y1 - y0) / 2
+        dx, dy = np.abs(X - cx) - hx, np.abs(Y - cy) - hy
+        d = np.hypot(np.maximum(dx, 0), np.maximum(dy, 0)) + np.minimum(np.maximum(dx, dy), 0)
+        closer = d < S
+        S = np.where(closer, d, S)
+        lay = np.where(closer, layer, lay)
+    S = S.astype(np.float32)
+    hf = np.float32(h)
+    tol = np.float32(tol_cells) * hf
+    oid = np.full((Ny, Nx), 255, np.uint8)
+    for j in range(1, Ny - 1):
+        for i in range(1, Nx - 1):
+            s = S[j, i]
+            if not (s >= 0 and abs(s) <= tol):
+                continue
+            gx = np.float32(0.5) * (S[j, i + 1] - S[j, i - 1]) / hf
+            gy = np.float32(0.5) * (S[j + 1, i] - S[j - 1, i]) / hf
+            if gx * gx + gy * gy <= 1e-24:
+                continue
+            oid[j, i] = lay[j, i]
+    return S, oid
+
+
+def legacy2d_materials(nmat, K, L, seed=0):
+    """Passive-looking ADE coefficients (Rinf, A, zeta, B, C, alpha, beta) for nmat materials."""
+    rng = np.random.default_rng(seed)
+    Rinf = rng.uniform(0.5, 0.9, nmat)
+    zeta = rng.uniform(300.0, 4000.0, (nmat, K))
+    A = rng.uniform(-0.2, 0.2, (nmat, K)) * zeta
+    alpha = rng.uniform(200.0, 2000.0, (nmat, L))
+    beta = rng.uniform(300.0, 3000.0, (nmat, L))
+    B = rng.uniform(-0.1, 0.1, (nmat, L)) * alpha
+    Cc = rng.uniform(-0.1, 0.1, (nmat, L)) * beta
+    return dict(Rinf=Rinf, A=A, zeta=zeta, B=B, C=Cc, alpha=alpha, beta=beta)

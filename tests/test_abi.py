@@ -1,4 +1,5 @@
-"""The C ABI library loads and exports every function include/fz.h declares (no GPU needed)."""
+"""The C ABI library loads and exports every function include/fz.h and include/fz_legacy2d.h declare
+(no GPU needed)."""
 import ctypes
 import os
 import re
@@ -11,9 +12,12 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def _declared():
-    src = open(os.path.join(ROOT, "include", "fz.h")).read()
-    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b(fz_[a-z0-9_]+)\s*\(", src)))
+    names = set()
+    for hdr in ("fz.h", "fz_legacy2d.h"):
+        src = open(os.path.join(ROOT, "include", hdr)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names |= set(re.findall(r"\b(fz_[a-z0-9_]+)\s*\(", src))
+    return sorted(names)
 
 
 def test_every_declared_symbol_is_exported():
@@ -69,3 +73,25 @@ def test_null_handle_calls_are_errors():
     assert L.fz_sync(None, 1) == _abi.FZ_EINVAL
     assert L.fz_energy(None, None) == _abi.FZ_EINVAL
     L.fz_destroy(None)
+
+
+def test_legacy2d_params_and_errors_without_gpu():
+    import torch
+    L = _abi.lib()
+    p = _abi.FzL2dParams()
+    L.fz_l2d_params_init(ctypes.byref(p))
+    # the reference's float set-up at 22 degC, C_CFL 0.2 (2D-solver/core/main.cu:82, 378-392, 591)
+    f32 = np.float32
+    c = np.sqrt(f32(1.4) * f32(287.05) * (f32(22.0) + f32(273.15)), dtype=f32)
+    assert p.c == float(c) and p.h == float(f32(0.005)) and p.dt == float(f32(0.2) * f32(0.005) / c)
+    assert p.tol == float(f32(3.0) * f32(0.005)) and p.eps == float(f32(1e-7))
+    assert (p.pml_n, p.pml_s, p.pml_e, p.pml_w) == (1, 1, 0, 0) and p.Nx == 0
+    h = ctypes.c_void_p()
+    assert L.fz_l2d_create(ctypes.byref(p), ctypes.byref(h)) == _abi.FZ_EINVAL  # grid not set
+    p.Nx, p.Ny = 40, 30
+    if not torch.cuda.is_available():
+        assert L.fz_l2d_create(ctypes.byref(p), ctypes.byref(h)) == _abi.FZ_ENODEV
+        assert not h.value
+    assert L.fz_l2d_run(None, 1) == _abi.FZ_EINVAL
+    assert L.fz_l2d_destroy(None) == _abi.FZ_EINVAL
+    assert L.fz_l2d_step_count(None) == -1
