@@ -46,8 +46,9 @@ CASES = {
 }
 
 
-def write_project(case, dest):
-    c = CASES[case]
+def write_project(case, dest, spec=None):
+    """Writes the reference 2D project of CASES[case] (or of the given spec) into dest."""
+    c = spec if spec is not None else CASES[case]
     os.makedirs(os.path.join(dest, "config"), exist_ok=True)
     for d in ("input/fit", "input/src", "input/rec", "output"):
         os.makedirs(os.path.join(dest, d), exist_ok=True)
@@ -101,6 +102,30 @@ def run_reference(dest, exe):
     path = os.path.join(dest, "output", "pressure.bin")
     if os.path.exists(path):
         os.remove(path)
+
+
+def run_reference_timed(dest, timeout=1800):
+    """Runs the reference 2D solver on dest, stamping each stdout line with time.perf_counter();
+    returns (returncode, [(t, line), ...]). The stamps of "Simulation start" and "Simulation time"
+    bracket its time loop on the wall clock (its own figure is process CPU time, main.cu:888-891)."""
+    import time
+    exe = os.path.join(ROOT, "oracle", "_ref", "phases2D")
+    cmd = [exe, "scene.obj", "config/config.txt", "input/src/src.txt", "input/rec/rec.txt"]
+    if shutil.which("stdbuf"):
+        cmd = ["stdbuf", "-oL"] + cmd  # line-buffered, so each line is stamped when it is printed
+    stamped = []
+    t_end = time.perf_counter() + timeout
+    with subprocess.Popen(cmd, cwd=dest, stdin=subprocess.PIPE, stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
+                          text=True, bufsize=1) as proc:
+        proc.stdin.write("2\n1\n1\n")
+        proc.stdin.close()
+        for line in proc.stdout:
+            stamped.append((time.perf_counter(), line))
+            if time.perf_counter() > t_end:
+                proc.kill()
+                break
+        rc = proc.wait(timeout=60)
+    return rc, stamped
 
 
 def main(out):
