@@ -100,6 +100,144 @@ def rect_scene(Nx, Ny, h, rects, tol_cells=3.0):
     return S, oid
 
 
+def _parse_obj2d(path):
+    """2D OBJ reader of 2D-solver/include/parsing.h:142-237: one polygon per `o`/`g` group (all
+    its `f` lines appended to one vertex loop), vertices (x, y) as float, shifted so the minimum
+    corner is at the origin; the boundary polygon is the first whose name contains "boundary"
+    (any case). Returns (vertices [n, 2] float32, polygons [(name, [indices])], Lx, Ly, boundary)."""
+    verts, polys = [], []
+    cur, have, cur_name = None, False, "unnamed"
+
+    def flush():
+        if have and len(cur[1]) >= 3:
+            polys.append(cur)
+
+    for raw in open(path):
+        line = raw.strip()
+        if not line or line[0] == "#":
+            continue
+        tok = line.split()
+        if tok[0] in ("o", "g"):
+            flush()
+            cur_name = tok[1] if len(tok) >= 2 else "unnamed"
+            cur, have = (cur_name, []), True
+        elif tok[0] == "v":
+            if len(tok) < 3:
+                continue
+            verts.append((f32(float(tok[1])), f32(float(tok[2]))))
+        elif tok[0] == "f":
+            if len(tok) < 4:
+                continue
+            if not have:
+                cur, have = (cur_name, []), True
+            for t in tok[1:]:
+                t = t.split("/", 1)[0]
+                try:
+                    idx = int(t)
+                except ValueError:
+                    idx = 0
+                cur[1].append(idx - 1 if idx > 0 else idx)
+    flush()
+    V = np.array(verts, np.float32).reshape(-1, 2)
+    Lx = Ly = f32(0)
+    if len(V):
+        lo, hi = V.min(axis=0), V.max(axis=0)
+        V = (V - lo).astype(np.float32)
+        Lx, Ly = f32(hi[0] - lo[0]), f32(hi[1] - lo[1])
+    boundary = next((k for k, (nm, _) in enumerate(polys) if "boundary" in nm.lower()), -1)
+    return V, polys, Lx, Ly, boundary
+
+
+def _dist_to_poly(px, py, V, face):
+    """dist_to_poly_edges of parsing.h:104-113 (dist_point_seg 76-86) in float, for arrays of
+    points."""
+    d = np.full(px.shape, np.finfo(np.float32).max, np.float32)
+    m = len(face)
+    for e in range(m):
+        A, B = V[face[e]], V[face[(e + 1) % m]]
+        abx, aby = f32(B[0] - A[0]), f32(B[1] - A[1])
+        apx, apy = px - A[0], py - A[1]
+        den = f32(abx * abx + aby * aby)
+        t = (apx * abx + apy * aby) / den if den > 0 else np.zeros_like(px)
+        t = np.clip(t, f32(0), f32(1)).astype(np.float32)
+        cx, cy = A[0] + t * abx, A[1] + t * aby
+        dx, dy = px - cx, py - cy
+        d = np.minimum(d, np.sqrt(dx * dx + dy * dy))
+    return d
+
+
+def _inside_poly(px, py, V, face):
+    """point_in_poly of parsing.h:88-102 (crossing number) in float, for arrays of points."""
+    inside = np.zeros(px.shape, bool)
+    m = len(face)
+    j = m - 1
+    for i in range(m):
+        A, B = V[face[i]], V[face[j]]
+        cond = (A[1] > py) != (B[1] > py)
+        xint = (B[0] - A[0]) * (py - A[1]) / (f32(B[1] - A[1]) + f32(1e-30)) + A[0]
+        inside ^= cond & (px < xint)
+        j = i
+    return inside
+
+
+def scene_from_obj(path, h, tol_cells=3.0):
+    """The reference 2D solver's scene set-up (2D-solver/include/parsing.h: parse_obj2d,
+    build_sdf, build_oid_dense_cpu; main.cu:82, 104-144) restated in float arithmetic: the node
+    grid Nx = ceil(Lx / h) + 1 by Ny = ceil(Ly / h) + 1, the node-based signed distance S to the
+    non-boundary polygons (negative inside any), and oid = the layer id (boundary 0, other names
+    1.. in first-appearance order) of the polygon nearest to the wall foot point of each node
+    1..N-2 with 0 <= S <= tol and a nonzero gradient, 255 elsewhere. Returns a dict with S, oid,
+    Nx, Ny, Lx, Ly and the layer names (the .fit file of layer m >= 1 is input/fit/<name>.fit)."""
+    V, polys, Lx, Ly, bnd = _parse_obj2d(path)
+    h = f32(h)
+    Nx = int(np.ceil(f32(Lx / h))) + 1
+    Ny = int(np.ceil(f32(Ly / h))) + 1
+    X = np.broadcast_to((np.arange(Nx, dtype=np.float32) * h)[None, :], (Ny, Nx))
+    Y = np.broadcast_to((np.arange(Ny, dtype=np.float32) * h)[:, None], (Ny, Nx))
+    dmin = np.full((Ny, Nx), np.finfo(np.float32).max, np.float32)
+    inside = np.zeros((Ny, Nx), bool)
+    for k, (_, face) in enumerate(polys):
+        if k == bnd:
+            continue
+        dmin = np.minimum(dmin, _dist_to_poly(X, Y, V, face))
+        inside |= _inside_poly(X, Y, V, face)
+    S = np.where(inside, -dmin, dmin).astype(np.float32)
+    # layers (parsing.h:316-379)
+    names = [polys[bnd][0]] if bnd >= 0 else []
+    for k, (nm, _) in enumerate(polys):
+        if k != bnd and nm not in names:
+            names.append(nm)
+    layer = [0 if k == bnd else names.index(nm) for k, (nm, _) in enumerate(polys)]
+    # oid (parsing.h:418-466)
+    tol = f32(tol_cells) * h
+    oid = np.full((Ny, Nx), 255, np.uint8)
+    core = S[1:-1, 1:-1]
+    gx = f32(0.5) * (S[1:-1, 2:] - S[1:-1, :-2]) / h
+    gy = f32(0.5) * (S[2:, 1:-1] - S[:-2, 1:-1]) / h
+    gn2 = gx * gx + gy * gy
+    sel = (core >= 0) & (np.abs(core) <= tol) & ~(gn2 <= f32(1e-24))
+    jj, ii = np.nonzero(sel)
+    if len(jj):
+        s = core[jj, ii]
+        inv = f32(1.0) / np.sqrt(gn2[jj, ii])
+        nx, ny = gx[jj, ii] * inv, gy[jj, ii] * inv
+        Wx = (ii + 1).astype(np.float32) * h - s * nx
+        Wy = (jj + 1).astype(np.float32) * h - s * ny
+        best = np.full(len(jj), np.finfo(np.float32).max, np.float32)
+        pid = np.full(len(jj), -1)
+        for k, (_, face) in enumerate(polys):
+            if k == bnd:
+                continue
+            d = _dist_to_poly(Wx, Wy, V, face)
+            closer = d < best
+            best = np.where(closer, d, best)
+            pid = np.where(closer, k, pid)
+        lid = np.array([layer[k] if k >= 0 else -1 for k in pid])
+        ok = (pid >= 0) & (lid >= 0) & (lid <= 254)
+        oid[jj[ok] + 1, ii[ok] + 1] = lid[ok].astype(np.uint8)
+    return {"S": S, "oid": oid, "Nx": Nx, "Ny": Ny, "Lx": float(Lx), "Ly": float(Ly), "layers": names}
+
+
 class Legacy2D:
     """One 2D legacy solve (include/fz_legacy2d.h) on the given CUDA device."""
 
@@ -204,4 +342,4 @@ class Legacy2D:
             pass
 
 
-__all__ = ["Legacy2D", "plane_wave_fields", "rect_scene", "reference_setup"]
+__all__ = ["Legacy2D", "plane_wave_fields", "rect_scene", "reference_setup", "scene_from_obj"]

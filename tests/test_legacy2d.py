@@ -205,3 +205,59 @@ def test_argument_and_state_errors():
     with pytest.raises(FzError):
         s.load_geometry(np.full((Ny, Nx), np.nan, np.float32), fx["oid"])
     s.close()
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_scene_from_obj_reproduces_the_reference_s_and_oid(case):
+    """The 2D OBJ -> S / oid restatement gives the reference's own output/S.bin and output/oid.bin
+    bit for bit."""
+    from fases_b200.legacy2d import scene_from_obj
+    fx = _fixture(case)
+    sc = scene_from_obj(os.path.join(HERE, "golden", case, "scene.obj"), fx["h"])
+    assert (sc["Ny"], sc["Nx"]) == fx["S"].shape
+    assert np.array_equal(sc["S"], fx["S"])
+    assert np.array_equal(sc["oid"], fx["oid"])
+    assert sc["layers"][0] == "Boundary"
+
+
+def _project_copy(case, dest):
+    import shutil
+    src = os.path.join(HERE, "golden", case)
+    shutil.copytree(src, dest)
+    for f in ("S.bin", "oid.bin", "IR.bin", "header.txt", "pre_header.txt"):
+        p = os.path.join(dest, "output", f)
+        if os.path.exists(p):
+            os.remove(p)
+    return dest
+
+
+def test_phases2d_cli_rejects_a_bad_project(tmp_path, monkeypatch):
+    from fases_b200 import phases2d
+    d = _project_copy("l2d_channel", str(tmp_path / "p"))
+    os.remove(os.path.join(d, "input", "fit", "barrier.fit"))
+    monkeypatch.chdir(d)
+    assert phases2d.main(["scene.obj", "config/config.txt", "input/src/src.txt", "input/rec/rec.txt"]) == 1
+    # S.bin / oid.bin are written before the materials are read, as the reference does
+    assert os.path.getsize(os.path.join("output", "S.bin")) == 122 * 91 * 4
+
+
+@pytest.mark.gpu
+def test_phases2d_cli_reproduces_the_reference_outputs(tmp_path, monkeypatch):
+    from fases_b200 import phases2d
+    fx = _fixture("l2d_channel")
+    d = _project_copy("l2d_channel", str(tmp_path / "p"))
+    monkeypatch.chdir(d)
+    assert phases2d.main(["scene.obj", "config/config.txt", "input/src/src.txt", "input/rec/rec.txt"]) == 0
+    Ny, Nx = fx["S"].shape
+    assert np.array_equal(np.fromfile("output/S.bin", np.float32).reshape(Ny, Nx), fx["S"])
+    assert np.array_equal(np.fromfile("output/oid.bin", np.uint8).reshape(Ny, Nx), fx["oid"])
+    ir = np.fromfile("output/IR.bin", np.float32).astype(np.float64)
+    assert len(ir) == fx["Nt"] and rel_l2(ir, fx["ir"]) < REF_TOL["l2d_channel"]
+    hdr = open("output/header.txt").read().split()
+    anim = int(0.008 * fx["Nt"])
+    assert (int(hdr[0]), int(hdr[1]), int(hdr[2]), int(hdr[6])) == (Nx, Ny, fx["Nt"], anim)
+    frames = int(hdr[5])
+    assert frames == len(range(0, fx["Nt"], anim))
+    P = np.fromfile("output/pressure.bin", np.float32).reshape(frames, Ny, Nx)
+    assert np.isfinite(P).all() and np.abs(P[-1]).max() > 0
+    assert open("output/pre_header.txt").read().split()[:2] == [str(Nx), str(Ny)]
