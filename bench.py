@@ -260,8 +260,9 @@ def run_legacy2d(args):
     p0, u0, v0 = plane_wave_fields(Nx, Ny, P.h, 0.5, P.rho, P.c)
     s.set_fields(p0, u0, v0)
     steps = args.steps if args.steps != 300 else 2000
-    s.set_receiver(Nx // 2, Ny // 2, args.warmup + steps)
-    s.run(args.warmup)
+    warm = max(args.warmup, 64)  # builds the 32-step CUDA graph before the timed region
+    s.set_receiver(Nx // 2, Ny // 2, warm + steps)
+    s.run(warm)
     ms = s.run_timed(steps)
     ir = s.ir()
     nodes = (Nx - 6) * (Ny - 6)
@@ -274,7 +275,7 @@ def run_legacy2d(args):
     print(json.dumps({
         "metric": "Gnode-updates/s, 2D legacy scheme (WENO-JS, sPML, bicubic ADE boundary)",
         "value": nodes * steps / (ms / 1e3) / 1e9, "unit": "Gnode/s", "n_gpus": 1, "steps": steps,
-        "warmup": args.warmup, "ms_per_step": ms / steps, "higher_is_better": True,
+        "warmup": warm, "ms_per_step": ms / steps, "higher_is_better": True,
         "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic (seeded)",
         "config": {"workload": "2D legacy scheme, 803x815 nodes (4.0 x 4.07 m at h=5 mm), 2 rectangular ADE "
                                "obstacles, sPML on y faces, raised-cosine plane wave, 1 receiver",
