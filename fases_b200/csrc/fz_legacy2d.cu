@@ -2,9 +2,13 @@
 //
 // One fused kernel per SSP-RK3 stage replaces the reference's stage kernel, its in-kernel
 // ghost-row copy and its separate immersed-boundary kernel (2D-solver/core/main.cu:816-825):
-//   - a 32 x 8 tile of nodes with a 3-node halo of the stage input (p, u, v) is staged in shared
+//   - a 32 x 6 tile of nodes with a 3-node halo of the stage input (p, u, v) is staged in shared
 //     memory; the WENO-JS stencils and the bicubic boundary probe (always within 3 nodes of the
 //     band node: D = C - h n) read only from there;
+//   - every node's two face values per direction and variable (V+ at i+1/2, V- at i-1/2) are
+//     reconstructed once, by one thread, into shared memory (34 x 6 nodes for x, 32 x 8 for y:
+//     one pass of the 256 threads each), where the reference reconstructs every face twice, once
+//     from each side;
 //   - fluid nodes (S >= h) get the stage update and the multiplicative sPML;
 //   - the nodes of rows 3, Ny-5 and Ny-4 write the ghost rows of p and v of their column;
 //   - band nodes then run their ADE stage and blend the boundary state in, from the same tile;
@@ -29,8 +33,9 @@
 
 namespace l2d {
 
-constexpr int TX = 32, TY = 8, HALO = 3;
+constexpr int TX = 32, TY = 6, HALO = 3, NT = 256;
 constexpr int SX = TX + 2 * HALO, SY = TY + 2 * HALO;
+constexpr int FX = TX + 2, FY = TY + 2;  // face-value columns (x) and rows (y) of a tile
 constexpr uint8_t FLUID = 1, BAND = 2;
 constexpr int32_t ERR_PROBE = 1;
 constexpr int GRAPH_STEPS = 32;  // even: a graph starts and ends with U0 in buffer 0
@@ -110,10 +115,13 @@ __device__ __forceinline__ R cubic(R fm1, R f0, R f1, R f2, R s) {
 }
 
 template <class R, int STAGE>
-__global__ void __launch_bounds__(TX * TY) k_l2d_stage(const Args<R> a) {
+__global__ void __launch_bounds__(NT) k_l2d_stage(const Args<R> a) {
   __shared__ R sm[3][SY][SX];
+  __shared__ R xf[4][TY][FX];  // p+, p-, u+, u- of nodes i0-1 .. i0+TX
+  __shared__ R yf[4][FY][TX];  // p+, p-, v+, v- of nodes j0-1 .. j0+TY
+  const int t = threadIdx.x;
   const int i0 = blockIdx.x * TX + HALO, j0 = blockIdx.y * TY + HALO;
-  for (int q = threadIdx.x + threadIdx.y * TX; q < SX * SY; q += TX * TY) {
+  for (int q = t; q < SX * SY; q += NT) {
     const int x = q % SX, y = q / SX;
     const int gi = i0 - HALO + x, gj = j0 - HALO + y;
     const bool ok = gi < a.Nx && gj < a.Ny;
@@ -122,7 +130,28 @@ __global__ void __launch_bounds__(TX * TY) k_l2d_stage(const Args<R> a) {
     for (int f = 0; f < 3; f++) sm[f][y][x] = ok ? a.in[f][g] : R(0);
   }
   __syncthreads();
-  const int tx = threadIdx.x, ty = threadIdx.y;
+  // face values: WENO_x / WENO_y of functions.cuh:1125-1176, each face once
+  if (t < FX * TY) {
+    const int row = t / FX, col = t % FX;  // node (i0 + col - 1, j0 + row)
+    const R* fp = &sm[0][row + HALO][col + HALO - 1];
+    const R* fu = &sm[1][row + HALO][col + HALO - 1];
+    xf[0][row][col] = weno_js<R, 1>(fp, 1, a.eps);
+    xf[1][row][col] = weno_js<R, 0>(fp, 1, a.eps);
+    xf[2][row][col] = weno_js<R, 1>(fu, 1, a.eps);
+    xf[3][row][col] = weno_js<R, 0>(fu, 1, a.eps);
+  }
+  {
+    const int row = t / TX, col = t % TX;  // node (i0 + col, j0 + row - 1)
+    const R* fp = &sm[0][row + HALO - 1][col + HALO];
+    const R* fv = &sm[2][row + HALO - 1][col + HALO];
+    yf[0][row][col] = weno_js<R, 1>(fp, SX, a.eps);
+    yf[1][row][col] = weno_js<R, 0>(fp, SX, a.eps);
+    yf[2][row][col] = weno_js<R, 1>(fv, SX, a.eps);
+    yf[3][row][col] = weno_js<R, 0>(fv, SX, a.eps);
+  }
+  __syncthreads();
+  if (t >= TX * TY) return;
+  const int tx = t % TX, ty = t / TX;
   const int i = i0 + tx, j = j0 + ty;
   if (i >= a.Nx - 3 || j >= a.Ny - 3) return;
   const size_t C = (size_t)j * a.Nx + i;
@@ -133,26 +162,25 @@ __global__ void __launch_bounds__(TX * TY) k_l2d_stage(const Args<R> a) {
     const R* su = &sm[1][ty + HALO][tx + HALO];
     const R* sv = &sm[2][ty + HALO][tx + HALO];
     const R rho = a.rho, c = a.c;
-    // Godunov fluxes of functions.cuh:199-213 (the 0.5 applied in double as there)
+    // Godunov fluxes of functions.cuh:199-213 (the 0.5 applied in double as there) on the face
+    // values of compute_Vs_x / compute_Vs_y: [0] V+ at i, [1] V- at i+1, [2] V+ at i-1, [3] V- at i
     auto Fp = [&](R pM, R pP, R uM, R uP) { return (R)(0.5 * (double)(rho * c * c * (uP + uM) - c * (pP - pM))); };
     auto Fu = [&](R pM, R pP, R uM, R uP) { return (R)(0.5 * (double)((pP + pM) / rho - c * (uP - uM))); };
     auto Gv = [&](R pM, R pP, R vM, R vP) { return (R)(0.5 * (double)((pM + pP) / rho - c * (vP - vM))); };
     R FpP, FpM, FuP, FuM, GpP, GpM, GvP, GvM;
     {
-      const R p0 = weno_js<R, 1>(sp, 1, a.eps), p1 = weno_js<R, 0>(sp + 1, 1, a.eps);
-      const R p2 = weno_js<R, 1>(sp - 1, 1, a.eps), p3 = weno_js<R, 0>(sp, 1, a.eps);
-      const R u0 = weno_js<R, 1>(su, 1, a.eps), u1 = weno_js<R, 0>(su + 1, 1, a.eps);
-      const R u2 = weno_js<R, 1>(su - 1, 1, a.eps), u3 = weno_js<R, 0>(su, 1, a.eps);
+      const int x = tx + 1;
+      const R p0 = xf[0][ty][x], p1 = xf[1][ty][x + 1], p2 = xf[0][ty][x - 1], p3 = xf[1][ty][x];
+      const R u0 = xf[2][ty][x], u1 = xf[3][ty][x + 1], u2 = xf[2][ty][x - 1], u3 = xf[3][ty][x];
       FpP = Fp(p0, p1, u0, u1);
       FpM = Fp(p2, p3, u2, u3);
       FuP = Fu(p0, p1, u0, u1);
       FuM = Fu(p2, p3, u2, u3);
     }
     {
-      const R p0 = weno_js<R, 1>(sp, SX, a.eps), p1 = weno_js<R, 0>(sp + SX, SX, a.eps);
-      const R p2 = weno_js<R, 1>(sp - SX, SX, a.eps), p3 = weno_js<R, 0>(sp, SX, a.eps);
-      const R v0 = weno_js<R, 1>(sv, SX, a.eps), v1 = weno_js<R, 0>(sv + SX, SX, a.eps);
-      const R v2 = weno_js<R, 1>(sv - SX, SX, a.eps), v3 = weno_js<R, 0>(sv, SX, a.eps);
+      const int y = ty + 1;
+      const R p0 = yf[0][y][tx], p1 = yf[1][y + 1][tx], p2 = yf[0][y - 1][tx], p3 = yf[1][y][tx];
+      const R v0 = yf[2][y][tx], v1 = yf[3][y + 1][tx], v2 = yf[2][y - 1][tx], v3 = yf[3][y][tx];
       GpP = Fp(p0, p1, v0, v1);
       GpM = Fp(p2, p3, v2, v3);
       GvP = Gv(p0, p1, v0, v1);
@@ -463,7 +491,7 @@ l2d::Args<R> args(fz_l2d* h, int stage, int par) {
 
 template <class R>
 cudaError_t enqueue_step(fz_l2d* h, int par) {
-  const dim3 blk(l2d::TX, l2d::TY);
+  const dim3 blk(l2d::NT);
   const dim3 grd((h->prm.Nx - 6 + l2d::TX - 1) / l2d::TX, (h->prm.Ny - 6 + l2d::TY - 1) / l2d::TY);
   l2d::k_l2d_stage<R, 0><<<grd, blk, 0, h->stream>>>(args<R>(h, 0, par));
   l2d::k_l2d_stage<R, 1><<<grd, blk, 0, h->stream>>>(args<R>(h, 1, par));
