@@ -63,7 +63,8 @@ int fz_l2d_destroy(fz_l2d* h);
 
 /* Signed distances S (float, > 0 in the fluid) and object ids oid (1..nmat at band cells, 0 or 255
  * elsewhere) of the node grid: the arrays the reference writes to output/S.bin and output/oid.bin
- * (main.cu:104-134). Builds the band list in raster order (common/filterABC.h:95-108). */
+ * (main.cu:104-134). Builds the band list in raster order (common/filterABC.h:95-108). Like
+ * fz_l2d_set_materials, it resets the solve to zero fields at step 0: set the fields after both. */
 int fz_l2d_load_geometry(fz_l2d* h, const float* S, const uint8_t* oid);
 
 /* ADE coefficients of nmat materials with K real and L complex pole pairs each (zero-padded,
