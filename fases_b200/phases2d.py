@@ -127,9 +127,15 @@ def main(argv=None):
         s.set_receiver(rec[0], rec[1], Nt)
         print(f"\n[OK] Will now start {Nt} iterations.\n\n[OK] Simulation start\n", flush=True)
         frames = 0
+        last = -1
         with open(os.path.join("output", "pressure.bin"), "wb") as fp:
             done = 0
             while done < Nt:
+                if 10 * done // Nt > last:
+                    # the progress bar of print_progress (functions.cuh:1475-1488), every 10 %
+                    last = 10 * done // Nt
+                    filled = 50 * done // Nt
+                    print("\r[%-50s] %3d%%" % ("=" * filled, int(100.0 * done / Nt + 0.5)), end="", flush=True)
                 # a frame after step n (0-based) whenever n % anim_step == 0 (main.cu:838-845)
                 n_next = ((done + anim_step - 1) // anim_step) * anim_step if done else 0
                 chunk = min(n_next - done + 1, Nt - done)
@@ -138,6 +144,7 @@ def main(argv=None):
                 if (done - 1) % anim_step == 0:
                     s.fields()[0].astype(np.float32).tofile(fp)
                     frames += 1
+        print("\r[%-50s] %3d%%" % ("=" * 50, 100), flush=True)
         ir = s.ir().astype(np.float32)
         s.close()
     except L2.FzError as e:
