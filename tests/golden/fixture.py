@@ -126,9 +126,16 @@ def load(case_dir):
         v = [f32(x) for x in line.split()]
         rec.append([int(v[a] / h) + 3 for a in range(3)])
     from oracle.oracle import waveform
-    us, pref, pk = waveform(src_opt, float(glob_f), float(f_cutoff), float(dt), Nt, float(h), float(rho))
-    sval = np.array([f32(s / f32(pk)) for s in spress], np.float64)
-    us32 = us.astype(np.float32).astype(np.float64)
+    if src_opt == 2:
+        # sinusoids: each source scaled by its own rho A_s f / 2 (main3D.cu:1071-1075), no waveform
+        As = 6.0 * float(h) * float(h)
+        sval = np.array([f32(s / f32(float(rho) * As * float(f) / 2.0)) for s, f in zip(spress, sfreq)], np.float64)
+        us32 = np.zeros(2 * Nt + 1)
+        pref, pk = None, None
+    else:
+        us, pref, pk = waveform(src_opt, float(glob_f), float(f_cutoff), float(dt), Nt, float(h), float(rho))
+        sval = np.array([f32(s / f32(pk)) for s in spress], np.float64)
+        us32 = us.astype(np.float32).astype(np.float64)
     nrec = len(rec)
     ir = np.stack([np.fromfile(os.path.join(case_dir, "output", f"IR{r}_0.bin"), np.float32) for r in range(nrec)])
     vel = np.stack([np.fromfile(os.path.join(case_dir, "output", f"VEL{r}_0.bin"), np.float32).reshape(-1, 3)
@@ -136,7 +143,7 @@ def load(case_dir):
     return {"S": S, "oid": oid, "h": float(h), "c": float(c), "rho": float(rho), "dt": float(dt), "Nt": Nt,
             "pml": pml, "materials": mat, "src": np.array(src, np.int32), "sval": sval, "src_opt": src_opt,
             "src_freq": np.array(sfreq, np.float64), "u_s": us32, "rec": np.array(rec, np.int32), "ir": ir,
-            "vel": vel, "p_ref_scaled": pref * float(f32(spress[0] / f32(pk))) if spress else None,
+            "vel": vel, "p_ref_scaled": pref * float(f32(spress[0] / f32(pk))) if spress and pref is not None else None,
             "case_dir": case_dir}
 
 

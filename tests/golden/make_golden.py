@@ -72,6 +72,11 @@ CASES = {
                        pml=(0, 0, 0, 0, 0, 0), obstacles=[], src_opt=1, glob_f=300.0,
                        src=[(0.4, 0.35, 0.3, 80.0)], rec=[(0.7, 0.6, 0.45), (0.2, 0.2, 0.5)], seed=2,
                        open_wall=None),
+    # two sinusoidal sources of their own frequencies (src.txt's fifth column), one open face
+    "box_sine": dict(room=(1.1, 0.9, 0.8), h=0.04, t_max=0.012, f_in=250.0, temp=18.0, cfl=0.5,
+                     pml=(0, 0, 1, 0, 0, 0), obstacles=[((0.6, 0.3, 0.2), (0.8, 0.5, 0.45))], src_opt=2,
+                     glob_f=200.0, src=[(0.3, 0.3, 0.4, 80.0, 180.0), (0.5, 0.6, 0.5, 75.0, 260.0)],
+                     rec=[(0.9, 0.7, 0.5), (0.25, 0.75, 0.3), (0.8, 0.2, 0.6)], seed=3, open_wall=1),
 }
 
 
@@ -113,9 +118,9 @@ def make_project(case, dest, spec=None):
         for v, n in zip(cfg, names):
             f.write("%s\t# %s\n" % (repr(v), n))
     with open(os.path.join(dest, "src.txt"), "w") as f:
-        f.write("# x y z Lp\n")
+        f.write("# x y z Lp [f0]\n")
         for s in c["src"]:
-            f.write("%g %g %g %g\n" % s)
+            f.write(" ".join("%g" % v for v in s) + "\n")
     with open(os.path.join(dest, "rec.txt"), "w") as f:
         f.write("# x y z\n")
         for r in c["rec"]:
