@@ -16,6 +16,7 @@ The reference needs a CUDA GPU; the committed fixtures let the CPU tests check t
 without one.
 """
 import json
+import math
 import os
 import shutil
 import subprocess
@@ -24,25 +25,41 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 
+
+def _ngon(cx, cy, r, n):
+    return [(cx + r * math.cos(2 * math.pi * k / n), cy + r * math.sin(2 * math.pi * k / n)) for k in range(n)]
+
+
 CASES = {
     # a reflecting panel and a wedge of a second material; sPML on both y faces and x-high; fluid
     # up to the ghost rows, where the reference's ghost-row copy races with its stage update
     "l2d_panel": dict(L=(0.8, 0.5), h=0.005, t_max=0.0012, temp=22.0, cfl=0.2, pml=(1, 1, 1, 0),
-                      polys={"panel": [(0.40, 0.15), (0.46, 0.15), (0.46, 0.35), (0.40, 0.35)],
-                             "wedge": [(0.55, 0.05), (0.70, 0.05), (0.62, 0.15)]},
+                      polys=[("panel", [(0.40, 0.15), (0.46, 0.15), (0.46, 0.35), (0.40, 0.35)]),
+                             ("wedge", [(0.55, 0.05), (0.70, 0.05), (0.62, 0.15)])],
                       fits={"panel": (0.82, [(171.9, 317.2), (-343.5, 3796.2)], [(-21.96, -42.35, 39.14, 348.0)]),
                             "wedge": (0.9, [(120.0, 900.0)], [])},
                       poles=(2, 1), src=(0.15, 0.25, 9.0), rec=(0.30, 0.26)),
     # a channel: solid walls over the bottom and top rows (so the reference's racing ghost-row copy
     # only ever copies never-written wall nodes) and a slanted barrier; sPML on x-low only
     "l2d_channel": dict(L=(0.6, 0.45), h=0.005, t_max=0.0016, temp=18.0, cfl=0.25, pml=(0, 0, 0, 1),
-                        polys={"wall": [(0.0, 0.0), (0.6, 0.0), (0.6, 0.035), (0.0, 0.035)],
-                               "barrier": [(0.30, 0.10), (0.33, 0.09), (0.38, 0.30), (0.35, 0.31)],
-                               "ceiling": [(0.0, 0.415), (0.6, 0.415), (0.6, 0.45), (0.0, 0.45)]},
+                        polys=[("wall", [(0.0, 0.0), (0.6, 0.0), (0.6, 0.035), (0.0, 0.035)]),
+                               ("barrier", [(0.30, 0.10), (0.33, 0.09), (0.38, 0.30), (0.35, 0.31)]),
+                               ("ceiling", [(0.0, 0.415), (0.6, 0.415), (0.6, 0.45), (0.0, 0.45)])],
                         fits={"wall": (0.95, [(40.0, 2500.0)], []),
                               "barrier": (0.7, [(250.0, 1500.0)], [(15.0, -30.0, 600.0, 1800.0)]),
                               "ceiling": (0.9, [], [(5.0, 8.0, 900.0, 2600.0)])},
                         poles=(1, 1), src=(0.12, 0.2, 9.0), rec=(0.45, 0.22)),
+    # curved and repeated geometry: a 40-gon pillar, a second polygon of the same layer name (one
+    # material for both), a 'g' group; solid floor and ceiling rows as in l2d_channel; sPML x-high
+    "l2d_pillars": dict(L=(0.7, 0.5), h=0.005, t_max=0.0015, temp=20.0, cfl=0.3, pml=(0, 0, 1, 0),
+                        polys=[("floor", [(0.0, 0.0), (0.7, 0.0), (0.7, 0.03), (0.0, 0.03)]),
+                               ("pillar", _ngon(0.35, 0.25, 0.06, 40)),
+                               ("pillar", [(0.52, 0.10), (0.58, 0.12), (0.55, 0.18)], "g"),
+                               ("roof", [(0.0, 0.47), (0.7, 0.47), (0.7, 0.5), (0.0, 0.5)])],
+                        fits={"floor": (0.95, [(40.0, 2500.0)], []),
+                              "pillar": (0.75, [(200.0, 1200.0), (-80.0, 3000.0)], [(10.0, -20.0, 500.0, 2000.0)]),
+                              "roof": (0.9, [], [(5.0, 8.0, 900.0, 2600.0)])},
+                        poles=(2, 1), src=(0.12, 0.25, 9.0), rec=(0.25, 0.3)),
 }
 
 
@@ -56,8 +73,9 @@ def write_project(case, dest, spec=None):
     lines = ["o Boundary", "v 0.000000 0.000000 0.0", "v %.6f 0.000000 0.0" % Lx, "v %.6f %.6f 0.0" % (Lx, Ly),
              "v 0.000000 %.6f 0.0" % Ly, "f 1 2 3 4"]
     nv = 4
-    for name, pts in c["polys"].items():
-        lines.append("o %s" % name)
+    for poly in c["polys"]:
+        name, pts, kind = poly[0], poly[1], (poly[2] if len(poly) > 2 else "o")
+        lines.append("%s %s" % (kind, name))
         for x, y in pts:
             lines.append("v %.6f %.6f 0.0" % (x, y))
         lines.append("f " + " ".join(str(nv + k + 1) for k in range(len(pts))))

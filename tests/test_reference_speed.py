@@ -111,9 +111,9 @@ def test_legacy2d_beats_the_reference_2d_solver_on_the_same_project(tmp_path):
     steps = int(os.environ.get("FZ_REFSPEED2D_STEPS", "1500"))
     dt = 0.2 * 0.005 / 344.4
     spec = dict(L=(Lx, Ly), h=0.005, t_max=(steps - 0.5) * dt, temp=22.0, cfl=0.2, pml=(0, 0, 1, 0),
-                polys={"floor": [(0.0, 0.0), (Lx, 0.0), (Lx, 0.03), (0.0, 0.03)],
-                       "barrier": [(1.6, 0.8), (1.7, 0.8), (2.2, 3.0), (2.1, 3.0)],
-                       "ceiling": [(0.0, Ly - 0.03), (Lx, Ly - 0.03), (Lx, Ly), (0.0, Ly)]},
+                polys=[("floor", [(0.0, 0.0), (Lx, 0.0), (Lx, 0.03), (0.0, 0.03)]),
+                       ("barrier", [(1.6, 0.8), (1.7, 0.8), (2.2, 3.0), (2.1, 3.0)]),
+                       ("ceiling", [(0.0, Ly - 0.03), (Lx, Ly - 0.03), (Lx, Ly), (0.0, Ly)])],
                 fits={"floor": (0.95, [(40.0, 2500.0)], []),
                       "barrier": (0.8, [(171.9, 317.2), (-343.5, 3796.2)], [(-21.96, -42.35, 39.14, 348.0)]),
                       "ceiling": (0.9, [], [(5.0, 8.0, 900.0, 2600.0)])},
