@@ -18,6 +18,9 @@
 // restatement copies after the whole stage update (the outcome when the copying threads run
 // last), from columns that hold at least one cell with S >= h.
 //
+// The node loops run on OpenMP threads; every node writes only its own outputs and ADE states,
+// so the results do not depend on the thread count.
+//
 // Parity pin: checked against receiver traces of the reference's own 2D solver, built from its
 // sources (oracle/build_ref.sh) and run on a B200 by tests/golden/make_golden_legacy2d.py.
 #include <algorithm>
@@ -129,6 +132,7 @@ struct Legacy2D {
     const T* U = u[in].data();
     const T* V = v[in].data();
     const float hf = (float)h;
+#pragma omp parallel for schedule(static)
     for (int j = 3; j < Ny - 3; j++)
       for (int i = 3; i < Nx - 3; i++) {
         const size_t C = at(i, j);
@@ -254,6 +258,8 @@ struct Legacy2D {
     const T* Po = p[in].data();
     const T* Uo = u[in].data();
     const T* Vo = v[in].data();
+    // every band node owns its ADE states and its own output node
+#pragma omp parallel for schedule(static)
     for (int j = 3; j < Ny - 3; j++)
       for (int i = 3; i < Nx - 3; i++) {
         const size_t Cij = at(i, j);
