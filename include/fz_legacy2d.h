@@ -67,8 +67,9 @@ int fz_l2d_destroy(fz_l2d* h);
  * fz_l2d_set_materials, it resets the solve to zero fields at step 0: set the fields after both. */
 int fz_l2d_load_geometry(fz_l2d* h, const float* S, const uint8_t* oid);
 
-/* ADE coefficients of nmat materials with K real and L complex pole pairs each (zero-padded,
- * material-major: A[m*K + k]; common/filterABC.h:31-90, main.cu:231-295). K or L may be 0. */
+/* ADE coefficients of nmat (1..254) materials with K real and L complex pole pairs each
+ * (zero-padded, material-major: A[m*K + k]; common/filterABC.h:31-90, main.cu:231-295);
+ * 0 <= K, L <= 64. */
 int fz_l2d_set_materials(fz_l2d* h, int nmat, int K, int L, const double* Rinf, const double* A,
                          const double* zeta, const double* B, const double* C, const double* alpha,
                          const double* beta);
