@@ -77,6 +77,13 @@ CASES = {
                      pml=(0, 0, 1, 0, 0, 0), obstacles=[((0.6, 0.3, 0.2), (0.8, 0.5, 0.45))], src_opt=2,
                      glob_f=200.0, src=[(0.3, 0.3, 0.4, 80.0, 180.0), (0.5, 0.6, 0.5, 75.0, 260.0)],
                      rec=[(0.9, 0.7, 0.5), (0.25, 0.75, 0.3), (0.8, 0.2, 0.6)], seed=3, open_wall=1),
+    # walls with 5 real poles and 3 complex pairs (the general-order band path), cPML on the x-hi and
+    # y-lo faces, two obstacles
+    "box_poles": dict(room=(1.2, 1.0, 0.8), h=0.04, t_max=0.012, f_in=250.0, temp=22.0, cfl=0.5,
+                      pml=(0, 0, 1, 0, 1, 0), obstacles=[((0.5, 0.4, 0.3), (0.7, 0.6, 0.5)),
+                                                         ((0.85, 0.15, 0.1), (1.0, 0.3, 0.35))],
+                      src_opt=0, glob_f=100.0, src=[(0.3, 0.5, 0.4, 85.0)],
+                      rec=[(0.9, 0.7, 0.5), (0.2, 0.8, 0.2), (0.6, 0.2, 0.6)], seed=4, open_wall=1, K=5, L=3),
 }
 
 
@@ -99,7 +106,7 @@ def make_project(case, dest, spec=None):
     for nm in wall_names:
         if nm == "BoundingBox":
             continue
-        m = mats.random_passive(rng, dt, f_cut, K=2, L=2)
+        m = mats.random_passive(rng, dt, f_cut, K=c.get("K", 2), L=c.get("L", 2))
         m.write_fit(os.path.join(dest, "input", "fit", nm + ".fit"))
         materials[nm] = m
     for q in range(len(c["obstacles"])):
@@ -107,7 +114,7 @@ def make_project(case, dest, spec=None):
         m.write_fit(os.path.join(dest, "input", "fit", "obstacle%d.fit" % q))
         materials["obstacle%d" % q] = m
     with open(os.path.join(dest, "config", "poles.txt"), "w") as f:
-        f.write("2 2\n")
+        f.write("%d %d\n" % (c.get("K", 2), c.get("L", 2)))
     x0, y0, z0 = [0.5 * L for L in c["room"]]
     cfg = [c["h"], c["t_max"], c["f_in"], c["temp"], c["cfl"], 8, *c["pml"], 0, 0, 0, c["src_opt"], c["glob_f"], 0,
            x0, y0, z0, c.get("frames", 60)]
