@@ -261,3 +261,30 @@ def test_phases2d_cli_reproduces_the_reference_outputs(tmp_path, monkeypatch):
     P = np.fromfile("output/pressure.bin", np.float32).reshape(frames, Ny, Nx)
     assert np.isfinite(P).all() and np.abs(P[-1]).max() > 0
     assert open("output/pre_header.txt").read().split()[:2] == [str(Nx), str(Ny)]
+
+
+def test_scene_from_obj_parsing_rules(tmp_path):
+    """The reference 2D parser's rules (2D-solver/include/parsing.h:142-237): vertices shifted to
+    the origin, `v/vt` face tokens, short `f` lines skipped, polygons with fewer than 3 vertices
+    dropped, the first name containing "boundary" (any case) is the boundary and adds no
+    distance, later polygons of a known name join its layer."""
+    from fases_b200.legacy2d import scene_from_obj
+    obj = tmp_path / "s.obj"
+    obj.write_text("\n".join([
+        "# comment", "o MyBOUNDARYBox",
+        "v -1.0 -2.0 0", "v -0.5 -2.0 0", "v -0.5 -1.7 0", "v -1.0 -1.7 0", "f 1/1 2/2 3/3 4/4",
+        "o block", "v -0.8 -1.9 0", "v -0.7 -1.9 0", "v -0.7 -1.8 0", "v -0.8 -1.8 0", "f 5 6 7 8",
+        "o stub", "f 1 2",
+        "g block", "v -0.65 -1.95 0", "v -0.6 -1.95 0", "v -0.6 -1.9 0", "f 9 10 11",
+        "o other", "v -0.55 -1.8 0", "v -0.52 -1.8 0", "v -0.52 -1.75 0", "f 12 13 14", ""]))
+    sc = scene_from_obj(str(obj), 0.005)
+    assert sc["layers"] == ["MyBOUNDARYBox", "block", "other"]
+    assert abs(sc["Lx"] - 0.5) < 1e-6 and abs(sc["Ly"] - 0.3) < 1e-6
+    assert (sc["Nx"], sc["Ny"]) == (101, 61)
+    S, oid = sc["S"], sc["oid"]
+    # inside the first block (x 0.2..0.3, y 0.1..0.2 after the shift) S < 0; far from all, S > 0
+    assert S[30, 50] < 0 and S[5, 5] > 0
+    # the boundary polygon adds no distance: S at its edge nodes is the distance to the blocks
+    assert S[0, 0] > 0.1
+    layers = set(np.unique(oid)) - {255}
+    assert layers == {1, 2}  # both "block" polygons are layer 1, "other" is layer 2
