@@ -9,6 +9,11 @@ flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl fz|reference] [--room NX NY NZ]
 
+The line states the result's accuracy: the e2e job's receiver traces against the all-FP64 path
+on the same room, source and receivers (`accuracy`, rel-L2 per receiver; --no-accuracy skips that
+run). The timed steps start with both step graphs instantiated (autotune, then graph set-up, then
+the warm-up steps); clocks are sampled through NVML every 5 ms during them.
+
 --impl reference times the CPU restatement of the reference update loop (the reference has no
 CPU solver of its own; its CUDA solver has no library interface) on bounded z-slab samples of
 the same room. Multi-GPU: independent replicas, one per rank (one solve runs on one GPU; a
@@ -41,6 +46,8 @@ def parse():
     ap.add_argument("--room", type=int, nargs=3, default=[500, 400, 200])
     ap.add_argument("--e2e-steps", type=int, default=12000, help="length of the end-to-end job")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the all-FP64 run of the e2e job that gives the IR error of the FP32 result")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--config", default="plain3d", choices=["plain3d", "plain2d", "precision", "batched", "adjoint",
                                                             "legacy2d"],
@@ -65,15 +72,73 @@ def max_over_ranks(rep, x):
     return rep.max(x)
 
 
-class Clocks:
-    """nvidia-smi samples during the timed region."""
+def _nvml_handle(device):
+    """NVML handle of CUDA device `device` (matched by PCI bus id, so CUDA_VISIBLE_DEVICES and
+    NVML's own ordering cannot disagree)."""
+    import pynvml
+    pynvml.nvmlInit()
+    try:
+        from cuda.bindings import runtime as rt
+        err, bus = rt.cudaDeviceGetPCIBusId(32, device)
+        if int(err) == 0:
+            bus = bus.decode() if isinstance(bus, bytes) else str(bus)
+            return pynvml.nvmlDeviceGetHandleByPciBusId(bus.strip("\x00"))
+    except Exception:
+        pass
+    return pynvml.nvmlDeviceGetHandleByIndex(device)
 
-    def __init__(self, gpu):
+
+class Clocks:
+    """SM clock, power and clock-event reasons sampled during the timed region: NVML from a
+    thread every 5 ms (the timed region can be ~50 ms), nvidia-smi at 200 ms when NVML is
+    unavailable."""
+
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
+
+    def __init__(self, gpu, interval_s=0.005):
         self.gpu = gpu
-        self.rows = []
+        self.interval = interval_s
+        self.rows = []  # (sm_mhz, sm_max_mhz, power_w, reasons bitmask)
         self.proc = None
+        self.th = None
+        self.stop = threading.Event()
+        self.source = None
+
+    def _nvml_loop(self, hd):
+        import pynvml
+        mx = pynvml.nvmlDeviceGetMaxClockInfo(hd, pynvml.NVML_CLOCK_SM)
+        while not self.stop.is_set():
+            try:
+                sm = pynvml.nvmlDeviceGetClockInfo(hd, pynvml.NVML_CLOCK_SM)
+                pw = pynvml.nvmlDeviceGetPowerUsage(hd) / 1000.0
+                rs = pynvml.nvmlDeviceGetCurrentClocksEventReasons(hd)
+                self.rows.append((float(sm), float(mx), pw, int(rs)))
+            except Exception:
+                pass
+            self.stop.wait(self.interval)
+
+    def _smi_read(self):
+        for line in self.proc.stdout:
+            r = [x.strip() for x in line.split(",")]
+            try:
+                mask = 0
+                for (nm, bit), v in zip(self.REASONS[:4], r[4:8]):
+                    if v.lower() == "active":
+                        mask |= bit
+                self.rows.append((float(r[0]), float(r[1]), float(r[2]), mask))
+            except (ValueError, IndexError):
+                pass
 
     def __enter__(self):
+        try:
+            hd = _nvml_handle(self.gpu)
+            self.th = threading.Thread(target=self._nvml_loop, args=(hd,), daemon=True)
+            self.th.start()
+            self.source = "nvml, 5 ms"
+            return self
+        except Exception:
+            pass
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -81,37 +146,32 @@ class Clocks:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th = threading.Thread(target=self._smi_read, daemon=True)
             self.th.start()
+            self.source = "nvidia-smi, 200 ms"
         except Exception:
             self.proc = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
-
     def __exit__(self, *a):
+        self.stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        if self.th:
+            self.th.join(timeout=5)
 
     def summary(self):
         if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for r in self.rows:
-            for nm, v in zip(names, r[4:8]):
-                if v.strip().lower() == "active":
-                    reasons.add(nm)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [r[0] for r in self.rows]
+        reasons = sorted({nm for r in self.rows for nm, bit in self.REASONS if r[3] & bit})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(r[1] for r in self.rows),
+                "sm_mhz_min": min(sm), "power_w_max": max(r[2] for r in self.rows), "reasons": reasons,
+                "samples": len(self.rows), "sampler": self.source}
 
 
 def workload(room):
@@ -490,10 +550,11 @@ def main():
     nsteps_total = args.warmup + args.steps
     s = make_solver(b, args.precision, nsteps_total + 31, device=local)
     info = s.info()
-    s.run(args.warmup)
     depth, _ = s.autotune()  # z chunks of the stage kernels, timed on this room
     depth_heuristic = s.kz_chunk()[1]
     zsched = s.z_schedule()
+    s.prepare()  # both step graphs instantiated and uploaded before the warm-up and the timed steps
+    s.run(args.warmup)
     barrier(pg)
     # the timed steps: CUDA graphs of 10 steps, as fz_run issues them
     with Clocks(local) as clk:
@@ -551,6 +612,28 @@ def main():
     t_e2e = time.perf_counter() - t0
     e.close()
     t_e2e = max_over_ranks(pg, t_e2e)
+
+    # accuracy of the e2e job: its receiver traces against the all-FP64 path on the same room,
+    # source and receivers (the FP64 path matches the CPU oracle to 1e-10 on small rooms)
+    accuracy = None
+    if not args.no_accuracy and args.precision == "fp32":
+        prm64 = params(h=b["h"], c=b["c"], rho=b["rho"], dt=b["dt"], pml=b["pml"], pml_cells=20, precision="fp64",
+                       device=local)
+        r64 = Solver(prm64)
+        r64.load_geometry(sc.S, sc.oid)
+        r64.set_materials(m["Rinf"], m["A"], m["zeta"], m["B"], m["Cc"], m["alpha"], m["beta"])
+        r64.set_receivers(b["receivers"], ne)
+        r64.set_fields(p=b["p0"])
+        r64.autotune()
+        t64 = time.perf_counter()
+        r64.run(ne)
+        ir64 = r64.ir()
+        t64 = time.perf_counter() - t64
+        r64.close()
+        errs = [rel_l2(ir[r], ir64[r]) for r in range(ir64.shape[0])]
+        accuracy = {"ir_rel_l2_vs_fp64": errs, "ir_rel_l2_max": max(errs), "steps": ne, "target": 1e-5,
+                    "reference": "all-FP64 GPU path (FZ_FP64) on the same room, source and receivers",
+                    "fp64_seconds": t64}
     h2d = sc.S.nbytes + sc.oid.nbytes + b["p0"].nbytes + sum(np.asarray(v).nbytes for v in m.values())
     d2h = ir.nbytes + vel.nbytes
     e2e = {"value": world * room_cells * ne / t_e2e / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d / ne,
@@ -588,6 +671,7 @@ def main():
             "gpu_launches": launches,
             "cpu_baseline": cpu,
             "finite": finite,
+            "accuracy": accuracy,
         }
         print(json.dumps(line), flush=True)
     pg.close()

@@ -11,6 +11,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 # FZ_BOUNDS_CHECK=1 loads the bounds-checked build (every computed index of the stepping kernels
 # checked against its array; an out-of-range one sets an error bit and is skipped)
 LIB_PATH = os.path.join(HERE, "libfz_checked.so" if os.environ.get("FZ_BOUNDS_CHECK") == "1" else "libfz.so")
+# FZ_WAIT_TEST=1 loads the wait-test build (bounded waits of about a millisecond and the test hook
+# fz_test_skip_plane); only the bounded-wait tests use it
+if os.environ.get("FZ_WAIT_TEST") == "1":
+    LIB_PATH = os.path.join(HERE, "libfz_waittest.so")
 
 FZ_OK = 0
 FZ_EINVAL = -1
@@ -123,6 +127,7 @@ SIGNATURES = {
     "fz_set_fields": (C.c_int, [_P, _dp, _dp, _dp, _dp]),
     "fz_run": (C.c_int, [_P, _i64]),
     "fz_run_timed": (C.c_int, [_P, _i64, _dp]),
+    "fz_prepare": (C.c_int, [_P]),
     "fz_run_progress": (C.c_int, [_P, _i64, _i32, C.c_void_p, C.c_void_p]),
     "fz_sync": (C.c_int, [_P, _i64]),
     "fz_steps_done": (C.c_int, [_P, _i64p]),

@@ -11,6 +11,9 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libfz.so")
 # the same sources with -DFZ_BOUNDS_CHECK: every computed index of the stepping kernels is checked
 CHECKED_LIB = os.path.join(HERE, "libfz_checked.so")
+# the same sources with -DFZ_WAIT_TEST: bounded waits give up after about a millisecond, and a test
+# hook (fz_test_skip_plane) makes the stage kernels skip one tile so that the wait for it runs out
+WAIT_TEST_LIB = os.path.join(HERE, "libfz_waittest.so")
 SOURCES = ["fz_kernels.cu", "fz_adjoint.cu", "fz_geometry.cu", "fz_api.cpp", "fz_project.cpp", "fz_group.cpp",
            "fz_adjoint.cpp", "fz_noalloc.cu", "fz_tune.cpp", "fz_legacy2d.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

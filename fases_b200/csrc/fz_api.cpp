@@ -537,6 +537,7 @@ fz::StageArgs<R> stage_args(fz_handle* h, int stage) {
     a.npc[1] = h->Ny;
     a.npc[2] = (int64_t)h->Nz * h->nb;
   }
+  a.test_skip_plane = h->test_skip_plane;
   return a;
 }
 
@@ -661,28 +662,62 @@ cudaError_t enqueue_step(fz_handle* h) {
   return enqueue_finish<R>(h);
 }
 
+// Captures and instantiates the graph of G steps for the current buffer parity (h->i0), unless it
+// exists. Capture advances the host-side rotation by G (even) steps: back where it started.
+template <class R>
+int ensure_graph(fz_handle* h) {
+  const int G = h->graph_steps;
+  const int par = h->i0;  // buffer assignment repeats every 2 steps
+  if (h->graph[par]) return FZ_OK;
+  cudaGraph_t g = nullptr;
+  FZ_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+  cudaError_t e = cudaSuccess;
+  for (int s = 0; s < G && e == cudaSuccess; s++) e = enqueue_step<R>(h);
+  cudaError_t e2 = cudaStreamEndCapture(h->stream, &g);
+  if (e != cudaSuccess) return cuda_fail(h, e, "capture step");
+  if (e2 != cudaSuccess) return cuda_fail(h, e2, "end capture");
+  e = cudaGraphInstantiate(&h->graph[par], g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return cuda_fail(h, e, "graph instantiate");
+  FZ_CUDA(h, cudaGraphUpload(h->graph[par], h->stream), "graph upload");
+  return FZ_OK;
+}
+
+bool graphs_on(const fz_handle* h) { return !h->profiling && h->graph_steps > 0 && (h->graph_steps % 2) == 0; }
+
+// Finalises the set-up and instantiates the step graphs of both buffer parities without running
+// a step: the parity is flipped on the host only (the field-set and ADE-set roles swap together
+// every step) and flipped back.
+template <class R>
+int prepare_graphs(fz_handle* h) {
+  int rc = finalize<R>(h);
+  if (rc != FZ_OK || !graphs_on(h)) return rc;
+  for (int flip = 0; flip < 2; flip++) {
+    rc = ensure_graph<R>(h);
+    std::swap(h->i0, h->i1);
+    std::swap(h->ph_old, h->ph_cur);
+    if (rc != FZ_OK) {
+      if (flip == 0) {
+        std::swap(h->i0, h->i1);
+        std::swap(h->ph_old, h->ph_cur);
+      }
+      return rc;
+    }
+  }
+  return FZ_OK;
+}
+
 template <class R>
 int run_steps(fz_handle* h, int64_t nsteps) {
   int rc = finalize<R>(h);
   if (rc != FZ_OK) return rc;
   int64_t done = 0;
   const int G = h->graph_steps;
-  if (!h->profiling && G > 0 && (G % 2) == 0) {
+  if (graphs_on(h)) {
     while (nsteps - done >= G) {
-      const int par = h->i0;  // buffer assignment repeats every 2 steps
-      if (!h->graph[par]) {
-        cudaGraph_t g = nullptr;
-        FZ_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-        cudaError_t e = cudaSuccess;
-        for (int s = 0; s < G && e == cudaSuccess; s++) e = enqueue_step<R>(h);
-        cudaError_t e2 = cudaStreamEndCapture(h->stream, &g);
-        if (e != cudaSuccess) return cuda_fail(h, e, "capture step");
-        if (e2 != cudaSuccess) return cuda_fail(h, e2, "end capture");
-        e = cudaGraphInstantiate(&h->graph[par], g, 0);
-        cudaGraphDestroy(g);
-        if (e != cudaSuccess) return cuda_fail(h, e, "graph instantiate");
-        // capture advanced the host-side rotation by G (even) steps: back where it started
-      }
+      const int par = h->i0;
+      rc = ensure_graph<R>(h);
+      if (rc != FZ_OK) return rc;
       FZ_CUDA(h, cudaGraphLaunch(h->graph[par], h->stream), "graph launch");
       done += G;
       h->steps_enqueued += G;
@@ -1153,7 +1188,10 @@ int fz_set_fields(fz_handle* h, const double* p, const double* u, const double* 
   if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
   if (!h->have_geometry) return set_error(h, FZ_ESTATE, "fz_set_fields before fz_load_geometry_raw");
   int rc = fz_sync(h, 0);
-  if (rc != FZ_OK && rc != FZ_ENONFINITE) return rc;  // a blown-up state is what this call replaces
+  // a blown-up state, or one a kernel's bounded wait left invalid, is what this call replaces; a
+  // host-side timeout (work still running) is not
+  if (rc == FZ_ETIMEOUT && cudaStreamQuery(h->stream) != cudaSuccess) return rc;
+  if (rc != FZ_OK && rc != FZ_ENONFINITE && rc != FZ_ETIMEOUT) return rc;
   cudaSetDevice(h->device);
   // a new initial state, as a fresh solver has it: the two other field sets zero (cells the stage
   // kernels skip keep their values from set to set), quiescent ADE and cPML auxiliary states and
@@ -1186,9 +1224,50 @@ int fz_set_fields(fz_handle* h, const double* p, const double* u, const double* 
 namespace {
 struct StateHeader {
   char magic[8];
-  int32_t precision, nb, Nx, Ny, Nz, K, L, nrec, slices;
+  int32_t precision, nb, Nx, Ny, Nz, K, L, nrec, slices, pml_cells;
   int64_t nB, rec_cap, step, sl_cap, psi_bytes[3];
+  uint64_t physics;  // hash of what the update arithmetic depends on beyond the shapes
 };
+
+// FNV-1a (64 bit) over byte ranges.
+struct Fnv {
+  uint64_t h = 1469598103934665603ull;
+  void add(const void* p, size_t n) {
+    const unsigned char* b = (const unsigned char*)p;
+    for (size_t i = 0; i < n; i++) h = (h ^ b[i]) * 1099511628211ull;
+  }
+};
+#define FNV_VAL(f, x) (f).add(&(x), sizeof(x))
+#define FNV_VEC(f, v)                                                   \
+  do {                                                                  \
+    const uint64_t n__ = (uint64_t)(v).size();                          \
+    (f).add(&n__, sizeof(n__));                                         \
+    if (n__) (f).add((v).data(), (size_t)n__ * sizeof((v)[0]));         \
+  } while (0)
+
+// The parameters a saved state was stepped with: grid spacing, speed of sound, density, time step,
+// blending band, cPML faces, thickness and profile, the geometry, every material coefficient and
+// the sources. A state saved under other physics must not continue here.
+uint64_t physics_hash(const fz_handle* h) {
+  Fnv f;
+  const fz_params& p = h->prm;
+  for (double x : {p.h, p.c, p.rho, p.dt, p.tol_cells, p.pml_R0, p.pml_kappa_max, p.pml_alpha_max, p.pml_order})
+    FNV_VAL(f, x);
+  FNV_VAL(f, p.pml);
+  FNV_VAL(f, p.pml_cells);
+  FNV_VAL(f, p.two_d);
+  FNV_VEC(f, h->S_host);
+  FNV_VEC(f, h->oid_host);
+  FNV_VAL(f, h->nMat);
+  for (const std::vector<double>* v : {&h->Rinf, &h->A, &h->zeta, &h->B, &h->C, &h->alpha, &h->beta}) FNV_VEC(f, *v);
+  FNV_VEC(f, h->src_ijk);
+  FNV_VEC(f, h->src_val);
+  FNV_VEC(f, h->src_freq);
+  FNV_VEC(f, h->u_s);
+  FNV_VAL(f, h->src_opt);
+  FNV_VEC(f, h->src_member);
+  return f.h;
+}
 
 struct StatePart {
   void* dev;
@@ -1220,8 +1299,10 @@ std::vector<StatePart> state_parts(fz_handle* h) {
 
 void state_header(fz_handle* h, StateHeader& hd) {
   std::memset(&hd, 0, sizeof(hd));
-  std::memcpy(hd.magic, "FZSTATE1", 8);
+  std::memcpy(hd.magic, "FZSTATE2", 8);
   hd.precision = h->prm.precision;
+  hd.pml_cells = h->prm.pml_cells;
+  hd.physics = physics_hash(h);
   hd.nb = h->nb; hd.Nx = h->Nx; hd.Ny = h->Ny; hd.Nz = h->Nz; hd.K = h->K; hd.L = h->L;
   hd.nrec = h->nrec; hd.slices = h->sl_on ? 1 : 0;
   hd.nB = h->nB; hd.rec_cap = h->rec_cap; hd.sl_cap = h->sl_on ? h->sl_cap : 0;
@@ -1274,9 +1355,16 @@ int fz_state_load(fz_handle* h, const void* buf, int64_t len) {
   std::memcpy(&hd, buf, sizeof(hd));
   const int64_t step = hd.step;
   hd.step = 0;
+  if (std::memcmp(mine.magic, hd.magic, sizeof(hd.magic)) != 0)
+    return set_error(h, FZ_EINVAL, "fz_state_load: not a state of this library version");
+  const uint64_t their_physics = hd.physics;
+  hd.physics = mine.physics;
   if (std::memcmp(&mine, &hd, sizeof(hd)) != 0)
     return set_error(h, FZ_EINVAL, "fz_state_load: the state was saved by a solver of another configuration "
                                    "(grid, precision, batch, band, poles, receivers, cPML or slices differ)");
+  if (their_physics != mine.physics)
+    return set_error(h, FZ_EINVAL, "fz_state_load: the state was saved by a solver with other physics "
+                                   "(h, c, rho, dt, geometry, materials, cPML profile or sources differ)");
   const char* o = (const char*)buf + sizeof(hd);
   for (const auto& p : state_parts(h)) {
     FZ_CUDA(h, cudaMemcpy(p.dev, o, p.bytes, cudaMemcpyHostToDevice), "state H2D");
@@ -1316,6 +1404,26 @@ int fz_run(fz_handle* h, int64_t nsteps) {
   if (nsteps < 0) return set_error(h, FZ_EINVAL, "fz_run: negative step count");
   cudaSetDevice(h->device);
   return h->fp64 ? run_steps<double>(h, nsteps) : run_steps<float>(h, nsteps);
+}
+
+#ifdef FZ_WAIT_TEST
+// Wait-test build only: the stage kernels never issue the tile of plane `plane` of each z chunk
+// (-1: every tile is issued), so their bounded wait for it runs out.
+extern "C" int fz_test_skip_plane(fz_handle* h, int32_t plane) {
+  if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  h->test_skip_plane = plane;
+  free_graphs(h);  // captured launches carry the old value
+  return FZ_OK;
+}
+#endif
+
+int fz_prepare(fz_handle* h) {
+  fz_range nvtx_range("fz_prepare");
+  if (!check_handle(h)) return fzi::set_global_error(FZ_EINVAL, "NULL handle");
+  cudaSetDevice(h->device);
+  int rc = h->fp64 ? prepare_graphs<double>(h) : prepare_graphs<float>(h);
+  if (rc == FZ_OK) rc = fz_sync(h, 0);
+  return rc;
 }
 
 int fz_run_progress(fz_handle* h, int64_t nsteps, int32_t every_percent, fz_progress_fn cb, void* user) {

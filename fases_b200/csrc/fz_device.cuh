@@ -109,6 +109,9 @@ struct StageArgs {
   int64_t nfield;
   int64_t npsi[3];
   int64_t npc[3];
+  // wait-test build only (-DFZ_WAIT_TEST): plane index of each chunk whose tile is never issued,
+  // so that the bounded wait for it runs out (-1: none)
+  int32_t test_skip_plane;
 };
 
 // Kernel error codes written to the handle's device error word.

@@ -118,6 +118,9 @@ struct fz_handle {
   int stage_occ = 1;        // stage-kernel CTAs per SM
   dim3 stage_grid;
 
+  // wait-test build: plane of each z chunk whose tile the stage kernels never issue (-1: none)
+  int test_skip_plane = -1;
+
   // graphs, keyed by buffer parity
   int graph_steps = 10;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};

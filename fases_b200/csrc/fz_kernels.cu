@@ -46,12 +46,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait: gives up after ~2^31 clock cycles (about a second) and reports failure.
+// Bounded wait: gives up after ~2^31 clock cycles (about a second) and reports failure. The
+// wait-test build (-DFZ_WAIT_TEST) gives up after 2^21 cycles (about a millisecond), so that a
+// test can make a wait run out without a long stall.
+#ifdef FZ_WAIT_TEST
+constexpr long long kWaitCycles = 1ll << 21;
+#else
+constexpr long long kWaitCycles = 1ll << 31;
+#endif
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
   while (!mbar_try_wait(bar, parity)) {
-    if (clock64() - t0 > (1ll << 31)) return false;
+    if (clock64() - t0 > kWaitCycles) return false;
   }
   return true;
 }
@@ -62,6 +69,15 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
           "r"(smem_u32(dst)),
       "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
       : "memory");
+}
+
+// Error path of the stage kernel (out of line: it must not cost the stepping loop registers).
+// Waits, bounded, for the tile copies a block still has in flight when the wait for plane it_fail
+// ran out: plane it_fail itself (unless it was never issued: `skipped`) and plane it_fail + 1.
+__device__ __noinline__ void drain_ring(uint64_t* mbar, int it_fail, int nplanes, int skipped) {
+  const int hi = min(it_fail + 1, nplanes - 1);
+  for (int q = it_fail; q <= hi; ++q)
+    if (q != skipped) (void)mbar_wait_bounded(&mbar[q % NBUF], (uint32_t)((q / NBUF) & 1));
 }
 
 // Shared-memory layout of the stage kernel.
@@ -156,7 +172,12 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
     return reinterpret_cast<R*>(ring + buf * L::BUF + 3 * L::FIELD + f * L::OWN);
   };
   auto clsb = [&](int buf) -> uint8_t* { return ring + buf * L::BUF + 3 * L::FIELD + 4 * L::OWN; };
+  // plane `it` of the chunk into ring slot it % NBUF (wait-test build: the plane A.test_skip_plane
+  // is never issued, so the wait for it runs out)
   auto issue = [&](int it) {
+#ifdef FZ_WAIT_TEST
+    if (it == A.test_skip_plane) return;
+#endif
     const int b = it % NBUF;
     const int z = kb + it;
     mbar_expect_tx(&mbar[b], TILE_BYTES);
@@ -171,10 +192,18 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
     }
     tma_load_3d(clsb(b), &M.cls, &mbar[b], tma_x + HX, j0, z);
   };
+  // Error path of a wait that ran out: every thread leaves through the same exit after the
+  // block-wide barrier; thread 0 first waits (bounded, drain_ring) for the copies this block still
+  // has in flight -- plane it_fail (if it was issued) and plane it_fail + 1 (issued one iteration
+  // earlier; plane it_fail + 2 is issued only after the abort check) -- so that no copy lands in
+  // shared memory after the block has gone. If that wait runs out as well, the block exits
+  // anyway and the error word already says that the results are invalid.
+  __shared__ int s_abort;
 
   if (lt == 0) {
     for (int b = 0; b < NBUF; ++b) mbar_init(&mbar[b], 1);
     fence_mbar_init();
+    s_abort = 0;
   }
   __syncthreads();
   if (lt == 0) {
@@ -235,7 +264,7 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
     // ---- plane k tile
     if (!mbar_wait_bounded(&mbar[buf], parity)) {
       atomicOr(A.err, KERR_TMA_TIMEOUT);
-      return;
+      s_abort = 1;  // the block leaves after the barrier below; the tile is not used for stores
     }
     const R* Tp = field(buf, 0);
     const R* Tu = field(buf, 1);
@@ -278,6 +307,14 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
       YCp[(r + 1) * TX + c] = ep;
     }
     __syncthreads();
+    if (s_abort) {
+#ifdef FZ_WAIT_TEST
+      if (lt == 0) drain_ring(mbar, it, nplanes, A.test_skip_plane);
+#else
+      if (lt == 0) drain_ring(mbar, it, nplanes, -1);
+#endif
+      return;
+    }
     // the tile ring slot of plane it-1 is free now: fetch plane it+2 into it
     if (lt == 0 && it + 2 < nplanes) {
       fence_proxy_async();

@@ -67,12 +67,30 @@ __global__ void __launch_bounds__(kThreads) k_energy_finish(const double* partia
   }
 }
 
-// Device address of the scratch array, looked up once per device. In host code the symbol
-// g_energy_partials is only a host-side stand-in: a kernel given it would read the wrong memory,
-// so kernels get the address from cudaGetSymbolAddress, taken with that device current.
+// Device address of the scratch array, looked up once per device and context. In host code the
+// symbol g_energy_partials is only a host-side stand-in: a kernel given it would read the wrong
+// memory, so kernels get the address from cudaGetSymbolAddress, taken with that device current.
+// The address belongs to the module loaded into the device's current context; after
+// cudaDeviceReset (or any other re-creation of the primary context) the module is loaded again,
+// possibly elsewhere, so the cached address is keyed on the context it was taken in.
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 double* g_scratch[kMaxDevices] = {nullptr};
+void* g_scratch_ctx[kMaxDevices] = {nullptr};
+
+// cuCtxGetCurrent, fetched from the driver at run time (no link-time libcuda dependency).
+typedef int (*CtxGetCurrentFn)(void**);
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (CtxGetCurrentFn)p;
+  }
+  return fn;
+}
 
 }  // namespace
 
@@ -92,15 +110,25 @@ extern "C" int fz_energy_noalloc(const float* p, const float* u, const float* v,
   if (dev < 0 || dev >= kMaxDevices) return fzi::set_global_error(FZ_EINVAL, "fz_energy_noalloc: device ordinal too large");
   double* scratch = nullptr;
   {
-    // one-time set-up per device, with that device current (the calling thread's current device)
+    // set-up once per device (and context), with that device current (the calling thread's
+    // current device). Before the runtime's first call on this thread the current context can
+    // still be unset: the lookup then runs, and makes the device's primary context current.
+    CtxGetCurrentFn getctx = ctx_get_current();
+    if (!getctx) return fzi::set_global_error(FZ_ECUDA, "fz_energy_noalloc: cuCtxGetCurrent not available");
+    void* ctx = nullptr;
+    if (getctx(&ctx) != 0) ctx = nullptr;
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch[dev]) {
-      e = cudaGetSymbolAddress((void**)&g_scratch[dev], g_energy_partials);
-      if (e != cudaSuccess) {
-        g_scratch[dev] = nullptr;
+    if (!ctx || !g_scratch[dev] || g_scratch_ctx[dev] != ctx) {
+      g_scratch[dev] = nullptr;
+      g_scratch_ctx[dev] = nullptr;
+      double* a = nullptr;
+      e = cudaGetSymbolAddress((void**)&a, g_energy_partials);
+      if (e != cudaSuccess)
         return fzi::set_global_error(FZ_ECUDA, std::string("fz_energy_noalloc: cudaGetSymbolAddress: ") +
                                                    cudaGetErrorString(e));
-      }
+      if (getctx(&ctx) != 0 || !ctx) return fzi::set_global_error(FZ_ECUDA, "fz_energy_noalloc: no current CUDA context");
+      g_scratch[dev] = a;
+      g_scratch_ctx[dev] = ctx;
     }
     scratch = g_scratch[dev];
   }

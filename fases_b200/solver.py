@@ -191,6 +191,11 @@ class Solver:
         fn = _abi.PROGRESS_FN(_cb)
         self._chk(lib().fz_run_progress(self._h, int(nsteps), int(every_percent), C.cast(fn, C.c_void_p), None))
 
+    def prepare(self):
+        """Finalises the set-up and instantiates the step graphs, so the next run launches
+        without capturing (call after autotune / set_z_schedule, which discard the graphs)."""
+        self._chk(lib().fz_prepare(self._h))
+
     def run_timed(self, nsteps):
         """Runs nsteps and returns their device time in ms (CUDA events on the solver's stream)."""
         ms = C.c_double()

@@ -178,6 +178,13 @@ int fz_run(fz_handle* h, int64_t nsteps);
  * the device time of the nsteps steps. */
 int fz_run_timed(fz_handle* h, int64_t nsteps, double* ms);
 
+/* Finalises the set-up (band list, cPML tables, TMA descriptors) and instantiates the CUDA graphs
+ * fz_run launches (one per buffer parity) without running a step, then waits; the first fz_run
+ * after it launches graphs only. fz_autotune and fz_set_z_schedule discard the graphs, so call it
+ * after them. No counterpart in the reference, which launches every kernel of every step from the
+ * host (main3D.cu:1280-1319). */
+int fz_prepare(fz_handle* h);
+
 /* Progress protocol: fz_run in slices of every_percent % of nsteps (the reference prints "NN%"
  * every 5 %, functions3D.cuh:1431-1439, parsed by common/gui.py:6713), a bounded wait after each
  * slice, then cb(steps_done_in_this_call, nsteps, user) on the calling thread (cb may be NULL).
@@ -192,8 +199,10 @@ int fz_sync(fz_handle* h, int64_t timeout_ms);
  * complete state of a solver -- all three field sets, the ADE states, the cPML psi tiles, the step
  * counter, the receiver traces so far and the animation frames -- copied into a caller-owned host
  * buffer of fz_state_bytes bytes, and back. Loading needs a solver set up the same way (geometry,
- * precision, batch, materials' pole counts, receivers and capacity, cPML faces, slices); the run
- * then continues exactly as the saved one would have (same results bit for bit). */
+ * precision, batch, materials' pole counts, receivers and capacity, cPML faces and thickness,
+ * slices) and with the same physics (h, c, rho, dt, blending band, cPML profile, geometry values,
+ * material coefficients and sources, compared through a hash saved with the state); the run then
+ * continues exactly as the saved one would have (same results bit for bit). */
 int fz_state_bytes(fz_handle* h, int64_t* bytes);
 int fz_state_save(fz_handle* h, void* buf, int64_t cap);
 int fz_state_load(fz_handle* h, const void* buf, int64_t len);
@@ -349,7 +358,8 @@ int fz_global_error(char* buf, size_t cap);
  * waiting. It calls no cudaMalloc/cudaFree: its scratch is a fixed device array of
  * FZ_NOALLOC_MAX_BLOCKS doubles (32 KB) in the library, held by every GPU that loads it until
  * the process exits. n may be at most FZ_NOALLOC_MAX_CELLS; larger n returns FZ_EINVAL.
- * The first call on a device looks up that array's device address (with the device current);
+ * The first call on a device looks up that array's device address (with the device current),
+ * and looks it up again when the device's context has been re-created (cudaDeviceReset);
  * make that first call before any stream capture. All calls share the array: calls that overlap
  * on the GPU race and give wrong results; order them (one stream, or events). */
 #define FZ_NOALLOC_MAX_BLOCKS 4096

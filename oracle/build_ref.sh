@@ -3,10 +3,12 @@
 # for sm_100a, into oracle/_ref/fases3D, and its 2D legacy solver into oracle/_ref/phases2D. It is the checker the CPU restatement is pinned
 # against (tests/golden/make_golden.py runs it on a B200); it is never part of the product.
 # The source tree is read in place; nothing is copied into this repository.
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_ref.sh [REFERENCE_ROOT]
+#   REFERENCE_ROOT defaults to $FZ_REFERENCE_ROOT, else to a checkout named "reference" beside this
+#   repository's directory.
 set -euo pipefail
-REF="${1:-/root/reference}"
 HERE="$(cd "$(dirname "$0")" && pwd)"
+REF="${1:-${FZ_REFERENCE_ROOT:-$(cd "$HERE/../.." && pwd)/reference}}"
 OUT="$HERE/_ref"
 mkdir -p "$OUT"
 if [ ! -f "$REF/3D-solver/core/main3D.cu" ]; then

@@ -173,6 +173,22 @@ def run_reference_timed(dest, timeout=1800):
     return rc, stamped
 
 
+def neutral_paths(dest, prefix=None):
+    """The reference writes the absolute path of the project into output/scene_cache.txt,
+    output/header.txt and its stdout. The fixtures keep the project-relative form ("./scene.obj"),
+    so that no path of the machine that generated them is committed; no test reads those fields
+    (the cache key is checked against the live path, which never matches a copied project)."""
+    prefix = (prefix or dest).rstrip("/") + "/"
+    for rel in (os.path.join("output", "scene_cache.txt"), os.path.join("output", "header.txt"),
+                "reference_stdout.txt"):
+        p = os.path.join(dest, rel)
+        if os.path.exists(p):
+            with open(p) as f:
+                txt = f.read()
+            with open(p, "w") as f:
+                f.write(txt.replace(prefix, "./"))
+
+
 def prune(dest):
     """Keep only what the tests read (inputs + FVM outputs)."""
     out = os.path.join(dest, "output")
@@ -204,5 +220,6 @@ if __name__ == "__main__":
         rc = run_reference(dest)
         print(case, "reference exit code", rc)
         prune(dest)
+        neutral_paths(dest)
         rc_all |= rc
     sys.exit(rc_all)

@@ -1,6 +1,7 @@
 """Checkpoint / resume (fz_state_save / fz_state_load): a solver that loads a state saved after 30
 steps and runs 25 more gives, bit for bit, the receiver traces (all 55 samples) and fields of the
-solver that ran 55 steps straight; a solver of another configuration refuses the state."""
+solver that ran 55 steps straight; a solver of another configuration, or with other physics (time
+step, materials, cPML thickness), refuses the state."""
 import numpy as np
 import pytest
 
@@ -46,3 +47,16 @@ def test_resume_continues_bit_for_bit(precision, tmp_path):
         c.load_state(state)
     assert ei.value.code == _abi.FZ_EINVAL
     c.close()
+
+    # so do solvers with the same shapes but other physics: another time step, another material
+    # coefficient, another cPML thickness
+    mats = {k: np.array(v, dtype=np.float64, copy=True) for k, v in cfg["materials"].items()}
+    mats["A"] = mats["A"] * 1.01
+    for other, what in ((dict(cfg, dt=cfg["dt"] * 0.9), ("physics",)), (dict(cfg, materials=mats), ("physics",)),
+                        (dict(cfg, pml_cells=cfg["pml_cells"] - 1), ("configuration", "wrong size"))):
+        c = run_gpu(other, precision, run=False)
+        with pytest.raises(FzError) as ei:
+            c.load_state(state)
+        assert ei.value.code == _abi.FZ_EINVAL
+        assert any(w in str(ei.value) for w in what), str(ei.value)
+        c.close()

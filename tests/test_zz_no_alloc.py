@@ -54,3 +54,30 @@ def test_noalloc_energy_matches_fz_energy_on_two_calls():
         results.append(e)
     assert results[0] != results[1]
     s.close()
+
+
+@pytest.mark.gpu
+def test_noalloc_energy_ragged_many_blocks_and_empty():
+    """Caller-owned arrays of a size that needs several blocks with a partial last one (and of
+    size zero, where *out must become 0), against an FP64 torch sum of the same formula."""
+    import torch
+
+    L = _abi.lib()
+    stream = torch.cuda.current_stream()
+    rho, c = 1.2, 343.0
+    g = torch.Generator(device="cuda").manual_seed(5)
+    for n in (3 * 16384 + 5, 1, 0):
+        fields = [torch.randn(max(n, 1), generator=g, device="cuda", dtype=torch.float32)[:n] for _ in range(4)]
+        out = torch.full((1,), -1.0, dtype=torch.float64, device="cuda")
+        ptrs = [t.data_ptr() for t in fields]  # views of one-element storage when n = 0: never NULL
+        assert all(ptrs)
+        rc = L.fz_energy_noalloc(*ptrs, n, rho, c, out.data_ptr(), stream.cuda_stream)
+        assert rc == _abi.FZ_OK, _abi.last_error()
+        torch.cuda.synchronize()
+        p, u, v, w = (t.double() for t in fields)
+        want = 0.5 * float((p * p / (rho * c * c) + rho * (u * u + v * v + w * w)).sum())
+        got = out.item()
+        if n == 0:
+            assert got == 0.0
+        else:
+            assert abs(got - want) <= 1e-12 * abs(want), (n, got, want)
