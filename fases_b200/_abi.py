@@ -15,6 +15,9 @@ LIB_PATH = os.path.join(HERE, "libfz_checked.so" if os.environ.get("FZ_BOUNDS_CH
 # fz_test_skip_plane); only the bounded-wait tests use it
 if os.environ.get("FZ_WAIT_TEST") == "1":
     LIB_PATH = os.path.join(HERE, "libfz_waittest.so")
+# FZ_LIB=<path> loads another build of the same sources (a kernel variant being measured)
+if os.environ.get("FZ_LIB"):
+    LIB_PATH = os.path.abspath(os.environ["FZ_LIB"])
 
 FZ_OK = 0
 FZ_EINVAL = -1

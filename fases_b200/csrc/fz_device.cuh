@@ -15,7 +15,10 @@ constexpr int GHOST = 3;
 
 // Stage-kernel tile: 32 x 16 cells per CTA, one thread per (i, j) column, streaming along z.
 constexpr int TX = 32;
-constexpr int TY = 16;
+#ifndef FZ_TY
+#define FZ_TY 16
+#endif
+constexpr int TY = FZ_TY;
 constexpr int HX = 4;  // x halo held in shared memory (3 needed; 4 keeps rows 16-byte aligned)
 constexpr int HY = 3;  // y halo
 constexpr int PW = TX + 2 * HX;  // 40 tile columns

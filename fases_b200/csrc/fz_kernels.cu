@@ -28,6 +28,9 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
 __device__ __forceinline__ void fence_mbar_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
@@ -131,7 +134,7 @@ __device__ __forceinline__ R source_sum(const StageArgs<R>& A, int64_t g) {
 }
 
 #ifndef FZ_STAGE_MINBLOCKS_F32
-#define FZ_STAGE_MINBLOCKS_F32 2  // two 16-warp CTAs per SM in FP32 (64 registers, no spills)
+#define FZ_STAGE_MINBLOCKS_F32 (1024 / NTHREADS)  // 32 warps per SM in FP32 (64 registers, no spills)
 #endif
 // DIM2: planar solve (one updated z-plane, no z fluxes): the 3D scheme restricted to 2D.
 template <class R, int STAGE, bool DIM2>
@@ -200,8 +203,15 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
   // anyway and the error word already says that the results are invalid.
   __shared__ int s_abort;
 
+#if defined(FZ_V_SPLITBAR)
+  __shared__ __align__(8) uint64_t cbar[2];  // centre buffers: one arrival per warp
+#endif
   if (lt == 0) {
     for (int b = 0; b < NBUF; ++b) mbar_init(&mbar[b], 1);
+#if defined(FZ_V_SPLITBAR)
+    mbar_init(&cbar[0], NTHREADS / 32);
+    mbar_init(&cbar[1], NTHREADS / 32);
+#endif
     fence_mbar_init();
     s_abort = 0;
   }
@@ -255,10 +265,12 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
     P vmC = zero, Fz_hi = zero;
     if (!DIM2) {
       if (it + 1 < nplanes) qe_next = ld_pw(k + 4);
+#if !defined(FZ_V_ZAFTER) && !defined(FZ_V_SPLITBAR)
       // ---- z: centre k+1 -> flux through face k+1/2
       P vpC;
       weno_center<R>(qa, qb, qc, qd, qe, vmC, vpC);
       Fz_hi = godunov<R>(zm, vpC, kA, kC);
+#endif
     }
 
     // ---- plane k tile
@@ -270,6 +282,13 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
     const R* Tu = field(buf, 1);
     const R* Tv = field(buf, 2);
     const uint8_t cls = clsb(buf)[lt];
+#if defined(FZ_V_ZAFTER)
+    if (!DIM2) {
+      P vpC;
+      weno_center<R>(qa, qb, qc, qd, qe, vmC, vpC);
+      Fz_hi = godunov<R>(zm, vpC, kA, kC);
+    }
+#endif
 
     // ---- x and y centres of this thread's cell
     P xm, xp, ym, yp;
@@ -286,7 +305,7 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
     }
     // ---- halo centres: warp 0 the x edges (i0-1, i0+TX) of all 16 rows, warps 1-2 the y edge
     //      rows (j0-1, j0+TY)
-    if (lt < TX) {
+    if (lt < 2 * TY) {
       const int r = lt >> 1, side = lt & 1;
       const int c0 = (r + HY) * PW + (side ? (HX + TX) : (HX - 1));
       P em, ep;
@@ -295,8 +314,8 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
       const int slot = r * (TX + 2) + (side ? TX + 1 : 0);
       XCm[slot] = em;
       XCp[slot] = ep;
-    } else if (lt < 3 * TX) {
-      const int e = lt - TX;
+    } else if (lt >= 32 && lt < 32 + 2 * TX) {
+      const int e = lt - 32;
       const int r = (e < TX) ? -1 : TY;
       const int c = e & (TX - 1);
       const int c0 = (r + HY) * PW + (c + HX);
@@ -306,7 +325,23 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
       YCm[(r + 1) * TX + c] = em;
       YCp[(r + 1) * TX + c] = ep;
     }
+#if defined(FZ_V_SPLITBAR)
+    // split barrier: each warp arrives once its centres are in shared memory, computes the z centre
+    // (registers only) and only then waits for the other warps' centres
+    __syncwarp();
+    if ((lt & 31) == 0) mbar_arrive(&cbar[it & 1]);
+    if (!DIM2) {
+      P vpC;
+      weno_center<R>(qa, qb, qc, qd, qe, vmC, vpC);
+      Fz_hi = godunov<R>(zm, vpC, kA, kC);
+    }
+    if (!mbar_wait_bounded(&cbar[it & 1], (uint32_t)((it >> 1) & 1))) {
+      atomicOr(A.err, KERR_TMA_TIMEOUT);
+      return;
+    }
+#else
     __syncthreads();
+#endif
     if (s_abort) {
 #ifdef FZ_WAIT_TEST
       if (lt == 0) drain_ring(mbar, it, nplanes, A.test_skip_plane);

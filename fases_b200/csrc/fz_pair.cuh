@@ -76,10 +76,20 @@ __device__ __forceinline__ void weno_core(typename Pair<R>::T a, typename Pair<R
   const P B1 = pfma(D1, D1, pfma(pmul(E1, k313), E1, eps));
   const P B2 = pfma(D2, D2, pfma(pmul(E2, k313), E2, eps));
   const P tau = pabs(psub(B0, B2));
+#if defined(FZ_V_FEWRCP)
+  // w_r ~ d_r (1 + tau/B_r) = d_r (B_r + tau) / B_r: the normalised weights do not change when
+  // every (1 + tau/B_r) is scaled by B0 B1 B2, which leaves (B_r + tau) times the other two B's
+  const P B01 = pmul(B0, B1), B02 = pmul(B0, B2), B12 = pmul(B1, B2);
+  const P B012 = pmul(B12, B0);
+  const P q0w = pfma(tau, B12, B012);
+  const P q1w = pfma(tau, B02, B012);
+  const P q2w = pfma(tau, B01, B012);
+#else
   const P one = psplat<R>(R(1));
   const P q0w = pfma(tau, prcp(B0), one);
   const P q1w = pfma(tau, prcp(B1), one);
   const P q2w = pfma(tau, prcp(B2), one);
+#endif
   // normalisers: V- uses d = (3/10, 3/5, 1/10), V+ the mirrored (1/10, 3/5, 3/10)
   const P t1 = pmul(q1w, psplat<R>(R(0.6)));
   const P Sm = pfma(q0w, psplat<R>(R(0.3)), pfma(q2w, psplat<R>(R(0.1)), t1));
