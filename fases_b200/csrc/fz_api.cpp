@@ -66,6 +66,7 @@ int64_t ref_index(const fz_handle* h, int i, int j, int k) {
 }
 
 void free_graphs(fz_handle* h) {
+  h->launch_gen++;
   for (auto& g : h->graph) {
     if (g) cudaGraphExecDestroy(g);
     g = nullptr;
@@ -862,6 +863,7 @@ cudaError_t enqueue_stage(fz_handle* h, int st) {
   return h->fp64 ? ::enqueue_stage<double>(h, st) : ::enqueue_stage<float>(h, st);
 }
 int bind_field_set(fz_handle* h, int set, void* const* f) {
+  h->launch_gen++;
   const CUtensorMapDataType t = h->fp64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
   for (int q = 0; q < 4; q++) h->U[set][q] = f[q];
   for (int q = 0; q < 3; q++) {
@@ -897,6 +899,7 @@ int set_z_sizes(fz_handle* h, const std::vector<int>& sizes) {
   h->kz_chunk = *std::max_element(sizes.begin(), sizes.end());
   h->stage_grid = grid;
   if (same) return FZ_OK;
+  h->launch_gen++;
   for (auto& g : h->graph)
     if (g) {
       cudaGraphExecDestroy(g);
@@ -950,6 +953,50 @@ std::vector<int> guided_z_sizes(fz_handle* h, int depth) {
   return sizes;
 }
 cudaError_t enqueue_finish(fz_handle* h) { return h->fp64 ? ::enqueue_finish<double>(h) : ::enqueue_finish<float>(h); }
+
+template <class R>
+void stage_desc(fz_handle* h, int st, fz::StageArgs<R>* a, fz::StageMaps* m) {
+  const int in_set = (st == 0) ? h->i0 : (st == 1) ? h->i1 : h->i2;
+  m->p = h->halo_map[in_set][0];
+  m->u = h->halo_map[in_set][1];
+  m->v = h->halo_map[in_set][2];
+  m->bp = h->own_map[h->i0][0];
+  m->bu = h->own_map[h->i0][1];
+  m->bv = h->own_map[h->i0][2];
+  m->bw = h->own_map[h->i0][3];
+  m->cls = h->cls_map;
+  *a = stage_args<R>(h, st);
+}
+template <class R>
+void band_desc(fz_handle* h, int st, fz::BandArgs<R>* b) {
+  *b = band_args<R>(h, st);
+}
+template <class R>
+void rec_desc(fz_handle* h, fz::RecArgs<R>* r) {
+  R* const* u1 = (R* const*)h->U[h->i1];
+  r->p = u1[0];
+  r->u = u1[1];
+  r->v = u1[2];
+  r->w = u1[3];
+  r->rcell = h->d_rec_cell;
+  r->nrec = h->nrec * h->nb;
+  r->ir = h->d_ir;
+  r->vel = h->d_vel;
+  r->cap = h->rec_cap;
+  r->step = h->d_step;
+  r->err = h->d_err;
+  r->nfield = h->ncell_dev * h->nb;
+}
+void rotate(fz_handle* h) {
+  std::swap(h->i0, h->i1);
+  std::swap(h->ph_old, h->ph_cur);
+}
+template void stage_desc<float>(fz_handle*, int, fz::StageArgs<float>*, fz::StageMaps*);
+template void stage_desc<double>(fz_handle*, int, fz::StageArgs<double>*, fz::StageMaps*);
+template void band_desc<float>(fz_handle*, int, fz::BandArgs<float>*);
+template void band_desc<double>(fz_handle*, int, fz::BandArgs<double>*);
+template void rec_desc<float>(fz_handle*, fz::RecArgs<float>*);
+template void rec_desc<double>(fz_handle*, fz::RecArgs<double>*);
 }  // namespace fzi
 
 // ==========================================================================================

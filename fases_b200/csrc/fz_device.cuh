@@ -189,4 +189,40 @@ struct BandArgs {
   int64_t nfield;  // elements of one field array (bounds-checked build)
 };
 
+// Receiver gather of one room (the arguments of its receiver kernel).
+template <class R>
+struct RecArgs {
+  const R* p;
+  const R* u;
+  const R* v;
+  const R* w;
+  const int64_t* rcell;
+  int32_t nrec;
+  double* ir;
+  double* vel;
+  int64_t cap;
+  int64_t* step;
+  int32_t* err;
+  int64_t nfield;
+};
+
+// Groups of rooms stepped by one launch per kernel kind (see k_stage_group).
+constexpr int FZ_MAX_GROUP = 64;
+
+template <class R>
+struct GroupStageArgs {
+  const StageArgs<R>* args;  // [n] in device memory: each member's stage arguments
+  const StageMaps* maps;     // [n] in device memory (64-byte aligned): each member's TMA descriptors
+  int32_t n;
+  int32_t cta_start[FZ_MAX_GROUP + 1];  // first CTA of member m in the group grid; [n] = total
+  int32_t gx[FZ_MAX_GROUP], gy[FZ_MAX_GROUP];  // member m's tiles along x and y
+};
+
+template <class R>
+struct GroupBandArgs {
+  const BandArgs<R>* args;  // [n] in device memory
+  int32_t n;
+  int32_t blk_start[FZ_MAX_GROUP + 1];  // first 256-thread block of member m; [n] = total
+};
+
 }  // namespace fz

@@ -1,6 +1,10 @@
-// fz_group.cpp -- several solver handles (rooms) advanced together, one CUDA graph per run of
-// graph_steps steps whose parallel branches are the members. Small rooms leave most of the GPU
-// idle when stepped one after another; as branches of one graph their kernels share the SMs.
+// fz_group.cpp -- several solver handles (rooms) advanced together. Small rooms leave most of the
+// GPU idle when stepped one after another. Rooms of one precision (3D, without animation slices,
+// up to FZ_MAX_GROUP) are stepped by one launch per kernel kind: each stage kernel, band kernel
+// and receiver gather covers every member, its CTAs laid end to end (fz_kernels.cu,
+// k_stage_group), from argument tables in device memory; runs of graph_steps steps are CUDA
+// graphs of these launches. Other groups run each member's own launches as parallel branches of
+// one graph per run.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -11,6 +15,22 @@
 #include <vector>
 
 #include "fz_internal.h"
+#include "fz_kernels.h"
+
+// Launch arguments of every member for one buffer-parity key, laid side by side in one device
+// buffer: [3 stages][n] stage arguments, [3][n] TMA descriptor sets, [3][n] band arguments, [n]
+// receiver arguments.
+struct FlatTables {
+  void* dev = nullptr;
+  std::vector<char> host;
+  size_t off_maps = 0, off_band = 0, off_rec = 0, stage_bytes = 0, band_bytes = 0, rec_bytes = 0;
+  int ctas = 0;             // stage CTAs of all members
+  int band_blocks = 0;      // band blocks of all members
+  int band_fit = 0;         // pole-count form of the band kernel (2, 4 or 0 = general)
+  std::vector<char> gstage; // GroupStageArgs<R> host copy per stage (kernel parameters)
+  std::vector<char> gband;  // GroupBandArgs<R> host copy per stage
+  std::vector<uint64_t> gen;  // the members' launch_gen when the tables were built
+};
 
 struct fz_group {
   std::vector<fz_handle*> m;
@@ -21,6 +41,11 @@ struct fz_group {
   std::vector<cudaEvent_t> join;
   // keyed by the members' buffer parities (the field-set rotation repeats every 2 steps)
   std::map<std::vector<int>, cudaGraphExec_t> graphs;
+  // one launch per kernel kind for all members (3D rooms of one precision, no animation slices,
+  // at most FZ_MAX_GROUP); otherwise each member's own launches are branches of the graph
+  bool flat = false;
+  bool fp64 = false;
+  std::map<std::vector<int>, FlatTables> tables;
 };
 
 namespace {
@@ -49,11 +74,156 @@ int order_after(fz_group* g, bool members_wait_for_group) {
   return FZ_OK;
 }
 
+std::vector<int> parity_key(const fz_group* g) {
+  std::vector<int> key;
+  for (const fz_handle* h : g->m) key.push_back(h->i0);
+  return key;
+}
+
+void free_tables(fz_group* g) {
+  for (auto& kv : g->tables)
+    if (kv.second.dev) cudaFree(kv.second.dev);
+  g->tables.clear();
+}
+
+void drop_graphs(fz_group* g) {
+  for (auto& kv : g->graphs) cudaGraphExecDestroy(kv.second);
+  g->graphs.clear();
+}
+
+// Builds (or checks) the flat tables of the members' current roles. When a member's launches
+// changed since the tables were uploaded (a new launch shape, reallocated or rebound arrays: its
+// launch_gen moved), the tables are built again, and every captured graph goes, since graphs hold
+// the old kernel parameters.
+template <class R>
+int flat_tables(fz_group* g, const std::vector<int>& key) {
+  const int n = (int)g->m.size();
+  std::vector<uint64_t> gen;
+  for (const fz_handle* h : g->m) gen.push_back(h->launch_gen);
+  auto it = g->tables.find(key);
+  if (it != g->tables.end() && it->second.gen == gen) return FZ_OK;  // unchanged
+  FlatTables t;
+  t.gen = gen;
+  t.stage_bytes = sizeof(fz::StageArgs<R>) * n;
+  t.off_maps = ((3 * t.stage_bytes + 127) / 128) * 128;
+  const size_t maps_bytes = sizeof(fz::StageMaps) * n;
+  t.off_band = t.off_maps + ((3 * maps_bytes + 127) / 128) * 128;
+  t.band_bytes = sizeof(fz::BandArgs<R>) * n;
+  t.off_rec = t.off_band + ((3 * t.band_bytes + 127) / 128) * 128;
+  t.rec_bytes = sizeof(fz::RecArgs<R>) * n;
+  t.host.assign(t.off_rec + t.rec_bytes, 0);
+  std::vector<fz::GroupStageArgs<R>> gs(3);
+  std::vector<fz::GroupBandArgs<R>> gb(3);
+  int ctas = 0, blocks = 0, kmax = 0, lmax = 0;
+  for (int q = 0; q < n; q++) {
+    fz_handle* h = g->m[(size_t)q];
+    for (int st = 0; st < 3; st++) {
+      fz::StageArgs<R>* a = reinterpret_cast<fz::StageArgs<R>*>(t.host.data() + st * t.stage_bytes) + q;
+      fz::StageMaps* mp = reinterpret_cast<fz::StageMaps*>(t.host.data() + t.off_maps + st * maps_bytes) + q;
+      fzi::stage_desc<R>(h, st, a, mp);
+      fzi::band_desc<R>(h, st, reinterpret_cast<fz::BandArgs<R>*>(t.host.data() + t.off_band + st * t.band_bytes) + q);
+    }
+    fzi::rec_desc<R>(h, reinterpret_cast<fz::RecArgs<R>*>(t.host.data() + t.off_rec) + q);
+    const dim3 gr = h->stage_grid;
+    for (int st = 0; st < 3; st++) {
+      gs[st].cta_start[q] = ctas;
+      gs[st].gx[q] = (int)gr.x;
+      gs[st].gy[q] = (int)gr.y;
+      gb[st].blk_start[q] = blocks;
+    }
+    ctas += (int)(gr.x * gr.y * gr.z);
+    blocks += (int)((h->nB + 255) / 256);
+    if (h->nB > 0) {
+      kmax = std::max(kmax, h->K);
+      lmax = std::max(lmax, h->L);
+    }
+  }
+  for (int st = 0; st < 3; st++) {
+    gs[st].n = n;
+    gs[st].cta_start[n] = ctas;
+    gb[st].n = n;
+    gb[st].blk_start[n] = blocks;
+  }
+  t.ctas = ctas;
+  t.band_blocks = blocks;
+  t.band_fit = (kmax <= 2 && lmax <= 2) ? 2 : (kmax <= 4 && lmax <= 4) ? 4 : 0;
+  drop_graphs(g);
+  if (it != g->tables.end()) {
+    // launches still queued may read the old tables: a new buffer, the old one freed when idle
+    // (a new address also keeps TMA descriptors cached for the old contents out of the way)
+    FZ_GCUDA(g, cudaStreamSynchronize(g->stream), "group tables");
+    cudaFree(it->second.dev);
+    g->tables.erase(it);
+  }
+  FZ_GCUDA(g, cudaMalloc(&t.dev, t.host.size()), "group tables");
+  FZ_GCUDA(g, cudaMemcpy(t.dev, t.host.data(), t.host.size(), cudaMemcpyHostToDevice), "group tables upload");
+  char* d = (char*)t.dev;
+  for (int st = 0; st < 3; st++) {
+    gs[st].args = reinterpret_cast<const fz::StageArgs<R>*>(d + st * t.stage_bytes);
+    gs[st].maps = reinterpret_cast<const fz::StageMaps*>(d + t.off_maps + st * maps_bytes);
+    gb[st].args = reinterpret_cast<const fz::BandArgs<R>*>(d + t.off_band + st * t.band_bytes);
+  }
+  t.gstage.assign((const char*)gs.data(), (const char*)(gs.data() + 3));
+  t.gband.assign((const char*)gb.data(), (const char*)(gb.data() + 3));
+  g->tables.emplace(key, std::move(t));
+  return FZ_OK;
+}
+
+// Tables for the current roles and for the roles one step later (a graph covers both).
+int ensure_flat_tables(fz_group* g) {
+  for (int flip = 0; flip < 2; flip++) {
+    const int rc = g->fp64 ? flat_tables<double>(g, parity_key(g)) : flat_tables<float>(g, parity_key(g));
+    for (fz_handle* h : g->m) fzi::rotate(h);
+    if (rc != FZ_OK) {
+      if (flip == 0)
+        for (fz_handle* h : g->m) fzi::rotate(h);
+      return rc;
+    }
+  }
+  return FZ_OK;  // rotated twice: back where it was
+}
+
+// The three stage kernels of every member for the current roles, one launch per stage (the
+// autotuner's trial of the flat path).
+template <class R>
+cudaError_t flat_stage_kernels(fz_group* g, const FlatTables& t) {
+  const fz::GroupStageArgs<R>* gs = reinterpret_cast<const fz::GroupStageArgs<R>*>(t.gstage.data());
+  for (int st = 0; st < 3; st++) {
+    const cudaError_t e = fz::launch_stage_group<R>(st, gs[st], t.ctas, g->stream);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// One step of every member: per stage one stage launch and one band launch, then one receiver
+// launch; the members' roles advance as enqueue_finish advances them.
+template <class R>
+cudaError_t flat_step(fz_group* g) {
+  auto it = g->tables.find(parity_key(g));
+  if (it == g->tables.end()) return cudaErrorInvalidValue;  // built by ensure_flat_tables first
+  const FlatTables& t = it->second;
+  const fz::GroupStageArgs<R>* gs = reinterpret_cast<const fz::GroupStageArgs<R>*>(t.gstage.data());
+  const fz::GroupBandArgs<R>* gb = reinterpret_cast<const fz::GroupBandArgs<R>*>(t.gband.data());
+  for (int st = 0; st < 3; st++) {
+    cudaError_t e = fz::launch_stage_group<R>(st, gs[st], t.ctas, g->stream);
+    if (e == cudaSuccess) e = fz::launch_band_group<R>(st, gb[st], t.band_blocks, t.band_fit, g->stream);
+    if (e != cudaSuccess) return e;
+  }
+  const cudaError_t e = fz::launch_receivers_group<R>(
+      reinterpret_cast<const fz::RecArgs<R>*>((const char*)t.dev + t.off_rec), (int)g->m.size(), g->stream);
+  for (fz_handle* h : g->m) fzi::rotate(h);
+  return e;
+}
+
+cudaError_t flat_enqueue(fz_group* g) { return g->fp64 ? flat_step<double>(g) : flat_step<float>(g); }
+
 int capture(fz_group* g, cudaGraphExec_t* out) {
   cudaGraph_t graph = nullptr;
   FZ_GCUDA(g, cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
   cudaError_t e = cudaEventRecord(g->fork, g->stream);
-  for (size_t i = 0; i < g->m.size() && e == cudaSuccess; i++) {
+  if (g->flat)
+    for (int s = 0; s < g->graph_steps && e == cudaSuccess; s++) e = flat_enqueue(g);
+  for (size_t i = 0; i < g->m.size() && e == cudaSuccess && !g->flat; i++) {
     fz_handle* h = g->m[i];
     e = cudaStreamWaitEvent(h->stream, g->fork, 0);
     for (int s = 0; s < g->graph_steps && e == cudaSuccess; s++) e = fzi::enqueue(h);
@@ -81,6 +251,7 @@ void fz_group_destroy(fz_group* g) {
   cudaSetDevice(g->device);
   if (g->stream) cudaStreamSynchronize(g->stream);
   for (auto& kv : g->graphs) cudaGraphExecDestroy(kv.second);
+  free_tables(g);
   for (cudaEvent_t e : g->join) cudaEventDestroy(e);
   if (g->fork) cudaEventDestroy(g->fork);
   if (g->done) cudaEventDestroy(g->done);
@@ -108,6 +279,10 @@ int fz_group_create(fz_handle* const* members, int32_t n, fz_group** out) {
   if (!g) return fzi::set_global_error(FZ_ENOMEM, "fz_group_create: out of host memory");
   g->m.assign(members, members + n);
   g->device = members[0]->device;
+  g->fp64 = members[0]->fp64;
+  g->flat = n <= fz::FZ_MAX_GROUP;
+  for (fz_handle* h : g->m)
+    if (h->fp64 != g->fp64 || h->prm.two_d || h->sl_on) g->flat = false;
   cudaSetDevice(g->device);
   cudaError_t e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming);
@@ -123,6 +298,12 @@ int fz_group_create(fz_handle* const* members, int32_t n, fz_group** out) {
   return FZ_OK;
 }
 
+int fz_group_info(fz_group* g, int32_t* one_launch) {
+  if (!g || !one_launch) return fzi::set_global_error(FZ_EINVAL, "fz_group_info: NULL argument");
+  *one_launch = g->flat ? 1 : 0;
+  return FZ_OK;
+}
+
 int fz_group_run(fz_group* g, int64_t nsteps) {
   fz_range nvtx_range("fz_group_run");
   if (!g || nsteps < 0) return fzi::set_global_error(FZ_EINVAL, "fz_group_run: bad arguments");
@@ -131,6 +312,30 @@ int fz_group_run(fz_group* g, int64_t nsteps) {
     if (h->profiling) return fzi::set_global_error(FZ_EINVAL, "fz_group_run: a member has profiling enabled");
   const int G = g->graph_steps;
   int64_t done = 0;
+  if (g->flat) {
+    if (nsteps == 0) return FZ_OK;
+    int rc = ensure_flat_tables(g);
+    if (rc == FZ_OK) rc = order_after(g, false);  // the group starts after the members' earlier work
+    if (rc != FZ_OK) return rc;
+    while (nsteps - done >= G) {
+      const std::vector<int> key = parity_key(g);
+      auto it = g->graphs.find(key);
+      if (it == g->graphs.end()) {
+        cudaGraphExec_t ge = nullptr;
+        rc = capture(g, &ge);  // G is even: the members' roles are back where they were
+        if (rc != FZ_OK) return rc;
+        it = g->graphs.emplace(key, ge).first;
+      }
+      FZ_GCUDA(g, cudaGraphLaunch(it->second, g->stream), "group graph launch");
+      for (fz_handle* h : g->m) h->steps_enqueued += G;
+      done += G;
+    }
+    for (; done < nsteps; done++) {
+      FZ_GCUDA(g, flat_enqueue(g), "group step launch");
+      for (fz_handle* h : g->m) h->steps_enqueued += 1;
+    }
+    return order_after(g, true);  // later work on a member (fz_sync, fz_get_ir, fz_run) follows
+  }
   if (nsteps >= G) {
     int rc = order_after(g, false);  // the group starts after the members' earlier work
     if (rc != FZ_OK) return rc;
@@ -172,9 +377,24 @@ int fz_group_autotune(fz_group* g, int32_t reps, int32_t* kz_chunk, double* ms_p
   for (int c : {4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256})
     if (c <= nzmax) cand.push_back({c, 0});
   fzi::ZPlan best{0, 0};
-  rc = fzi::tune(g->m, g->stream, cand, reps, &best, ms_per_step);
-  for (auto& kv : g->graphs) cudaGraphExecDestroy(kv.second);  // captured with the old launch shape
-  g->graphs.clear();
+  if (g->flat) {
+    // trials of the flat path: the three one-launch stage kernels of all members
+    fzi::TuneHooks hooks;
+    hooks.on_plan = [g]() { return ensure_flat_tables(g); };
+    hooks.round = [g](int nrep) -> cudaError_t {
+      auto it = g->tables.find(parity_key(g));
+      if (it == g->tables.end()) return cudaErrorInvalidValue;
+      for (int r = 0; r < nrep; r++) {
+        const cudaError_t e = g->fp64 ? flat_stage_kernels<double>(g, it->second) : flat_stage_kernels<float>(g, it->second);
+        if (e != cudaSuccess) return e;
+      }
+      return cudaSuccess;
+    };
+    rc = fzi::tune(g->m, g->stream, cand, reps, &best, ms_per_step, &hooks);
+  } else {
+    rc = fzi::tune(g->m, g->stream, cand, reps, &best, ms_per_step);
+  }
+  drop_graphs(g);  // captured with the old launch shape
   if (rc != FZ_OK) return rc;
   if (kz_chunk) *kz_chunk = best.depth;
   return FZ_OK;

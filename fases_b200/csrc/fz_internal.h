@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -121,6 +122,10 @@ struct fz_handle {
   // wait-test build: plane of each z chunk whose tile the stage kernels never issue (-1: none)
   int test_skip_plane = -1;
 
+  // counts the events that invalidate captured launches (new launch shape, reallocated or rebound
+  // arrays): a group compares it with the value its argument tables were built at
+  uint64_t launch_gen = 0;
+
   // graphs, keyed by buffer parity
   int graph_steps = 10;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -177,10 +182,28 @@ struct ZPlan {
   int depth;
   int guided;
 };
+// Custom trial of a tuning run (the group path times its one-launch-per-kind stage kernels):
+// on_plan runs after each candidate has been applied to every handle, round(n) enqueues n steps'
+// stage kernels on the tuning stream.
+struct TuneHooks {
+  std::function<int()> on_plan;
+  std::function<cudaError_t(int)> round;
+};
 int tune(const std::vector<fz_handle*>& hs, cudaStream_t ts, const std::vector<ZPlan>& candidates, int reps,
-         ZPlan* best, double* ms_per_step);
+         ZPlan* best, double* ms_per_step, const TuneHooks* hooks = nullptr);
 // apply a candidate to one handle
 int apply_z_plan(fz_handle* h, const ZPlan& p);
+// Launch arguments of the handle's kernels for its current buffer roles (the group path lays the
+// arguments of several handles side by side in device memory): stage st's kernel and TMA
+// descriptors, stage st's band kernel, the receiver gather; rotate() advances the roles by one step
+// as enqueue_finish does.
+template <class R>
+void stage_desc(fz_handle* h, int st, fz::StageArgs<R>* a, fz::StageMaps* m);
+template <class R>
+void band_desc(fz_handle* h, int st, fz::BandArgs<R>* b);
+template <class R>
+void rec_desc(fz_handle* h, fz::RecArgs<R>* r);
+void rotate(fz_handle* h);
 // the launch shapes worth timing for one handle: the heuristic, the best-filling uniform depths and
 // guided schedules of the best of them
 std::vector<ZPlan> kz_candidates(fz_handle* h);

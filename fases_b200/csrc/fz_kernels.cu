@@ -137,9 +137,17 @@ __device__ __forceinline__ R source_sum(const StageArgs<R>& A, int64_t g) {
 #define FZ_STAGE_MINBLOCKS_F32 (1024 / NTHREADS)  // 32 warps per SM in FP32 (64 registers, no spills)
 #endif
 // DIM2: planar solve (one updated z-plane, no z fluxes): the 3D scheme restricted to 2D.
-template <class R, int STAGE, bool DIM2>
-__global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_F32 : 1)
-    k_stage(const StageArgs<R> A, const __grid_constant__ StageMaps M) {
+// CTA coordinates of a stage-kernel launch of one room: the launch grid itself.
+struct GridCta {
+  static __device__ __forceinline__ int x() { return blockIdx.x; }
+  static __device__ __forceinline__ int y() { return blockIdx.y; }
+  static __device__ __forceinline__ int z() { return blockIdx.z; }
+};
+
+// The body of one stage-kernel CTA: tile (CTA::x(), CTA::y()) of z chunk slot CTA::z() (batch
+// member x chunks) of the room A describes. A and M may live in parameter, shared or global memory.
+template <class R, int STAGE, bool DIM2, class CTA>
+__device__ __forceinline__ void stage_body(const StageArgs<R>& A, const StageMaps& M) {
   typedef typename Pair<R>::T P;
   typedef StageSmem<R> L;
   extern __shared__ __align__(128) unsigned char smem_dyn[];
@@ -151,12 +159,12 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
 
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int lt = ty * TX + tx;
-  const int i0 = GHOST + blockIdx.x * TX, j0 = GHOST + blockIdx.y * TY;
+  const int i0 = GHOST + CTA::x() * TX, j0 = GHOST + CTA::y() * TY;
   const int i = i0 + tx, j = j0 + ty;
   // batch members are stacked along z (member m owns planes [m Nz, (m+1) Nz)); the cPML z table,
   // the psi tiles and the class bytes are laid out per member the same way
-  const int member = blockIdx.z / A.zchunks;
-  const int chunk = blockIdx.z - member * A.zchunks;
+  const int member = CTA::z() / A.zchunks;
+  const int chunk = CTA::z() - member * A.zchunks;
   const int kb = GHOST + member * A.Nz + A.zoff[chunk];
   const int ke = min(GHOST + member * A.Nz + A.zoff[chunk + 1], (member + 1) * A.Nz - GHOST);
   if (kb >= ke) return;
@@ -453,6 +461,12 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
   }
 }
 
+template <class R, int STAGE, bool DIM2>
+__global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_F32 : 1)
+    k_stage(const __grid_constant__ StageArgs<R> A, const __grid_constant__ StageMaps M) {
+  stage_body<R, STAGE, DIM2, GridCta>(A, M);
+}
+
 // ------------------------------------------------------------------------------------------
 // Immersed ADE band (functions3D.cuh:462-565 + ADE_solver 426-459), one thread per band cell of
 // the compact list. Probe geometry (normal, trilinear corner and weights at C - 2h n, chi) is
@@ -488,9 +502,8 @@ struct Vec4<double> {
 // probe gathers, so one thread keeps ~50 loads in flight; KM = LM = 0 is the general form with
 // the state loads inside the pole loops.
 template <class R, int STAGE, int KM, int LM>
-__global__ void __launch_bounds__(256, (sizeof(R) == 4 && KM > 0 && KM <= 2) ? 4 : 3) k_band(const BandArgs<R> B) {
+__device__ __forceinline__ void band_body(const BandArgs<R>& B, const int64_t b) {
   typedef typename Vec4<R>::T V4;
-  const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= B.nB) return;
   const int4 rc = __ldg(B.rec + b);
   const int64_t cell = (int64_t)(((uint64_t)(uint32_t)rc.y << 32) | (uint32_t)rc.x);
@@ -603,12 +616,20 @@ __global__ void __launch_bounds__(256, (sizeof(R) == 4 && KM > 0 && KM <= 2) ? 4
   B.po[cell] = omc * po0 + chi * pb;
 }
 
+#define FZ_BAND_BOUNDS(R, KM) __launch_bounds__(256, (sizeof(R) == 4 && KM > 0 && KM <= 2) ? 4 : 3)
+
+template <class R, int STAGE, int KM, int LM>
+__global__ void FZ_BAND_BOUNDS(R, KM) k_band(const __grid_constant__ BandArgs<R> B) {
+  band_body<R, STAGE, KM, LM>(B, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 // Receiver gather after the last stage of a step (main3D.cu:1399-1414), into a device buffer;
 // then advances the device step counter. One block.
 template <class R>
-__global__ void k_receivers(const R* __restrict__ p, const R* __restrict__ u, const R* __restrict__ v,
-                            const R* __restrict__ w, const int64_t* __restrict__ rcell, int nrec,
-                            double* ir, double* vel, int64_t cap, int64_t* step, int32_t* err, int64_t nfield) {
+__device__ __forceinline__ void receivers_body(const R* __restrict__ p, const R* __restrict__ u,
+                                               const R* __restrict__ v, const R* __restrict__ w,
+                                               const int64_t* __restrict__ rcell, int nrec, double* ir, double* vel,
+                                               int64_t cap, int64_t* step, int32_t* err, int64_t nfield) {
   const int64_t n = *step;
   for (int r = threadIdx.x; r < nrec; r += blockDim.x) {
     const int64_t c = rcell[r];
@@ -626,6 +647,84 @@ __global__ void k_receivers(const R* __restrict__ p, const R* __restrict__ u, co
   }
   __syncthreads();
   if (threadIdx.x == 0) *step = n + 1;
+}
+
+template <class R>
+__global__ void k_receivers(const R* __restrict__ p, const R* __restrict__ u, const R* __restrict__ v,
+                            const R* __restrict__ w, const int64_t* __restrict__ rcell, int nrec,
+                            double* ir, double* vel, int64_t cap, int64_t* step, int32_t* err, int64_t nfield) {
+  receivers_body<R>(p, u, v, w, rcell, nrec, ir, vel, cap, step, err, nfield);
+}
+
+// ------------------------------------------------------------------------------------------
+// Groups of rooms in one launch per kernel kind. The CTAs (band blocks) of every member room are
+// laid end to end in one 1-D grid: a CTA finds its room from the prefix table of CTA counts,
+// copies that room's launch arguments from device memory into shared memory and runs the same
+// body as the one-room kernel, so each room's cells are updated exactly as a launch of its own
+// would update them.
+// ------------------------------------------------------------------------------------------
+__shared__ int g_group_cta[3];  // tile coordinates of this CTA inside its room
+
+struct GroupCta {
+  static __device__ __forceinline__ int x() { return g_group_cta[0]; }
+  static __device__ __forceinline__ int y() { return g_group_cta[1]; }
+  static __device__ __forceinline__ int z() { return g_group_cta[2]; }
+};
+
+// the member whose range [start[m], start[m+1]) holds `blk` (uniform across the block)
+__device__ __forceinline__ int group_member(const int32_t* start, int n, int blk) {
+  int m = 0;
+  while (m + 1 < n && blk >= start[m + 1]) ++m;
+  return m;
+}
+
+// word-wise copy of one member's argument block into shared memory by the whole block
+template <class T>
+__device__ __forceinline__ void copy_args(T& dst, const T* src, int t, int nt) {
+  static_assert(sizeof(T) % 4 == 0, "argument blocks are whole words");
+  const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
+  uint32_t* d = reinterpret_cast<uint32_t*>(&dst);
+  for (int w = t; w < (int)(sizeof(T) / 4); w += nt) d[w] = __ldg(s + w);
+}
+
+template <class R, int STAGE>
+__global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_F32 : 1)
+    k_stage_group(const __grid_constant__ GroupStageArgs<R> G) {
+  __shared__ __align__(16) StageArgs<R> sA;
+  const int t = threadIdx.y * blockDim.x + threadIdx.x;
+  const int m = group_member(G.cta_start, G.n, blockIdx.x);
+  copy_args(sA, G.args + m, t, NTHREADS);
+  if (t == 0) {
+    // the member's TMA descriptors were written to device memory by a copy: make them visible to
+    // the tensor-map proxy before this thread (the stage body's TMA issuer) uses them
+    const StageMaps* mp = G.maps + m;
+    for (int q = 0; q < (int)(sizeof(StageMaps) / sizeof(CUtensorMap)); q++)
+      asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<const CUtensorMap*>(mp) + q)
+                   : "memory");
+    const int local = (int)blockIdx.x - G.cta_start[m];
+    const int gx = G.gx[m], gy = G.gy[m];
+    g_group_cta[0] = local % gx;
+    g_group_cta[1] = (local / gx) % gy;
+    g_group_cta[2] = local / (gx * gy);
+  }
+  __syncthreads();
+  stage_body<R, STAGE, false, GroupCta>(sA, G.maps[m]);
+}
+
+template <class R, int STAGE, int KM, int LM>
+__global__ void FZ_BAND_BOUNDS(R, KM) k_band_group(const __grid_constant__ GroupBandArgs<R> G) {
+  __shared__ __align__(16) BandArgs<R> sB;
+  const int m = group_member(G.blk_start, G.n, blockIdx.x);
+  copy_args(sB, G.args + m, threadIdx.x, blockDim.x);
+  __syncthreads();
+  band_body<R, STAGE, KM, LM>(sB, (int64_t)((int)blockIdx.x - G.blk_start[m]) * blockDim.x + threadIdx.x);
+}
+
+// one block per member
+template <class R>
+__global__ void k_receivers_group(const RecArgs<R>* __restrict__ args) {
+  const RecArgs<R>& a = args[blockIdx.x];
+  receivers_body<R>(a.p, a.u, a.v, a.w, a.rcell, a.nrec, a.ir, a.vel, a.cap, a.step, a.err, a.nfield);
 }
 
 // Non-finite values in a state (p, u, v, w over n cells), counted into *count.
@@ -752,6 +851,12 @@ cudaError_t stage_setup() {
     const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return e;
   }
+  const void* gfns[3] = {(const void*)k_stage_group<R, 0>, (const void*)k_stage_group<R, 1>,
+                         (const void*)k_stage_group<R, 2>};
+  for (const void* f : gfns) {
+    const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+  }
   return cudaSuccess;
 }
 
@@ -839,6 +944,48 @@ cudaError_t launch_energy(const R* p, const R* u, const R* v, const R* w, int64_
   return cudaGetLastError();
 }
 
+template <class R>
+cudaError_t launch_stage_group(int stage, const GroupStageArgs<R>& g, int ctas, cudaStream_t s) {
+  if (ctas <= 0) return cudaSuccess;
+  const dim3 block(TX, TY, 1);
+  const size_t smem = stage_smem_bytes<R>();
+  if (stage == 0)
+    k_stage_group<R, 0><<<ctas, block, smem, s>>>(g);
+  else if (stage == 1)
+    k_stage_group<R, 1><<<ctas, block, smem, s>>>(g);
+  else
+    k_stage_group<R, 2><<<ctas, block, smem, s>>>(g);
+  return cudaGetLastError();
+}
+
+template <class R>
+cudaError_t launch_band_group(int stage, const GroupBandArgs<R>& g, int blocks, int fit, cudaStream_t s) {
+  if (blocks <= 0) return cudaSuccess;
+#define FZ_BANDG_LAUNCH(ST)                                      \
+  if (fit == 2)                                                  \
+    k_band_group<R, ST, 2, 2><<<blocks, 256, 0, s>>>(g);         \
+  else if (fit == 4)                                             \
+    k_band_group<R, ST, 4, 4><<<blocks, 256, 0, s>>>(g);         \
+  else                                                           \
+    k_band_group<R, ST, 0, 0><<<blocks, 256, 0, s>>>(g);
+  if (stage == 0) {
+    FZ_BANDG_LAUNCH(0)
+  } else if (stage == 1) {
+    FZ_BANDG_LAUNCH(1)
+  } else {
+    FZ_BANDG_LAUNCH(2)
+  }
+#undef FZ_BANDG_LAUNCH
+  return cudaGetLastError();
+}
+
+template <class R>
+cudaError_t launch_receivers_group(const RecArgs<R>* args, int n, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_receivers_group<R><<<n, 256, 0, s>>>(args);
+  return cudaGetLastError();
+}
+
 #define FZ_INSTANTIATE(R)                                                                          \
   template size_t stage_smem_bytes<R>();                                                           \
   template cudaError_t stage_setup<R>();                                                           \
@@ -853,7 +1000,10 @@ cudaError_t launch_energy(const R* p, const R* u, const R* v, const R* w, int64_
   template cudaError_t launch_slices<R>(const R*, const R*, const R*, const R*, int, int, int, int64_t, int, int, \
                                         int, const int64_t*, int64_t, int64_t, float*, int, cudaStream_t);       \
   template cudaError_t launch_energy<R>(const R*, const R*, const R*, const R*, int64_t, double,   \
-                                        double, double*, int, cudaStream_t);
+                                        double, double*, int, cudaStream_t);                       \
+  template cudaError_t launch_stage_group<R>(int, const GroupStageArgs<R>&, int, cudaStream_t);    \
+  template cudaError_t launch_band_group<R>(int, const GroupBandArgs<R>&, int, int, cudaStream_t); \
+  template cudaError_t launch_receivers_group<R>(const RecArgs<R>*, int, cudaStream_t);
 
 FZ_INSTANTIATE(float)
 FZ_INSTANTIATE(double)

@@ -29,6 +29,13 @@ template <class R>
 cudaError_t launch_slices(const R* p, const R* u, const R* v, const R* w, int Nx, int Ny, int Nz, int64_t Sx, int i0,
                           int j0, int k0, const int64_t* step, int64_t anim_step, int64_t cap, float* out,
                           int nsm, cudaStream_t s);
+// groups of rooms: one launch per kernel kind over the member rooms' CTAs laid end to end
+template <class R>
+cudaError_t launch_stage_group(int stage, const GroupStageArgs<R>& g, int ctas, cudaStream_t s);
+template <class R>
+cudaError_t launch_band_group(int stage, const GroupBandArgs<R>& g, int blocks, int fit, cudaStream_t s);
+template <class R>
+cudaError_t launch_receivers_group(const RecArgs<R>* args, int n, cudaStream_t s);
 template <class R>
 cudaError_t launch_energy(const R* p, const R* u, const R* v, const R* w, int64_t n, double inv_rc2,
                           double rho, double* out, int nsm, cudaStream_t s);

@@ -121,7 +121,7 @@ std::vector<ZPlan> kz_candidates(fz_handle* h) {
 }
 
 int tune(const std::vector<fz_handle*>& hs, cudaStream_t ts, const std::vector<ZPlan>& candidates, int reps,
-         ZPlan* best, double* ms_per_step) {
+         ZPlan* best, double* ms_per_step, const TuneHooks* hooks) {
   if (hs.empty() || candidates.empty()) return set_global_error(FZ_EINVAL, "autotune: nothing to tune");
   reps = std::max(1, std::min(reps, 100));
   for (fz_handle* h : hs) {
@@ -145,6 +145,7 @@ int tune(const std::vector<fz_handle*>& hs, cudaStream_t ts, const std::vector<Z
   for (size_t q = 0; q < hs.size() && e == cudaSuccess; q++) e = cudaEventCreateWithFlags(&join[q], cudaEventDisableTiming);
   // one round of `n` steps' stage kernels of every handle, side by side, forked from and joined to ts
   auto round = [&](int n) -> cudaError_t {
+    if (hooks && hooks->round) return hooks->round(n);
     cudaError_t x = cudaEventRecord(fork, ts);
     for (size_t q = 0; q < hs.size() && x == cudaSuccess; q++) {
       fz_handle* h = hs[q];
@@ -163,6 +164,7 @@ int tune(const std::vector<fz_handle*>& hs, cudaStream_t ts, const std::vector<Z
       const int rc = apply_z_plan(h, candidates[c]);
       if (rc != FZ_OK && e == cudaSuccess) e = cudaErrorInvalidValue;
     }
+    if (e == cudaSuccess && hooks && hooks->on_plan && hooks->on_plan() != FZ_OK) e = cudaErrorInvalidValue;
     e = round(1);  // warm-up of this launch shape
     if (e == cudaSuccess) e = cudaEventRecord(a, ts);
     if (e == cudaSuccess) e = round(reps);
@@ -184,6 +186,7 @@ int tune(const std::vector<fz_handle*>& hs, cudaStream_t ts, const std::vector<Z
   for (cudaEvent_t j : join)
     if (j) cudaEventDestroy(j);
   for (fz_handle* h : hs) apply_z_plan(h, chosen);
+  if (hooks && hooks->on_plan) hooks->on_plan();
   int rc = FZ_OK;
   for (size_t q = 0; q < hs.size(); q++) {
     const int r = restore_state(hs[q], saved[q]);

@@ -395,9 +395,10 @@ class Solver:
 
 
 class Group:
-    """Several solvers (rooms) on one device advanced together: every run of 10 steps is one CUDA
-    graph whose parallel branches are the members. The members stay usable alone and must outlive
-    the group."""
+    """Several solvers (rooms) on one device advanced together. 3D rooms of one precision without
+    animation slices (up to 64) are stepped with one launch per kernel kind for all of them;
+    other groups run each member's launches as parallel graph branches. Runs of 10 steps are CUDA
+    graphs. The members stay usable alone and must outlive the group."""
 
     def __init__(self, solvers):
         self.solvers = list(solvers)
@@ -406,6 +407,12 @@ class Group:
         g = C.c_void_p()
         check(lib().fz_group_create(arr, len(self.solvers), C.byref(g)))
         self._g = g
+
+    def one_launch(self):
+        """True when all members are stepped by one launch per kernel kind."""
+        v = C.c_int32()
+        check(lib().fz_group_info(self._g, C.byref(v)))
+        return bool(v.value)
 
     def run(self, nsteps, sync=True, timeout_ms=0):
         check(lib().fz_group_run(self._g, int(nsteps)))
@@ -418,8 +425,8 @@ class Group:
         return ms.value
 
     def autotune(self, reps=3):
-        """One tile depth for every member, timed with the members' stage kernels side by side
-        (0 = each member's own heuristic); returns (depth, stage ms per step of the group)."""
+        """One tile depth for every member, timed on the group's own stage launches (0 = each
+        member's own heuristic); returns (depth, stage ms per step of the group)."""
         k, ms = C.c_int32(), C.c_double()
         check(lib().fz_group_autotune(self._g, int(reps), C.byref(k), C.byref(ms)))
         return k.value, ms.value

@@ -218,11 +218,15 @@ int fz_check_health(fz_handle* h, int64_t* nonfinite);
 int fz_steps_done(fz_handle* h, int64_t* n);
 
 /* Groups: several handles (rooms) on one device advanced together. fz_group_run enqueues nsteps
- * steps of every member; each run of 10 steps is one CUDA graph whose parallel branches are the
- * members, so small rooms run side by side instead of one after another. Members keep their own
- * state and stay usable alone (fz_get_ir, fz_sync, fz_run); they must all be on one device, must
- * outlive the group, and are finalised (materials, sources, receivers fixed) by fz_group_create.
- * No counterpart in the reference (one process per room). */
+ * steps of every member. When every member is a 3D room of the group's precision without animation
+ * slices and there are at most 64 of them, each kernel kind of a step is ONE launch over all members
+ * (their CTAs laid end to end, each CTA reading its room's arguments from a table in device
+ * memory): three stage launches, three band launches and one receiver launch per step, whatever
+ * the member count; otherwise each member's own launches run as parallel branches. Runs of 10
+ * steps are CUDA graphs either way. Members keep their own state and stay usable alone (fz_get_ir,
+ * fz_sync, fz_run); they must all be on one device, must outlive the group, and are finalised
+ * (materials, sources, receivers fixed) by fz_group_create. Results are those of each member run
+ * alone, bit for bit. No counterpart in the reference (one process per room). */
 typedef struct fz_group fz_group;
 int fz_group_create(fz_handle* const* members, int32_t n, fz_group** out);
 int fz_group_run(fz_group* g, int64_t nsteps);
@@ -230,6 +234,9 @@ int fz_group_run(fz_group* g, int64_t nsteps);
 int fz_group_run_timed(fz_group* g, int64_t nsteps, double* ms);
 int fz_group_sync(fz_group* g, int64_t timeout_ms);
 void fz_group_destroy(fz_group* g);
+/* *one_launch = 1 when the group steps all members with one launch per kernel kind, 0 when each
+ * member's own launches run as graph branches. */
+int fz_group_info(fz_group* g, int32_t* one_launch);
 
 /* Launch-shape autotuner. A stage-kernel CTA covers 32 x 16 columns by one z chunk of planes;
  * the chunk lengths set how many CTAs a stage launches and how whole waves of SMs fill. fz_autotune

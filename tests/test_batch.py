@@ -95,6 +95,7 @@ def test_group_members_equal_solo_runs():
         s.close()
     members = [_solver(c, "fp32", src_rows=SOURCES[:1], p0=c["p0"]) for c in cfgs]
     with Group(members) as g:
+        assert g.one_launch()  # 3D rooms of one precision: one launch per kernel kind
         g.run(steps)
         for s, ref in zip(members, solos):
             assert s.steps_done() == steps
@@ -102,5 +103,67 @@ def test_group_members_equal_solo_runs():
         # a member stays usable alone after group runs
         members[1].run(3)
         assert members[1].steps_done() == steps + 3
+    for s in members:
+        s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_one_launch_group_of_unlike_rooms_equals_solo_runs(precision):
+    """The one-launch group path over rooms that differ in every way its tables carry: sizes
+    (ragged tiles), cPML faces and thickness, pole counts (the group then takes the general band
+    form), a room without obstacles, a batched member with two source positions; the members start
+    at different steps, and the group runs ungraphed steps, a tuning pass and a graph."""
+    from fases_b200 import Group
+    steps = 21
+    specs = [dict(seed=40, room=(37, 21, 19), pml=(0, 1, 0, 1, 0, 1), pml_cells=4),
+             dict(seed=41, room=(26, 22, 18), pml=(1, 1, 1, 1, 1, 1), pml_cells=5, K=5, L=3),
+             dict(seed=42, room=(30, 20, 16), pml=(0, 0, 0, 0, 0, 0), obstacle=False, K=1, L=1),
+             dict(seed=43, room=(24, 24, 22), pml=(0, 0, 1, 0, 0, 0))]
+    cfgs = [small_room(steps=steps, **kw) for kw in specs]
+    batch = [1, 1, 1, 2]
+
+    def make(q):
+        c = cfgs[q]
+        if batch[q] > 1:
+            return _solver(c, precision, batch=2, src_rows=SOURCES[:2], members=np.arange(2))
+        return _solver(c, precision, src_rows=SOURCES[:1], p0=c["p0"])
+
+    solos = []
+    for q in range(len(cfgs)):
+        s = make(q)
+        s.run(steps)
+        solos.append(s.ir())
+        s.close()
+    members = [make(q) for q in range(len(cfgs))]
+    members[0].run(3)  # members may start at different steps (and buffer parities)
+    with Group(members) as g:
+        assert g.one_launch()
+        g.run(8)         # graph-free steps of the group
+        g.autotune(reps=1)
+        g.run(10)        # one 10-step graph
+        for s in members[1:]:
+            s.run(3)     # the others finish alone
+        for q, s in enumerate(members):
+            assert s.steps_done() == steps
+            assert np.array_equal(s.ir(), solos[q]), q
+    for s in members:
+        s.close()
+
+
+@pytest.mark.gpu
+def test_group_with_a_sliced_member_uses_graph_branches():
+    from fases_b200 import Group
+    cfgs = [small_room(seed=50 + q, steps=12) for q in range(2)]
+    solo = _solver(cfgs[1], "fp32", src_rows=SOURCES[:1], p0=cfgs[1]["p0"])
+    solo.run(12)
+    ref = solo.ir()
+    solo.close()
+    members = [_solver(c, "fp32", src_rows=SOURCES[:1], p0=c["p0"]) for c in cfgs]
+    members[0].set_slices(10, 10, 9, 4, 4)
+    with Group(members) as g:
+        assert not g.one_launch()
+        g.run(12)
+        assert np.array_equal(members[1].ir(), ref)
     for s in members:
         s.close()
