@@ -128,7 +128,11 @@ template <class R>
 __device__ __forceinline__ typename Pair<R>::T godunov(typename Pair<R>::T vm, typename Pair<R>::T vp,
                                                        typename Pair<R>::T kA, typename Pair<R>::T kC) {
   const typename Pair<R>::T sum = padd(vm, vp), dif = psub(vp, vm);
+#if defined(FZ_V_SCALARFLUX)
+  return pmk(fma(dif.x, kC.x, sum.y * kA.x), fma(dif.y, kC.y, sum.x * kA.y));
+#else
   return pfma(dif, kC, pmul(pswap(sum), kA));
+#endif
 }
 
 // Difference of the Godunov fluxes through the low and the high face of a cell, F(lo) - F(hi),
@@ -141,7 +145,12 @@ __device__ __forceinline__ typename Pair<R>::T godunov_diff(typename Pair<R>::T 
                                                             typename Pair<R>::T kA, typename Pair<R>::T kC) {
   const typename Pair<R>::T S = psub(padd(vm_lo, vp_lo), padd(vm_hi, vp_hi));
   const typename Pair<R>::T D = psub(psub(vp_lo, vm_lo), psub(vp_hi, vm_hi));
+#if defined(FZ_V_SCALARFLUX)
+  // the swapped product in scalar form: the same arithmetic without moving the pair's halves
+  return pmk(fma(D.x, kC.x, S.y * kA.x), fma(D.y, kC.y, S.x * kA.y));
+#else
   return pfma(D, kC, pmul(pswap(S), kA));
+#endif
 }
 
 }  // namespace fz

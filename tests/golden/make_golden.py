@@ -6,8 +6,8 @@ its own sources by oracle/build_ref.sh into oracle/_ref/fases3D -- on it, and ke
 plus the reference's outputs: output/S.bin, output/oid.bin, output/scene_cache.txt,
 output/header.txt, output/pre_header.txt, config/p_ref.bin and output/IR*/VEL* traces.
 
-    python tests/golden/make_golden.py OUT_DIR      # on a machine with a GPU; then copy
-                                                    # OUT_DIR/<case> into tests/golden/<case>
+    python tests/golden/make_golden.py OUT_DIR [CASE ...]   # on a machine with a GPU; then copy
+                                                            # OUT_DIR/<case> into tests/golden/<case>
 
 The reference needs a CUDA GPU; the committed fixtures let the CPU tests check the oracle
 without one.
@@ -84,6 +84,13 @@ CASES = {
                                                          ((0.85, 0.15, 0.1), (1.0, 0.3, 0.35))],
                       src_opt=0, glob_f=100.0, src=[(0.3, 0.5, 0.4, 85.0)],
                       rec=[(0.9, 0.7, 0.5), (0.2, 0.8, 0.2), (0.6, 0.2, 0.6)], seed=4, open_wall=1, K=5, L=3),
+    # animation slices kept (pressure{X,Y,Z}.bin and the energy-flow planes I*_*.bin): 60 frames asked on
+    # the planes through (0.5, 0.45, 0.35) m, cPML on one face, one obstacle
+    "box_slices": dict(room=(1.2, 1.0, 0.8), h=0.04, t_max=0.012, f_in=250.0, temp=20.0, cfl=0.5,
+                       pml=(0, 0, 1, 0, 0, 0), obstacles=[((0.7, 0.5, 0.3), (0.9, 0.7, 0.5))],
+                       src_opt=0, glob_f=100.0, src=[(0.3, 0.3, 0.4, 85.0)],
+                       rec=[(0.9, 0.3, 0.5), (0.2, 0.8, 0.2)], seed=5, open_wall=1,
+                       slice=(0.5, 0.45, 0.35), frames=60, keep_slices=True),
 }
 
 
@@ -115,7 +122,7 @@ def make_project(case, dest, spec=None):
         materials["obstacle%d" % q] = m
     with open(os.path.join(dest, "config", "poles.txt"), "w") as f:
         f.write("%d %d\n" % (c.get("K", 2), c.get("L", 2)))
-    x0, y0, z0 = [0.5 * L for L in c["room"]]
+    x0, y0, z0 = c.get("slice", [0.5 * L for L in c["room"]])
     cfg = [c["h"], c["t_max"], c["f_in"], c["temp"], c["cfl"], 8, *c["pml"], 0, 0, 0, c["src_opt"], c["glob_f"], 0,
            x0, y0, z0, c.get("frames", 60)]
     names = ["h", "t_max", "wave band", "temperature", "CFL", "ADE poles", "U_PML", "D_PML", "R_PML", "L_PML",
@@ -189,10 +196,13 @@ def neutral_paths(dest, prefix=None):
                 f.write(txt.replace(prefix, "./"))
 
 
-def prune(dest):
-    """Keep only what the tests read (inputs + FVM outputs)."""
+def prune(dest, keep_slices=False):
+    """Keep only what the tests read (inputs + FVM outputs; the animation slices if asked)."""
     out = os.path.join(dest, "output")
     keep = {"S.bin", "oid.bin", "scene_cache.txt", "header.txt", "pre_header.txt"}
+    if keep_slices:
+        keep |= {"pressureX.bin", "pressureY.bin", "pressureZ.bin", "Iy_X.bin", "Iz_X.bin", "Ix_Y.bin",
+                 "Iz_Y.bin", "Ix_Z.bin", "Iy_Z.bin"}
     for fn in os.listdir(out):
         if fn in keep or (fn.startswith("IR") or fn.startswith("VEL")) and fn.endswith(".bin"):
             continue
@@ -209,17 +219,17 @@ def prune(dest):
 
 if __name__ == "__main__":
     if len(sys.argv) < 2:
-        sys.exit("usage: make_golden.py OUTPUT_DIR")
+        sys.exit("usage: make_golden.py OUTPUT_DIR [CASE ...]")
     out_root = os.path.abspath(sys.argv[1])
     rc_all = 0
-    for case in CASES:
+    for case in (sys.argv[2:] or CASES):
         dest = os.path.join(out_root, case)
         if os.path.exists(dest):
             shutil.rmtree(dest)
         make_project(case, dest)
         rc = run_reference(dest)
         print(case, "reference exit code", rc)
-        prune(dest)
+        prune(dest, keep_slices=CASES[case].get("keep_slices", False))
         neutral_paths(dest)
         rc_all |= rc
     sys.exit(rc_all)
