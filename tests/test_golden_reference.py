@@ -14,7 +14,7 @@ import pytest
 from tests.golden import fixture
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-CASES = ["box_pcs", "box_ricker", "box_sine", "box_poles"]
+CASES = ["box_pcs", "box_ricker", "box_sine", "box_poles", "box_slices"]
 # FP64 oracle vs the reference's FP32 solver: per-receiver relative L2
 TOL_ORACLE = 5e-6
 # FP32 CUDA stepper vs the reference's FP32 solver
