@@ -209,13 +209,17 @@ struct RecArgs {
 // Groups of rooms stepped by one launch per kernel kind (see k_stage_group).
 constexpr int FZ_MAX_GROUP = 64;
 
+// Members one stage launch of a group covers: their TMA descriptors travel as kernel parameters
+// (1 KB each; kernel parameters may take up to 32 KB), the rest of their arguments in device memory.
+constexpr int FZ_GROUP_LAUNCH = 28;
+
 template <class R>
 struct GroupStageArgs {
+  StageMaps maps[FZ_GROUP_LAUNCH];  // member m's TMA descriptors (parameter space, as a one-room launch)
   const StageArgs<R>* args;  // [n] in device memory: each member's stage arguments
-  const StageMaps* maps;     // [n] in device memory (64-byte aligned): each member's TMA descriptors
   int32_t n;
-  int32_t cta_start[FZ_MAX_GROUP + 1];  // first CTA of member m in the group grid; [n] = total
-  int32_t gx[FZ_MAX_GROUP], gy[FZ_MAX_GROUP];  // member m's tiles along x and y
+  int32_t cta_start[FZ_GROUP_LAUNCH + 1];  // first CTA of member m in this launch's grid; [n] = total
+  int32_t gx[FZ_GROUP_LAUNCH], gy[FZ_GROUP_LAUNCH];  // member m's tiles along x and y
 };
 
 template <class R>

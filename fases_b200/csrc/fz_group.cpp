@@ -1,14 +1,15 @@
 // fz_group.cpp -- several solver handles (rooms) advanced together. Small rooms leave most of the
 // GPU idle when stepped one after another. Rooms of one precision (3D, without animation slices,
-// up to FZ_MAX_GROUP) are stepped by one launch per kernel kind: each stage kernel, band kernel
-// and receiver gather covers every member, its CTAs laid end to end (fz_kernels.cu,
-// k_stage_group), from argument tables in device memory; runs of graph_steps steps are CUDA
-// graphs of these launches. Other groups run each member's own launches as parallel branches of
+// up to FZ_MAX_GROUP) share their launches: per stage one band launch over all members and one
+// stage launch per FZ_GROUP_LAUNCH members, their CTAs laid end to end (fz_kernels.cu,
+// k_stage_group), from argument tables in device memory, then one receiver launch; runs of
+// graph_steps steps are CUDA graphs of these launches. Other groups run each member's own launches as parallel branches of
 // one graph per run.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <chrono>
+#include <cstring>
 #include <map>
 #include <string>
 #include <thread>
@@ -17,19 +18,19 @@
 #include "fz_internal.h"
 #include "fz_kernels.h"
 
-// Launch arguments of every member for one buffer-parity key, laid side by side in one device
-// buffer: [3 stages][n] stage arguments, [3][n] TMA descriptor sets, [3][n] band arguments, [n]
-// receiver arguments.
+// Launch arguments of every member for one buffer-parity key. Device memory holds [3 stages][n]
+// stage arguments, [3][n] band arguments and [n] receiver arguments side by side; the stage launches'
+// kernel parameters (each covering up to FZ_GROUP_LAUNCH members, with their TMA descriptors) and
+// the band launches' parameters are kept on the host.
 struct FlatTables {
   void* dev = nullptr;
-  std::vector<char> host;
-  size_t off_maps = 0, off_band = 0, off_rec = 0, stage_bytes = 0, band_bytes = 0, rec_bytes = 0;
-  int ctas = 0;             // stage CTAs of all members
-  int band_blocks = 0;      // band blocks of all members
-  int band_fit = 0;         // pole-count form of the band kernel (2, 4 or 0 = general)
-  std::vector<char> gstage; // GroupStageArgs<R> host copy per stage (kernel parameters)
-  std::vector<char> gband;  // GroupBandArgs<R> host copy per stage
-  std::vector<uint64_t> gen;  // the members' launch_gen when the tables were built
+  size_t off_band = 0, off_rec = 0, stage_bytes = 0, band_bytes = 0;
+  std::vector<char> gstage[3];  // GroupStageArgs<R> of each stage launch, one per member chunk
+  std::vector<int> chunk_ctas;  // CTAs of each chunk's stage launch
+  std::vector<char> gband;      // GroupBandArgs<R> per stage
+  int band_blocks = 0;          // band blocks of all members
+  int band_fit = 0;             // pole-count form of the band kernel (2, 4 or 0 = general)
+  std::vector<uint64_t> gen;    // the members' launch_gen when the tables were built
 };
 
 struct fz_group {
@@ -41,8 +42,8 @@ struct fz_group {
   std::vector<cudaEvent_t> join;
   // keyed by the members' buffer parities (the field-set rotation repeats every 2 steps)
   std::map<std::vector<int>, cudaGraphExec_t> graphs;
-  // one launch per kernel kind for all members (3D rooms of one precision, no animation slices,
-  // at most FZ_MAX_GROUP); otherwise each member's own launches are branches of the graph
+  // shared launches for all members (3D rooms of one precision, no animation slices, at most
+  // FZ_MAX_GROUP); otherwise each member's own launches are branches of the graph
   bool flat = false;
   bool fp64 = false;
   std::map<std::vector<int>, FlatTables> tables;
@@ -105,33 +106,25 @@ int flat_tables(fz_group* g, const std::vector<int>& key) {
   FlatTables t;
   t.gen = gen;
   t.stage_bytes = sizeof(fz::StageArgs<R>) * n;
-  t.off_maps = ((3 * t.stage_bytes + 127) / 128) * 128;
-  const size_t maps_bytes = sizeof(fz::StageMaps) * n;
-  t.off_band = t.off_maps + ((3 * maps_bytes + 127) / 128) * 128;
+  t.off_band = ((3 * t.stage_bytes + 127) / 128) * 128;
   t.band_bytes = sizeof(fz::BandArgs<R>) * n;
   t.off_rec = t.off_band + ((3 * t.band_bytes + 127) / 128) * 128;
-  t.rec_bytes = sizeof(fz::RecArgs<R>) * n;
-  t.host.assign(t.off_rec + t.rec_bytes, 0);
-  std::vector<fz::GroupStageArgs<R>> gs(3);
+  std::vector<char> host(t.off_rec + sizeof(fz::RecArgs<R>) * n, 0);
+  std::vector<fz::StageMaps> maps((size_t)3 * n);
   std::vector<fz::GroupBandArgs<R>> gb(3);
-  int ctas = 0, blocks = 0, kmax = 0, lmax = 0;
+  std::vector<int> ctas_of(n);
+  int blocks = 0, kmax = 0, lmax = 0;
   for (int q = 0; q < n; q++) {
     fz_handle* h = g->m[(size_t)q];
     for (int st = 0; st < 3; st++) {
-      fz::StageArgs<R>* a = reinterpret_cast<fz::StageArgs<R>*>(t.host.data() + st * t.stage_bytes) + q;
-      fz::StageMaps* mp = reinterpret_cast<fz::StageMaps*>(t.host.data() + t.off_maps + st * maps_bytes) + q;
-      fzi::stage_desc<R>(h, st, a, mp);
-      fzi::band_desc<R>(h, st, reinterpret_cast<fz::BandArgs<R>*>(t.host.data() + t.off_band + st * t.band_bytes) + q);
-    }
-    fzi::rec_desc<R>(h, reinterpret_cast<fz::RecArgs<R>*>(t.host.data() + t.off_rec) + q);
-    const dim3 gr = h->stage_grid;
-    for (int st = 0; st < 3; st++) {
-      gs[st].cta_start[q] = ctas;
-      gs[st].gx[q] = (int)gr.x;
-      gs[st].gy[q] = (int)gr.y;
+      fzi::stage_desc<R>(h, st, reinterpret_cast<fz::StageArgs<R>*>(host.data() + st * t.stage_bytes) + q,
+                         &maps[(size_t)st * n + q]);
+      fzi::band_desc<R>(h, st, reinterpret_cast<fz::BandArgs<R>*>(host.data() + t.off_band + st * t.band_bytes) + q);
       gb[st].blk_start[q] = blocks;
     }
-    ctas += (int)(gr.x * gr.y * gr.z);
+    fzi::rec_desc<R>(h, reinterpret_cast<fz::RecArgs<R>*>(host.data() + t.off_rec) + q);
+    const dim3 gr = h->stage_grid;
+    ctas_of[q] = (int)(gr.x * gr.y * gr.z);
     blocks += (int)((h->nB + 255) / 256);
     if (h->nB > 0) {
       kmax = std::max(kmax, h->K);
@@ -139,31 +132,47 @@ int flat_tables(fz_group* g, const std::vector<int>& key) {
     }
   }
   for (int st = 0; st < 3; st++) {
-    gs[st].n = n;
-    gs[st].cta_start[n] = ctas;
     gb[st].n = n;
     gb[st].blk_start[n] = blocks;
   }
-  t.ctas = ctas;
   t.band_blocks = blocks;
   t.band_fit = (kmax <= 2 && lmax <= 2) ? 2 : (kmax <= 4 && lmax <= 4) ? 4 : 0;
   drop_graphs(g);
   if (it != g->tables.end()) {
     // launches still queued may read the old tables: a new buffer, the old one freed when idle
-    // (a new address also keeps TMA descriptors cached for the old contents out of the way)
     FZ_GCUDA(g, cudaStreamSynchronize(g->stream), "group tables");
     cudaFree(it->second.dev);
     g->tables.erase(it);
   }
-  FZ_GCUDA(g, cudaMalloc(&t.dev, t.host.size()), "group tables");
-  FZ_GCUDA(g, cudaMemcpy(t.dev, t.host.data(), t.host.size(), cudaMemcpyHostToDevice), "group tables upload");
+  FZ_GCUDA(g, cudaMalloc(&t.dev, host.size()), "group tables");
+  FZ_GCUDA(g, cudaMemcpy(t.dev, host.data(), host.size(), cudaMemcpyHostToDevice), "group tables upload");
   char* d = (char*)t.dev;
-  for (int st = 0; st < 3; st++) {
-    gs[st].args = reinterpret_cast<const fz::StageArgs<R>*>(d + st * t.stage_bytes);
-    gs[st].maps = reinterpret_cast<const fz::StageMaps*>(d + t.off_maps + st * maps_bytes);
-    gb[st].args = reinterpret_cast<const fz::BandArgs<R>*>(d + t.off_band + st * t.band_bytes);
+  // stage launches: members in chunks of at most FZ_GROUP_LAUNCH, as even as possible
+  const int nchunk = (n + fz::FZ_GROUP_LAUNCH - 1) / fz::FZ_GROUP_LAUNCH;
+  for (int c = 0; c < nchunk; c++) {
+    const int m0 = (int)((int64_t)n * c / nchunk), m1 = (int)((int64_t)n * (c + 1) / nchunk);
+    int ctas = 0;
+    for (int st = 0; st < 3; st++) {
+      fz::GroupStageArgs<R> ga;
+      std::memset(&ga, 0, sizeof(ga));
+      ga.args = reinterpret_cast<const fz::StageArgs<R>*>(d + st * t.stage_bytes) + m0;
+      ga.n = m1 - m0;
+      ctas = 0;
+      for (int q = m0; q < m1; q++) {
+        ga.maps[q - m0] = maps[(size_t)st * n + q];
+        ga.cta_start[q - m0] = ctas;
+        ga.gx[q - m0] = (int)g->m[(size_t)q]->stage_grid.x;
+        ga.gy[q - m0] = (int)g->m[(size_t)q]->stage_grid.y;
+        ctas += ctas_of[q];
+      }
+      ga.cta_start[m1 - m0] = ctas;
+      const char* b = reinterpret_cast<const char*>(&ga);
+      t.gstage[st].insert(t.gstage[st].end(), b, b + sizeof(ga));
+    }
+    t.chunk_ctas.push_back(ctas);
   }
-  t.gstage.assign((const char*)gs.data(), (const char*)(gs.data() + 3));
+  for (int st = 0; st < 3; st++)
+    gb[st].args = reinterpret_cast<const fz::BandArgs<R>*>(d + t.off_band + st * t.band_bytes);
   t.gband.assign((const char*)gb.data(), (const char*)(gb.data() + 3));
   g->tables.emplace(key, std::move(t));
   return FZ_OK;
@@ -186,10 +195,19 @@ int ensure_flat_tables(fz_group* g) {
 // The three stage kernels of every member for the current roles, one launch per stage (the
 // autotuner's trial of the flat path).
 template <class R>
+cudaError_t flat_stage_launches(fz_group* g, const FlatTables& t, int st) {
+  const fz::GroupStageArgs<R>* gs = reinterpret_cast<const fz::GroupStageArgs<R>*>(t.gstage[st].data());
+  for (size_t c = 0; c < t.chunk_ctas.size(); c++) {
+    const cudaError_t e = fz::launch_stage_group<R>(st, gs[c], t.chunk_ctas[c], g->stream);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+template <class R>
 cudaError_t flat_stage_kernels(fz_group* g, const FlatTables& t) {
-  const fz::GroupStageArgs<R>* gs = reinterpret_cast<const fz::GroupStageArgs<R>*>(t.gstage.data());
   for (int st = 0; st < 3; st++) {
-    const cudaError_t e = fz::launch_stage_group<R>(st, gs[st], t.ctas, g->stream);
+    const cudaError_t e = flat_stage_launches<R>(g, t, st);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -202,10 +220,9 @@ cudaError_t flat_step(fz_group* g) {
   auto it = g->tables.find(parity_key(g));
   if (it == g->tables.end()) return cudaErrorInvalidValue;  // built by ensure_flat_tables first
   const FlatTables& t = it->second;
-  const fz::GroupStageArgs<R>* gs = reinterpret_cast<const fz::GroupStageArgs<R>*>(t.gstage.data());
   const fz::GroupBandArgs<R>* gb = reinterpret_cast<const fz::GroupBandArgs<R>*>(t.gband.data());
   for (int st = 0; st < 3; st++) {
-    cudaError_t e = fz::launch_stage_group<R>(st, gs[st], t.ctas, g->stream);
+    cudaError_t e = flat_stage_launches<R>(g, t, st);
     if (e == cudaSuccess) e = fz::launch_band_group<R>(st, gb[st], t.band_blocks, t.band_fit, g->stream);
     if (e != cudaSuccess) return e;
   }
@@ -298,9 +315,9 @@ int fz_group_create(fz_handle* const* members, int32_t n, fz_group** out) {
   return FZ_OK;
 }
 
-int fz_group_info(fz_group* g, int32_t* one_launch) {
-  if (!g || !one_launch) return fzi::set_global_error(FZ_EINVAL, "fz_group_info: NULL argument");
-  *one_launch = g->flat ? 1 : 0;
+int fz_group_info(fz_group* g, int32_t* shared) {
+  if (!g || !shared) return fzi::set_global_error(FZ_EINVAL, "fz_group_info: NULL argument");
+  *shared = g->flat ? 1 : 0;
   return FZ_OK;
 }
 

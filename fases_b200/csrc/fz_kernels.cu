@@ -388,17 +388,16 @@ __device__ __forceinline__ void stage_body(const StageArgs<R>& A, const StageMap
           un = u_in + A.dt_h * Lx.y;
           vn = v_in + A.dt_h * Ly.y;
           wn = w_in + A.dt_h * Lz.y;
-        } else if (STAGE == 1) {
-          pn = R(0.75) * bp + R(0.25) * (p_in + A.dt_h * Lp);
-          un = R(0.75) * bu + R(0.25) * (u_in + A.dt_h * Lx.y);
-          vn = R(0.75) * bv + R(0.25) * (v_in + A.dt_h * Ly.y);
-          wn = R(0.75) * bw + R(0.25) * (w_in + A.dt_h * Lz.y);
         } else {
-          const R third = R(1.0 / 3.0), two3 = R(2.0 / 3.0);
-          pn = third * bp + two3 * (p_in + A.dt_h * Lp);
-          un = third * bu + two3 * (u_in + A.dt_h * Lx.y);
-          vn = third * bv + two3 * (v_in + A.dt_h * Ly.y);
-          wn = third * bw + two3 * (w_in + A.dt_h * Lz.y);
+          // the stage combination a U0 + b (U_in + dt L) with a + b = 1, written as
+          // U0 + b ((U_in + dt L) - U0): the weights sum to one exactly. In FP32 the rounded
+          // 1/3 and 2/3 sum to 1 + 3e-8, a gain the whole field would pick up every step (the
+          // reference divides by 3 instead, functions3D.cuh:1311-1314, which is unbiased too).
+          const R wb = (STAGE == 1) ? R(0.25) : R(2.0 / 3.0);
+          pn = bp + wb * ((p_in + A.dt_h * Lp) - bp);
+          un = bu + wb * ((u_in + A.dt_h * Lx.y) - bu);
+          vn = bv + wb * ((v_in + A.dt_h * Ly.y) - bv);
+          wn = bw + wb * ((w_in + A.dt_h * Lz.y) - bw);
         }
         if (pml_xy || (A.pml_on && fz_inb(A.err, k, A.npc[2]) && A.pcz[k].tile >= 0)) {
           // cPML (functions3D.cuh:725-755): field += w dt ((1/kappa - 1) D + psi), psi frozen
@@ -659,9 +658,9 @@ __global__ void k_receivers(const R* __restrict__ p, const R* __restrict__ u, co
 // ------------------------------------------------------------------------------------------
 // Groups of rooms in one launch per kernel kind. The CTAs (band blocks) of every member room are
 // laid end to end in one 1-D grid: a CTA finds its room from the prefix table of CTA counts,
-// copies that room's launch arguments from device memory into shared memory and runs the same
-// body as the one-room kernel, so each room's cells are updated exactly as a launch of its own
-// would update them.
+// copies that room's launch arguments from device memory into shared memory (its TMA descriptors
+// come as kernel parameters, as in a one-room launch) and runs the same body as the one-room
+// kernel, so each room's cells are updated exactly as a launch of its own would update them.
 // ------------------------------------------------------------------------------------------
 __shared__ int g_group_cta[3];  // tile coordinates of this CTA inside its room
 
@@ -695,12 +694,6 @@ __global__ void __launch_bounds__(NTHREADS, sizeof(R) == 4 ? FZ_STAGE_MINBLOCKS_
   const int m = group_member(G.cta_start, G.n, blockIdx.x);
   copy_args(sA, G.args + m, t, NTHREADS);
   if (t == 0) {
-    // the member's TMA descriptors were written to device memory by a copy: make them visible to
-    // the tensor-map proxy before this thread (the stage body's TMA issuer) uses them
-    const StageMaps* mp = G.maps + m;
-    for (int q = 0; q < (int)(sizeof(StageMaps) / sizeof(CUtensorMap)); q++)
-      asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<const CUtensorMap*>(mp) + q)
-                   : "memory");
     const int local = (int)blockIdx.x - G.cta_start[m];
     const int gx = G.gx[m], gy = G.gy[m];
     g_group_cta[0] = local % gx;

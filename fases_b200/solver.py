@@ -396,8 +396,8 @@ class Solver:
 
 class Group:
     """Several solvers (rooms) on one device advanced together. 3D rooms of one precision without
-    animation slices (up to 64) are stepped with one launch per kernel kind for all of them;
-    other groups run each member's launches as parallel graph branches. Runs of 10 steps are CUDA
+    animation slices (up to 64) share their launches (per stage one band launch for all and one
+    stage launch per 28 rooms); other groups run each member's launches as parallel graph branches. Runs of 10 steps are CUDA
     graphs. The members stay usable alone and must outlive the group."""
 
     def __init__(self, solvers):
@@ -408,8 +408,8 @@ class Group:
         check(lib().fz_group_create(arr, len(self.solvers), C.byref(g)))
         self._g = g
 
-    def one_launch(self):
-        """True when all members are stepped by one launch per kernel kind."""
+    def shared_launches(self):
+        """True when the members share their launches."""
         v = C.c_int32()
         check(lib().fz_group_info(self._g, C.byref(v)))
         return bool(v.value)

@@ -219,10 +219,11 @@ int fz_steps_done(fz_handle* h, int64_t* n);
 
 /* Groups: several handles (rooms) on one device advanced together. fz_group_run enqueues nsteps
  * steps of every member. When every member is a 3D room of the group's precision without animation
- * slices and there are at most 64 of them, each kernel kind of a step is ONE launch over all members
- * (their CTAs laid end to end, each CTA reading its room's arguments from a table in device
- * memory): three stage launches, three band launches and one receiver launch per step, whatever
- * the member count; otherwise each member's own launches run as parallel branches. Runs of 10
+ * slices and there are at most 64 of them, the members share their launches: per stage one band
+ * launch over all members and one stage launch per 28 members (their CTAs laid end to end, each CTA
+ * reading its room's arguments from a table in device memory; the rooms' TMA descriptors travel as
+ * kernel parameters), then one receiver launch, whatever the member count; otherwise each member's
+ * own launches run as parallel branches. Runs of 10
  * steps are CUDA graphs either way. Members keep their own state and stay usable alone (fz_get_ir,
  * fz_sync, fz_run); they must all be on one device, must outlive the group, and are finalised
  * (materials, sources, receivers fixed) by fz_group_create. Results are those of each member run
@@ -234,9 +235,9 @@ int fz_group_run(fz_group* g, int64_t nsteps);
 int fz_group_run_timed(fz_group* g, int64_t nsteps, double* ms);
 int fz_group_sync(fz_group* g, int64_t timeout_ms);
 void fz_group_destroy(fz_group* g);
-/* *one_launch = 1 when the group steps all members with one launch per kernel kind, 0 when each
+/* *shared = 1 when the group steps its members with shared launches (above), 0 when each
  * member's own launches run as graph branches. */
-int fz_group_info(fz_group* g, int32_t* one_launch);
+int fz_group_info(fz_group* g, int32_t* shared);
 
 /* Launch-shape autotuner. A stage-kernel CTA covers 32 x 16 columns by one z chunk of planes;
  * the chunk lengths set how many CTAs a stage launches and how whole waves of SMs fill. fz_autotune

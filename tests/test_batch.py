@@ -95,7 +95,7 @@ def test_group_members_equal_solo_runs():
         s.close()
     members = [_solver(c, "fp32", src_rows=SOURCES[:1], p0=c["p0"]) for c in cfgs]
     with Group(members) as g:
-        assert g.one_launch()  # 3D rooms of one precision: one launch per kernel kind
+        assert g.shared_launches()  # 3D rooms of one precision: shared launches
         g.run(steps)
         for s, ref in zip(members, solos):
             assert s.steps_done() == steps
@@ -109,8 +109,8 @@ def test_group_members_equal_solo_runs():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
-def test_one_launch_group_of_unlike_rooms_equals_solo_runs(precision):
-    """The one-launch group path over rooms that differ in every way its tables carry: sizes
+def test_shared_launch_group_of_unlike_rooms_equals_solo_runs(precision):
+    """The shared-launch group path over rooms that differ in every way its tables carry: sizes
     (ragged tiles), cPML faces and thickness, pole counts (the group then takes the general band
     form), a room without obstacles, a batched member with two source positions; the members start
     at different steps, and the group runs ungraphed steps, a tuning pass and a graph."""
@@ -138,7 +138,7 @@ def test_one_launch_group_of_unlike_rooms_equals_solo_runs(precision):
     members = [make(q) for q in range(len(cfgs))]
     members[0].run(3)  # members may start at different steps (and buffer parities)
     with Group(members) as g:
-        assert g.one_launch()
+        assert g.shared_launches()
         g.run(8)         # graph-free steps of the group
         g.autotune(reps=1)
         g.run(10)        # one 10-step graph
@@ -162,8 +162,33 @@ def test_group_with_a_sliced_member_uses_graph_branches():
     members = [_solver(c, "fp32", src_rows=SOURCES[:1], p0=c["p0"]) for c in cfgs]
     members[0].set_slices(10, 10, 9, 4, 4)
     with Group(members) as g:
-        assert not g.one_launch()
+        assert not g.shared_launches()
         g.run(12)
         assert np.array_equal(members[1].ir(), ref)
+    for s in members:
+        s.close()
+
+
+@pytest.mark.gpu
+def test_group_larger_than_one_stage_launch_equals_solo_runs():
+    """More members than one stage launch covers (its TMA descriptors are kernel parameters): the
+    stage kernels run as several launches over member chunks, the band and receiver kernels as one."""
+    from fases_b200 import Group
+    steps = 12
+    rooms = [(20 + (q % 5), 18 + (q % 3), 15 + (q % 4)) for q in range(30)]
+    cfgs = [small_room(seed=60 + q, room=r, steps=steps, obstacle=False) for q, r in enumerate(rooms)]
+    src = np.array([[6, 6, 7]], np.int32)
+    solos = []
+    for c in cfgs:
+        s = _solver(c, "fp32", src_rows=src, p0=c["p0"])
+        s.run(steps)
+        solos.append(s.ir())
+        s.close()
+    members = [_solver(c, "fp32", src_rows=src, p0=c["p0"]) for c in cfgs]
+    with Group(members) as g:
+        assert g.shared_launches()
+        g.run(steps)
+        for s, ref in zip(members, solos):
+            assert np.array_equal(s.ir(), ref)
     for s in members:
         s.close()
