@@ -152,7 +152,8 @@ SIGNATURES = {
     "fz_group_run_timed": (C.c_int, [_P, _i64, _dp]),
     "fz_group_sync": (C.c_int, [_P, _i64]),
     "fz_group_destroy": (None, [_P]),
-    "fz_group_info": (C.c_int, [_P, _ip]),
+    "fz_group_info": (C.c_int, [_P, _ip, _ip]),
+    "fz_group_set_branches": (C.c_int, [_P, _i32]),
     "fz_get_ir": (C.c_int, [_P, _fp, _i64]),
     "fz_get_ir64": (C.c_int, [_P, _dp, _i64]),
     "fz_get_vel": (C.c_int, [_P, _fp, _i64]),

@@ -19,18 +19,24 @@
 #include "fz_kernels.h"
 
 // Launch arguments of every member for one buffer-parity key. Device memory holds [3 stages][n]
-// stage arguments, [3][n] band arguments and [n] receiver arguments side by side; the stage launches'
-// kernel parameters (each covering up to FZ_GROUP_LAUNCH members, with their TMA descriptors) and
-// the band launches' parameters are kept on the host.
-struct FlatTables {
-  void* dev = nullptr;
-  size_t off_band = 0, off_rec = 0, stage_bytes = 0, band_bytes = 0;
+// stage arguments, [3][n] band arguments and [n] receiver arguments side by side, members ordered
+// by branch; each branch's stage launches' kernel parameters (each covering up to FZ_GROUP_LAUNCH
+// members, with their TMA descriptors) and its band launches' parameters are kept on the host.
+struct FlatBranch {
   std::vector<char> gstage[3];  // GroupStageArgs<R> of each stage launch, one per member chunk
   std::vector<int> chunk_ctas;  // CTAs of each chunk's stage launch
   std::vector<char> gband;      // GroupBandArgs<R> per stage
-  int band_blocks = 0;          // band blocks of all members
+  int band_blocks = 0;          // band blocks of the branch's members
   int band_fit = 0;             // pole-count form of the band kernel (2, 4 or 0 = general)
-  std::vector<uint64_t> gen;    // the members' launch_gen when the tables were built
+  size_t rec_off = 0;           // the branch's receiver arguments in the device buffer
+  int n = 0;                    // members in the branch
+};
+
+struct FlatTables {
+  void* dev = nullptr;
+  std::vector<FlatBranch> br;
+  std::vector<uint64_t> gen;  // the members' launch_gen when the tables were built
+  int nbranch = 0;            // the branch count they were built for
 };
 
 struct fz_group {
@@ -47,6 +53,12 @@ struct fz_group {
   bool flat = false;
   bool fp64 = false;
   std::map<std::vector<int>, FlatTables> tables;
+  // shared launches run as `nbranch` concurrent branches (streams), each over a set of members of
+  // about equal cells, so one branch's band and receiver launches overlap another's stage launch
+  int nbranch = 1;
+  std::vector<int> branch_of;  // branch of each member
+  std::vector<cudaStream_t> bstream;
+  std::vector<cudaEvent_t> bjoin;
 };
 
 namespace {
@@ -92,96 +104,155 @@ void drop_graphs(fz_group* g) {
   g->graphs.clear();
 }
 
+// Branches of a group of n rooms unless set (fz_group_set_branches).
+int default_branches(int n) { return n >= 16 ? 4 : n >= 4 ? 2 : 1; }
+
+// Members into branches of about equal cells (largest first into the lightest branch).
+void assign_branches(fz_group* g, int nbranch) {
+  const int n = (int)g->m.size();
+  nbranch = std::max(1, std::min(nbranch, n));
+  std::vector<int> idx(n);
+  for (int q = 0; q < n; q++) idx[q] = q;
+  auto cells = [&](int q) { return (int64_t)g->m[(size_t)q]->ncell_dev * g->m[(size_t)q]->nb; };
+  std::sort(idx.begin(), idx.end(), [&](int a, int b) { return cells(a) > cells(b); });
+  std::vector<int64_t> load((size_t)nbranch, 0);
+  g->branch_of.assign((size_t)n, 0);
+  for (int q : idx) {
+    const int b = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    g->branch_of[(size_t)q] = b;
+    load[(size_t)b] += cells(q);
+  }
+  g->nbranch = nbranch;
+}
+
+// Streams and join events of the branches (the group stream is branch 0's).
+int ensure_branch_streams(fz_group* g) {
+  while ((int)g->bstream.size() < g->nbranch) {
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev = nullptr;
+    FZ_GCUDA(g, cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "branch stream");
+    const cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+      cudaStreamDestroy(st);
+      return gfail(g, e, "branch event");
+    }
+    g->bstream.push_back(st);
+    g->bjoin.push_back(ev);
+  }
+  return FZ_OK;
+}
+
+cudaStream_t branch_stream(const fz_group* g, int b) { return b == 0 ? g->stream : g->bstream[(size_t)b]; }
+
 // Builds (or checks) the flat tables of the members' current roles. When a member's launches
 // changed since the tables were uploaded (a new launch shape, reallocated or rebound arrays: its
-// launch_gen moved), the tables are built again, and every captured graph goes, since graphs hold
-// the old kernel parameters.
+// launch_gen moved) or the branches changed, the tables are built again, and every captured graph
+// goes, since graphs hold the old kernel parameters.
 template <class R>
 int flat_tables(fz_group* g, const std::vector<int>& key) {
   const int n = (int)g->m.size();
   std::vector<uint64_t> gen;
   for (const fz_handle* h : g->m) gen.push_back(h->launch_gen);
   auto it = g->tables.find(key);
-  if (it != g->tables.end() && it->second.gen == gen) return FZ_OK;  // unchanged
+  if (it != g->tables.end() && it->second.gen == gen && it->second.nbranch == g->nbranch) return FZ_OK;
   FlatTables t;
   t.gen = gen;
-  t.stage_bytes = sizeof(fz::StageArgs<R>) * n;
-  t.off_band = ((3 * t.stage_bytes + 127) / 128) * 128;
-  t.band_bytes = sizeof(fz::BandArgs<R>) * n;
-  t.off_rec = t.off_band + ((3 * t.band_bytes + 127) / 128) * 128;
-  std::vector<char> host(t.off_rec + sizeof(fz::RecArgs<R>) * n, 0);
+  t.nbranch = g->nbranch;
+  // members in branch order: position q of the device arrays holds member order[q]
+  std::vector<int> order;
+  for (int b = 0; b < g->nbranch; b++)
+    for (int q = 0; q < n; q++)
+      if (g->branch_of[(size_t)q] == b) order.push_back(q);
+  const size_t stage_bytes = sizeof(fz::StageArgs<R>) * n;
+  const size_t off_band = ((3 * stage_bytes + 127) / 128) * 128;
+  const size_t band_bytes = sizeof(fz::BandArgs<R>) * n;
+  const size_t off_rec = off_band + ((3 * band_bytes + 127) / 128) * 128;
+  std::vector<char> host(off_rec + sizeof(fz::RecArgs<R>) * n, 0);
   std::vector<fz::StageMaps> maps((size_t)3 * n);
-  std::vector<fz::GroupBandArgs<R>> gb(3);
-  std::vector<int> ctas_of(n);
-  int blocks = 0, kmax = 0, lmax = 0;
   for (int q = 0; q < n; q++) {
-    fz_handle* h = g->m[(size_t)q];
+    fz_handle* h = g->m[(size_t)order[(size_t)q]];
     for (int st = 0; st < 3; st++) {
-      fzi::stage_desc<R>(h, st, reinterpret_cast<fz::StageArgs<R>*>(host.data() + st * t.stage_bytes) + q,
+      fzi::stage_desc<R>(h, st, reinterpret_cast<fz::StageArgs<R>*>(host.data() + st * stage_bytes) + q,
                          &maps[(size_t)st * n + q]);
-      fzi::band_desc<R>(h, st, reinterpret_cast<fz::BandArgs<R>*>(host.data() + t.off_band + st * t.band_bytes) + q);
-      gb[st].blk_start[q] = blocks;
+      fzi::band_desc<R>(h, st, reinterpret_cast<fz::BandArgs<R>*>(host.data() + off_band + st * band_bytes) + q);
     }
-    fzi::rec_desc<R>(h, reinterpret_cast<fz::RecArgs<R>*>(host.data() + t.off_rec) + q);
-    const dim3 gr = h->stage_grid;
-    ctas_of[q] = (int)(gr.x * gr.y * gr.z);
-    blocks += (int)((h->nB + 255) / 256);
-    if (h->nB > 0) {
-      kmax = std::max(kmax, h->K);
-      lmax = std::max(lmax, h->L);
-    }
+    fzi::rec_desc<R>(h, reinterpret_cast<fz::RecArgs<R>*>(host.data() + off_rec) + q);
   }
-  for (int st = 0; st < 3; st++) {
-    gb[st].n = n;
-    gb[st].blk_start[n] = blocks;
-  }
-  t.band_blocks = blocks;
-  t.band_fit = (kmax <= 2 && lmax <= 2) ? 2 : (kmax <= 4 && lmax <= 4) ? 4 : 0;
   drop_graphs(g);
   if (it != g->tables.end()) {
     // launches still queued may read the old tables: a new buffer, the old one freed when idle
-    FZ_GCUDA(g, cudaStreamSynchronize(g->stream), "group tables");
+    FZ_GCUDA(g, cudaDeviceSynchronize(), "group tables");
     cudaFree(it->second.dev);
     g->tables.erase(it);
   }
   FZ_GCUDA(g, cudaMalloc(&t.dev, host.size()), "group tables");
   FZ_GCUDA(g, cudaMemcpy(t.dev, host.data(), host.size(), cudaMemcpyHostToDevice), "group tables upload");
   char* d = (char*)t.dev;
-  // stage launches: members in chunks of at most FZ_GROUP_LAUNCH, as even as possible
-  const int nchunk = (n + fz::FZ_GROUP_LAUNCH - 1) / fz::FZ_GROUP_LAUNCH;
-  for (int c = 0; c < nchunk; c++) {
-    const int m0 = (int)((int64_t)n * c / nchunk), m1 = (int)((int64_t)n * (c + 1) / nchunk);
-    int ctas = 0;
-    for (int st = 0; st < 3; st++) {
-      fz::GroupStageArgs<R> ga;
-      std::memset(&ga, 0, sizeof(ga));
-      ga.args = reinterpret_cast<const fz::StageArgs<R>*>(d + st * t.stage_bytes) + m0;
-      ga.n = m1 - m0;
-      ctas = 0;
-      for (int q = m0; q < m1; q++) {
-        ga.maps[q - m0] = maps[(size_t)st * n + q];
-        ga.cta_start[q - m0] = ctas;
-        ga.gx[q - m0] = (int)g->m[(size_t)q]->stage_grid.x;
-        ga.gy[q - m0] = (int)g->m[(size_t)q]->stage_grid.y;
-        ctas += ctas_of[q];
+  int q0 = 0;
+  for (int b = 0; b < g->nbranch; b++) {
+    FlatBranch fb;
+    int q1 = q0;
+    while (q1 < n && g->branch_of[(size_t)order[(size_t)q1]] == b) q1++;
+    fb.n = q1 - q0;
+    fb.rec_off = off_rec + sizeof(fz::RecArgs<R>) * q0;
+    // band: one launch over the branch's members
+    std::vector<fz::GroupBandArgs<R>> gb(3);
+    int blocks = 0, kmax = 0, lmax = 0;
+    for (int q = q0; q < q1; q++) {
+      const fz_handle* h = g->m[(size_t)order[(size_t)q]];
+      for (int st = 0; st < 3; st++) gb[st].blk_start[q - q0] = blocks;
+      blocks += (int)((h->nB + 255) / 256);
+      if (h->nB > 0) {
+        kmax = std::max(kmax, h->K);
+        lmax = std::max(lmax, h->L);
       }
-      ga.cta_start[m1 - m0] = ctas;
-      const char* b = reinterpret_cast<const char*>(&ga);
-      t.gstage[st].insert(t.gstage[st].end(), b, b + sizeof(ga));
     }
-    t.chunk_ctas.push_back(ctas);
+    for (int st = 0; st < 3; st++) {
+      gb[st].n = fb.n;
+      gb[st].blk_start[fb.n] = blocks;
+      gb[st].args = reinterpret_cast<const fz::BandArgs<R>*>(d + off_band + st * band_bytes) + q0;
+    }
+    fb.band_blocks = blocks;
+    fb.band_fit = (kmax <= 2 && lmax <= 2) ? 2 : (kmax <= 4 && lmax <= 4) ? 4 : 0;
+    fb.gband.assign((const char*)gb.data(), (const char*)(gb.data() + 3));
+    // stage launches: the branch's members in chunks of at most FZ_GROUP_LAUNCH, as even as possible
+    const int nchunk = (fb.n + fz::FZ_GROUP_LAUNCH - 1) / fz::FZ_GROUP_LAUNCH;
+    for (int c = 0; c < nchunk; c++) {
+      const int m0 = q0 + (int)((int64_t)fb.n * c / nchunk), m1 = q0 + (int)((int64_t)fb.n * (c + 1) / nchunk);
+      int ctas = 0;
+      for (int st = 0; st < 3; st++) {
+        fz::GroupStageArgs<R> ga;
+        std::memset(&ga, 0, sizeof(ga));
+        ga.args = reinterpret_cast<const fz::StageArgs<R>*>(d + st * stage_bytes) + m0;
+        ga.n = m1 - m0;
+        ctas = 0;
+        for (int q = m0; q < m1; q++) {
+          const dim3 gr = g->m[(size_t)order[(size_t)q]]->stage_grid;
+          ga.maps[q - m0] = maps[(size_t)st * n + q];
+          ga.cta_start[q - m0] = ctas;
+          ga.gx[q - m0] = (int)gr.x;
+          ga.gy[q - m0] = (int)gr.y;
+          ctas += (int)(gr.x * gr.y * gr.z);
+        }
+        ga.cta_start[m1 - m0] = ctas;
+        const char* bp = reinterpret_cast<const char*>(&ga);
+        fb.gstage[st].insert(fb.gstage[st].end(), bp, bp + sizeof(ga));
+      }
+      fb.chunk_ctas.push_back(ctas);
+    }
+    t.br.push_back(std::move(fb));
+    q0 = q1;
   }
-  for (int st = 0; st < 3; st++)
-    gb[st].args = reinterpret_cast<const fz::BandArgs<R>*>(d + t.off_band + st * t.band_bytes);
-  t.gband.assign((const char*)gb.data(), (const char*)(gb.data() + 3));
   g->tables.emplace(key, std::move(t));
   return FZ_OK;
 }
 
 // Tables for the current roles and for the roles one step later (a graph covers both).
 int ensure_flat_tables(fz_group* g) {
+  int rc = ensure_branch_streams(g);
+  if (rc != FZ_OK) return rc;
   for (int flip = 0; flip < 2; flip++) {
-    const int rc = g->fp64 ? flat_tables<double>(g, parity_key(g)) : flat_tables<float>(g, parity_key(g));
+    rc = g->fp64 ? flat_tables<double>(g, parity_key(g)) : flat_tables<float>(g, parity_key(g));
     for (fz_handle* h : g->m) fzi::rotate(h);
     if (rc != FZ_OK) {
       if (flip == 0)
@@ -192,54 +263,83 @@ int ensure_flat_tables(fz_group* g) {
   return FZ_OK;  // rotated twice: back where it was
 }
 
-// The three stage kernels of every member for the current roles, one launch per stage (the
-// autotuner's trial of the flat path).
-template <class R>
-cudaError_t flat_stage_launches(fz_group* g, const FlatTables& t, int st) {
-  const fz::GroupStageArgs<R>* gs = reinterpret_cast<const fz::GroupStageArgs<R>*>(t.gstage[st].data());
-  for (size_t c = 0; c < t.chunk_ctas.size(); c++) {
-    const cudaError_t e = fz::launch_stage_group<R>(st, gs[c], t.chunk_ctas[c], g->stream);
-    if (e != cudaSuccess) return e;
-  }
-  return cudaSuccess;
+// Every branch's stream waits for the group stream (fork), and the group stream for every branch
+// (join).
+cudaError_t branches_fork(fz_group* g) {
+  if (g->nbranch <= 1) return cudaSuccess;
+  cudaError_t e = cudaEventRecord(g->fork, g->stream);
+  for (int b = 1; b < g->nbranch && e == cudaSuccess; b++) e = cudaStreamWaitEvent(g->bstream[(size_t)b], g->fork, 0);
+  return e;
 }
-
-template <class R>
-cudaError_t flat_stage_kernels(fz_group* g, const FlatTables& t) {
-  for (int st = 0; st < 3; st++) {
-    const cudaError_t e = flat_stage_launches<R>(g, t, st);
-    if (e != cudaSuccess) return e;
+cudaError_t branches_join(fz_group* g) {
+  cudaError_t e = cudaSuccess;
+  for (int b = 1; b < g->nbranch && e == cudaSuccess; b++) {
+    e = cudaEventRecord(g->bjoin[(size_t)b], g->bstream[(size_t)b]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(g->stream, g->bjoin[(size_t)b], 0);
   }
-  return cudaSuccess;
-}
-
-// One step of every member: per stage one stage launch and one band launch, then one receiver
-// launch; the members' roles advance as enqueue_finish advances them.
-template <class R>
-cudaError_t flat_step(fz_group* g) {
-  auto it = g->tables.find(parity_key(g));
-  if (it == g->tables.end()) return cudaErrorInvalidValue;  // built by ensure_flat_tables first
-  const FlatTables& t = it->second;
-  const fz::GroupBandArgs<R>* gb = reinterpret_cast<const fz::GroupBandArgs<R>*>(t.gband.data());
-  for (int st = 0; st < 3; st++) {
-    cudaError_t e = flat_stage_launches<R>(g, t, st);
-    if (e == cudaSuccess) e = fz::launch_band_group<R>(st, gb[st], t.band_blocks, t.band_fit, g->stream);
-    if (e != cudaSuccess) return e;
-  }
-  const cudaError_t e = fz::launch_receivers_group<R>(
-      reinterpret_cast<const fz::RecArgs<R>*>((const char*)t.dev + t.off_rec), (int)g->m.size(), g->stream);
-  for (fz_handle* h : g->m) fzi::rotate(h);
   return e;
 }
 
-cudaError_t flat_enqueue(fz_group* g) { return g->fp64 ? flat_step<double>(g) : flat_step<float>(g); }
+template <class R>
+cudaError_t flat_stage_launches(fz_group* g, const FlatBranch& fb, int st, cudaStream_t s) {
+  const fz::GroupStageArgs<R>* gs = reinterpret_cast<const fz::GroupStageArgs<R>*>(fb.gstage[st].data());
+  for (size_t c = 0; c < fb.chunk_ctas.size(); c++) {
+    const cudaError_t e = fz::launch_stage_group<R>(st, gs[c], fb.chunk_ctas[c], s);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// The three stage kernels of every member for the current roles (the autotuner's trial of the
+// shared-launch path), n times, on the branches.
+template <class R>
+cudaError_t flat_stage_kernels(fz_group* g, const FlatTables& t, int n) {
+  cudaError_t e = branches_fork(g);
+  for (int b = 0; b < g->nbranch && e == cudaSuccess; b++)
+    for (int r = 0; r < n && e == cudaSuccess; r++)
+      for (int st = 0; st < 3 && e == cudaSuccess; st++)
+        e = flat_stage_launches<R>(g, t.br[(size_t)b], st, branch_stream(g, b));
+  if (e == cudaSuccess) e = branches_join(g);
+  return e;
+}
+
+// nsteps steps of every member: each branch on its stream runs, per step and stage, its stage
+// launches and one band launch, then one receiver launch; the members' roles advance as
+// enqueue_finish advances them. Branches depend on nothing of each other within the run.
+template <class R>
+cudaError_t flat_steps(fz_group* g, int nsteps) {
+  cudaError_t e = branches_fork(g);
+  for (int s = 0; s < nsteps && e == cudaSuccess; s++) {
+    auto it = g->tables.find(parity_key(g));
+    if (it == g->tables.end()) return cudaErrorInvalidValue;  // built by ensure_flat_tables first
+    const FlatTables& t = it->second;
+    for (int b = 0; b < g->nbranch && e == cudaSuccess; b++) {
+      const FlatBranch& fb = t.br[(size_t)b];
+      const cudaStream_t bs = branch_stream(g, b);
+      const fz::GroupBandArgs<R>* gb = reinterpret_cast<const fz::GroupBandArgs<R>*>(fb.gband.data());
+      for (int st = 0; st < 3 && e == cudaSuccess; st++) {
+        e = flat_stage_launches<R>(g, fb, st, bs);
+        if (e == cudaSuccess) e = fz::launch_band_group<R>(st, gb[st], fb.band_blocks, fb.band_fit, bs);
+      }
+      if (e == cudaSuccess)
+        e = fz::launch_receivers_group<R>(reinterpret_cast<const fz::RecArgs<R>*>((const char*)t.dev + fb.rec_off),
+                                          fb.n, bs);
+    }
+    for (fz_handle* h : g->m) fzi::rotate(h);
+  }
+  if (e == cudaSuccess) e = branches_join(g);
+  return e;
+}
+
+cudaError_t flat_enqueue(fz_group* g, int nsteps) {
+  return g->fp64 ? flat_steps<double>(g, nsteps) : flat_steps<float>(g, nsteps);
+}
 
 int capture(fz_group* g, cudaGraphExec_t* out) {
   cudaGraph_t graph = nullptr;
   FZ_GCUDA(g, cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
   cudaError_t e = cudaEventRecord(g->fork, g->stream);
-  if (g->flat)
-    for (int s = 0; s < g->graph_steps && e == cudaSuccess; s++) e = flat_enqueue(g);
+  if (g->flat && e == cudaSuccess) e = flat_enqueue(g, g->graph_steps);
   for (size_t i = 0; i < g->m.size() && e == cudaSuccess && !g->flat; i++) {
     fz_handle* h = g->m[i];
     e = cudaStreamWaitEvent(h->stream, g->fork, 0);
@@ -269,6 +369,13 @@ void fz_group_destroy(fz_group* g) {
   if (g->stream) cudaStreamSynchronize(g->stream);
   for (auto& kv : g->graphs) cudaGraphExecDestroy(kv.second);
   free_tables(g);
+  for (size_t b = 0; b < g->bstream.size(); b++) {
+    if (g->bstream[b]) {
+      cudaStreamSynchronize(g->bstream[b]);
+      cudaStreamDestroy(g->bstream[b]);
+    }
+    if (g->bjoin[b]) cudaEventDestroy(g->bjoin[b]);
+  }
   for (cudaEvent_t e : g->join) cudaEventDestroy(e);
   if (g->fork) cudaEventDestroy(g->fork);
   if (g->done) cudaEventDestroy(g->done);
@@ -300,6 +407,9 @@ int fz_group_create(fz_handle* const* members, int32_t n, fz_group** out) {
   g->flat = n <= fz::FZ_MAX_GROUP;
   for (fz_handle* h : g->m)
     if (h->fp64 != g->fp64 || h->prm.two_d || h->sl_on) g->flat = false;
+  assign_branches(g, default_branches(n));
+  g->bstream.push_back(nullptr);  // branch 0 runs on the group stream
+  g->bjoin.push_back(nullptr);
   cudaSetDevice(g->device);
   cudaError_t e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming);
@@ -315,9 +425,20 @@ int fz_group_create(fz_handle* const* members, int32_t n, fz_group** out) {
   return FZ_OK;
 }
 
-int fz_group_info(fz_group* g, int32_t* shared) {
+int fz_group_info(fz_group* g, int32_t* shared, int32_t* branches) {
   if (!g || !shared) return fzi::set_global_error(FZ_EINVAL, "fz_group_info: NULL argument");
   *shared = g->flat ? 1 : 0;
+  if (branches) *branches = g->flat ? g->nbranch : (int32_t)g->m.size();
+  return FZ_OK;
+}
+
+int fz_group_set_branches(fz_group* g, int32_t branches) {
+  if (!g || branches < 0) return fzi::set_global_error(FZ_EINVAL, "fz_group_set_branches: bad arguments");
+  const int rc = fz_group_sync(g, 0);
+  if (rc != FZ_OK) return rc;
+  const int n = (int)g->m.size();
+  assign_branches(g, branches == 0 ? default_branches(n) : std::min(branches, std::min(n, 16)));
+  drop_graphs(g);  // tables follow on the next run (they record the branch count)
   return FZ_OK;
 }
 
@@ -347,9 +468,10 @@ int fz_group_run(fz_group* g, int64_t nsteps) {
       for (fz_handle* h : g->m) h->steps_enqueued += G;
       done += G;
     }
-    for (; done < nsteps; done++) {
-      FZ_GCUDA(g, flat_enqueue(g), "group step launch");
-      for (fz_handle* h : g->m) h->steps_enqueued += 1;
+    if (done < nsteps) {
+      FZ_GCUDA(g, flat_enqueue(g, (int)(nsteps - done)), "group step launch");
+      for (fz_handle* h : g->m) h->steps_enqueued += nsteps - done;
+      done = nsteps;
     }
     return order_after(g, true);  // later work on a member (fz_sync, fz_get_ir, fz_run) follows
   }
@@ -401,11 +523,7 @@ int fz_group_autotune(fz_group* g, int32_t reps, int32_t* kz_chunk, double* ms_p
     hooks.round = [g](int nrep) -> cudaError_t {
       auto it = g->tables.find(parity_key(g));
       if (it == g->tables.end()) return cudaErrorInvalidValue;
-      for (int r = 0; r < nrep; r++) {
-        const cudaError_t e = g->fp64 ? flat_stage_kernels<double>(g, it->second) : flat_stage_kernels<float>(g, it->second);
-        if (e != cudaSuccess) return e;
-      }
-      return cudaSuccess;
+      return g->fp64 ? flat_stage_kernels<double>(g, it->second, nrep) : flat_stage_kernels<float>(g, it->second, nrep);
     };
     rc = fzi::tune(g->m, g->stream, cand, reps, &best, ms_per_step, &hooks);
   } else {

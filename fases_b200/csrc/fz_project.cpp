@@ -512,7 +512,10 @@ int fz_load_project(const char* scene_path, const char* config_path, const char*
       int64_t frames = std::min<int64_t>(wanted, std::max<int64_t>(1, (int64_t)(fr / 4) / per_frame));
       frames = std::min<int64_t>(frames, Nt);
       const int64_t anim_step = std::max<int64_t>(1, Nt / std::max<int64_t>(frames, 1));
-      frames = Nt / anim_step;
+      // the time loop writes a frame at every step index n < Nt that anim_step divides
+      // (main3D.cu:1337, 1393): ceil(Nt / anim_step) of them, one more than Nt / anim_step when
+      // anim_step does not divide Nt
+      frames = (Nt + anim_step - 1) / anim_step;
       rc = fz_set_slices(H, si, sj, sk, anim_step, frames);
     }
   }

@@ -410,9 +410,19 @@ class Group:
 
     def shared_launches(self):
         """True when the members share their launches."""
-        v = C.c_int32()
-        check(lib().fz_group_info(self._g, C.byref(v)))
+        v, b = C.c_int32(), C.c_int32()
+        check(lib().fz_group_info(self._g, C.byref(v), C.byref(b)))
         return bool(v.value)
+
+    def branches(self):
+        """Concurrent branches the group's launches run as."""
+        v, b = C.c_int32(), C.c_int32()
+        check(lib().fz_group_info(self._g, C.byref(v), C.byref(b)))
+        return b.value
+
+    def set_branches(self, n):
+        """Concurrent branches of the shared launches (0 = the default)."""
+        check(lib().fz_group_set_branches(self._g, int(n)))
 
     def run(self, nsteps, sync=True, timeout_ms=0):
         check(lib().fz_group_run(self._g, int(nsteps)))

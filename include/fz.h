@@ -236,8 +236,13 @@ int fz_group_run_timed(fz_group* g, int64_t nsteps, double* ms);
 int fz_group_sync(fz_group* g, int64_t timeout_ms);
 void fz_group_destroy(fz_group* g);
 /* *shared = 1 when the group steps its members with shared launches (above), 0 when each
- * member's own launches run as graph branches. */
-int fz_group_info(fz_group* g, int32_t* shared);
+ * member's own launches run as graph branches; *branches (may be NULL) gets the number of
+ * concurrent branches: shared launches run as branches of rooms of about equal cells (one stream
+ * each), so that one branch's band and receiver launches overlap another's stage launches. */
+int fz_group_info(fz_group* g, int32_t* shared, int32_t* branches);
+/* Sets the number of concurrent branches of the shared launches (1 .. min(n, 16); 0 = the default:
+ * 4 for 16 rooms or more, 2 for 4 or more, else 1). Results do not depend on it. */
+int fz_group_set_branches(fz_group* g, int32_t branches);
 
 /* Launch-shape autotuner. A stage-kernel CTA covers 32 x 16 columns by one z chunk of planes;
  * the chunk lengths set how many CTAs a stage launches and how whole waves of SMs fill. fz_autotune

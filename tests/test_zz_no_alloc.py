@@ -67,9 +67,11 @@ def test_noalloc_energy_ragged_many_blocks_and_empty():
     rho, c = 1.2, 343.0
     g = torch.Generator(device="cuda").manual_seed(5)
     for n in (3 * 16384 + 5, 1, 0):
-        fields = [torch.randn(max(n, 1), generator=g, device="cuda", dtype=torch.float32)[:n] for _ in range(4)]
+        # at least one element of storage each, so that the pointers are valid (never NULL) at n = 0
+        store = [torch.randn(max(n, 1), generator=g, device="cuda", dtype=torch.float32) for _ in range(4)]
+        fields = [t[:n] for t in store]
         out = torch.full((1,), -1.0, dtype=torch.float64, device="cuda")
-        ptrs = [t.data_ptr() for t in fields]  # views of one-element storage when n = 0: never NULL
+        ptrs = [t.data_ptr() for t in store]
         assert all(ptrs)
         rc = L.fz_energy_noalloc(*ptrs, n, rho, c, out.data_ptr(), stream.cuda_stream)
         assert rc == _abi.FZ_OK, _abi.last_error()
