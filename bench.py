@@ -464,10 +464,19 @@ def run_batched(args):
         solo.prepare()
         ms_seq += solo.run_timed(steps_b)
     grp = Group([g for _, g in solvers])
-    shared = grp.shared_launches()
-    depth_grp, _ = grp.autotune()
+    depth_grp, _ = grp.autotune()  # tile depth and launch arrangement
+    shared, branches = grp.shared_launches(), grp.branches()
     grp.run(10)  # the group's step graphs, outside the timed steps
     ms_grp = grp.run_timed(steps_b)
+    # the arrangements the tuner did not keep, on a bounded number of steps (members keep running:
+    # their traces beyond the first steps_b steps are not compared)
+    arrangements = {}
+    n_alt = min(steps_b, 1000)
+    for mode in (-1, 1, 4):
+        grp.set_branches(mode)
+        grp.run(10)
+        arrangements["member_branches" if mode < 0 else f"shared_{mode}_branches"] = \
+            cells_b * n_alt / (grp.run_timed(n_alt) / 1e3) / 1e9
     same = all(np.array_equal(solo.ir(), g.ir()) for solo, g in solvers)
     grp.close()
     for solo, g in solvers:
@@ -478,7 +487,8 @@ def run_batched(args):
         "value": cells_b * steps_b / (ms_grp / 1e3) / 1e9, "unit": UNIT,
         "sequential_value": cells_b * steps_b / (ms_seq / 1e3) / 1e9, "per_room_speedup": ms_seq / ms_grp,
         "steps": steps_b, "ms_group": ms_grp, "ms_sequential": ms_seq, "members_bitwise_equal_solo": same,
-        "tile_depth_group": depth_grp, "shared_launches": shared,
+        "tile_depth_group": depth_grp, "shared_launches": shared, "branches": branches,
+        "arrangements_gcell_s": arrangements,
         "config": {"workload": "32 shoeboxes, edges uniform in [64, 160] cells (seed 45), 2 rigid obstacles, "
                                "6 ADE walls, cPML face, PCS source, 4 receivers each, FP32",
                    "rooms": rooms, "room_cells_total": cells_b}}

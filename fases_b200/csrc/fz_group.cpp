@@ -51,6 +51,7 @@ struct fz_group {
   // shared launches for all members (3D rooms of one precision, no animation slices, at most
   // FZ_MAX_GROUP); otherwise each member's own launches are branches of the graph
   bool flat = false;
+  bool flat_ok = false;  // the members can share launches
   bool fp64 = false;
   std::map<std::vector<int>, FlatTables> tables;
   // shared launches run as `nbranch` concurrent branches (streams), each over a set of members of
@@ -123,6 +124,16 @@ void assign_branches(fz_group* g, int nbranch) {
     load[(size_t)b] += cells(q);
   }
   g->nbranch = nbranch;
+}
+
+// The launch arrangement: -1 each member's own launches as graph branches; 0 the default (shared
+// launches in default_branches() branches where the members can share launches); b >= 1 shared
+// launches in b branches.
+void set_mode(fz_group* g, int mode) {
+  const int n = (int)g->m.size();
+  if (mode == 0) mode = g->flat_ok ? default_branches(n) : -1;
+  g->flat = g->flat_ok && mode > 0;
+  assign_branches(g, g->flat ? std::min(mode, std::min(n, 16)) : 1);
 }
 
 // Streams and join events of the branches (the group stream is branch 0's).
@@ -404,10 +415,10 @@ int fz_group_create(fz_handle* const* members, int32_t n, fz_group** out) {
   g->m.assign(members, members + n);
   g->device = members[0]->device;
   g->fp64 = members[0]->fp64;
-  g->flat = n <= fz::FZ_MAX_GROUP;
+  g->flat_ok = n <= fz::FZ_MAX_GROUP;
   for (fz_handle* h : g->m)
-    if (h->fp64 != g->fp64 || h->prm.two_d || h->sl_on) g->flat = false;
-  assign_branches(g, default_branches(n));
+    if (h->fp64 != g->fp64 || h->prm.two_d || h->sl_on) g->flat_ok = false;
+  set_mode(g, 0);
   g->bstream.push_back(nullptr);  // branch 0 runs on the group stream
   g->bjoin.push_back(nullptr);
   cudaSetDevice(g->device);
@@ -433,11 +444,13 @@ int fz_group_info(fz_group* g, int32_t* shared, int32_t* branches) {
 }
 
 int fz_group_set_branches(fz_group* g, int32_t branches) {
-  if (!g || branches < 0) return fzi::set_global_error(FZ_EINVAL, "fz_group_set_branches: bad arguments");
+  if (!g || branches < -1) return fzi::set_global_error(FZ_EINVAL, "fz_group_set_branches: bad arguments");
+  if (branches > 0 && !g->flat_ok)
+    return fzi::set_global_error(FZ_EINVAL, "fz_group_set_branches: these members cannot share launches "
+                                            "(2D rooms, animation slices, mixed precision or more than 64)");
   const int rc = fz_group_sync(g, 0);
   if (rc != FZ_OK) return rc;
-  const int n = (int)g->m.size();
-  assign_branches(g, branches == 0 ? default_branches(n) : std::min(branches, std::min(n, 16)));
+  set_mode(g, branches);
   drop_graphs(g);  // tables follow on the next run (they record the branch count)
   return FZ_OK;
 }
@@ -515,23 +528,50 @@ int fz_group_autotune(fz_group* g, int32_t reps, int32_t* kz_chunk, double* ms_p
   std::vector<fzi::ZPlan> cand{{0, 0}};
   for (int c : {4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256})
     if (c <= nzmax) cand.push_back({c, 0});
+  // the launch arrangements worth timing: each member's own launches side by side (-1) and, where
+  // the members can share launches, shared launches in 1, 2, 4 or 8 branches
+  std::vector<int> modes{-1};
+  if (g->flat_ok)
+    for (int b : {1, 2, 4, 8})
+      if (b <= (int)g->m.size()) modes.push_back(b);
   fzi::ZPlan best{0, 0};
-  if (g->flat) {
-    // trials of the flat path: the three one-launch stage kernels of all members
-    fzi::TuneHooks hooks;
-    hooks.on_plan = [g]() { return ensure_flat_tables(g); };
-    hooks.round = [g](int nrep) -> cudaError_t {
-      auto it = g->tables.find(parity_key(g));
-      if (it == g->tables.end()) return cudaErrorInvalidValue;
-      return g->fp64 ? flat_stage_kernels<double>(g, it->second, nrep) : flat_stage_kernels<float>(g, it->second, nrep);
-    };
-    rc = fzi::tune(g->m, g->stream, cand, reps, &best, ms_per_step, &hooks);
-  } else {
-    rc = fzi::tune(g->m, g->stream, cand, reps, &best, ms_per_step);
+  int best_mode = -1;
+  double best_ms = -1.0;
+  for (int mode : modes) {
+    set_mode(g, mode);
+    fzi::ZPlan b{0, 0};
+    double ms = 0.0;
+    if (g->flat) {
+      // trials of the shared path: the stage launches of all members, on the branches
+      fzi::TuneHooks hooks;
+      hooks.on_plan = [g]() { return ensure_flat_tables(g); };
+      hooks.round = [g](int nrep) -> cudaError_t {
+        auto it = g->tables.find(parity_key(g));
+        if (it == g->tables.end()) return cudaErrorInvalidValue;
+        return g->fp64 ? flat_stage_kernels<double>(g, it->second, nrep) : flat_stage_kernels<float>(g, it->second, nrep);
+      };
+      rc = fzi::tune(g->m, g->stream, cand, reps, &b, &ms, &hooks);
+    } else {
+      rc = fzi::tune(g->m, g->stream, cand, reps, &b, &ms);
+    }
+    if (rc != FZ_OK) break;
+    if (best_ms < 0.0 || ms < best_ms) {
+      best_ms = ms;
+      best = b;
+      best_mode = mode;
+    }
+  }
+  if (rc == FZ_OK) {
+    set_mode(g, best_mode);
+    for (fz_handle* h : g->m) {
+      rc = fzi::apply_z_plan(h, best);
+      if (rc != FZ_OK) break;
+    }
   }
   drop_graphs(g);  // captured with the old launch shape
   if (rc != FZ_OK) return rc;
   if (kz_chunk) *kz_chunk = best.depth;
+  if (ms_per_step) *ms_per_step = best_ms;
   return FZ_OK;
 }
 

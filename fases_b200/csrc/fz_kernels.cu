@@ -258,6 +258,9 @@ __device__ __forceinline__ void stage_body(const StageArgs<R>& A, const StageMap
 
   // cPML membership of this column along x and y (fixed during the march)
   const bool pml_xy = A.pml_on && valid && (A.pcx[i].tile >= 0 || A.pcy[j].tile >= 0);
+  // z layers sit at the two ends of a member's planes, so a chunk reaches one only through its
+  // first or last plane: chunks that do not skip the per-plane table read
+  const bool pml_zc = A.pml_on && fz_inb(A.err, ke - 1, A.npc[2]) && (A.pcz[kb].tile >= 0 || A.pcz[ke - 1].tile >= 0);
   int buf = 0;
   uint32_t parity = 0;
   int64_t gk = col + plane * kb;  // offset of (i, j, k)
@@ -399,7 +402,7 @@ __device__ __forceinline__ void stage_body(const StageArgs<R>& A, const StageMap
           vn = bv + wb * ((v_in + A.dt_h * Ly.y) - bv);
           wn = bw + wb * ((w_in + A.dt_h * Lz.y) - bw);
         }
-        if (pml_xy || (A.pml_on && fz_inb(A.err, k, A.npc[2]) && A.pcz[k].tile >= 0)) {
+        if (pml_xy || (pml_zc && fz_inb(A.err, k, A.npc[2]) && A.pcz[k].tile >= 0)) {
           // cPML (functions3D.cuh:725-755): field += w dt ((1/kappa - 1) D + psi), psi frozen
           // within the step and advanced once, in stage 2, by recursive convolution.
           const PmlCoef<R> cx = A.pcx[i], cy = A.pcy[j], cz = A.pcz[k];

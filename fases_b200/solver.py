@@ -421,7 +421,8 @@ class Group:
         return b.value
 
     def set_branches(self, n):
-        """Concurrent branches of the shared launches (0 = the default)."""
+        """Launch arrangement: n >= 1 shared launches in n concurrent branches, -1 each member's own
+        launches as graph branches, 0 the default."""
         check(lib().fz_group_set_branches(self._g, int(n)))
 
     def run(self, nsteps, sync=True, timeout_ms=0):
@@ -435,8 +436,9 @@ class Group:
         return ms.value
 
     def autotune(self, reps=3):
-        """One tile depth for every member, timed on the group's own stage launches (0 = each
-        member's own heuristic); returns (depth, stage ms per step of the group)."""
+        """One tile depth for every member and the launch arrangement (shared launches in 1, 2, 4
+        or 8 branches, or each member's own launches), timed on the stage kernels; keeps the
+        fastest and returns (depth, stage ms per step of the group)."""
         k, ms = C.c_int32(), C.c_double()
         check(lib().fz_group_autotune(self._g, int(reps), C.byref(k), C.byref(ms)))
         return k.value, ms.value

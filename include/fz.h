@@ -240,8 +240,11 @@ void fz_group_destroy(fz_group* g);
  * concurrent branches: shared launches run as branches of rooms of about equal cells (one stream
  * each), so that one branch's band and receiver launches overlap another's stage launches. */
 int fz_group_info(fz_group* g, int32_t* shared, int32_t* branches);
-/* Sets the number of concurrent branches of the shared launches (1 .. min(n, 16); 0 = the default:
- * 4 for 16 rooms or more, 2 for 4 or more, else 1). Results do not depend on it. */
+/* Sets the launch arrangement: branches >= 1: shared launches in that many concurrent branches (at
+ * most min(n, 16)); -1: each member's own launches as graph branches; 0: the default (shared
+ * launches in 4 branches for 16 rooms or more, 2 for 4 or more, else 1, where the members can share
+ * launches). fz_group_autotune times the arrangements with the tile depths and keeps the fastest.
+ * Results do not depend on it. */
 int fz_group_set_branches(fz_group* g, int32_t branches);
 
 /* Launch-shape autotuner. A stage-kernel CTA covers 32 x 16 columns by one z chunk of planes;

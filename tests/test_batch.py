@@ -187,10 +187,13 @@ def test_group_larger_than_one_stage_launch_equals_solo_runs():
     members = [_solver(c, "fp32", src_rows=src, p0=c["p0"]) for c in cfgs]
     with Group(members) as g:
         assert g.shared_launches() and g.branches() == 4  # the default for 30 rooms
-        g.run(6)
-        g.set_branches(1)  # the branch count changes the launch order, not the results
+        g.run(4)
+        g.set_branches(1)  # the launch arrangement changes the launch order, not the results
         assert g.branches() == 1
-        g.run(steps - 6)
+        g.run(4)
+        g.set_branches(-1)  # each member's own launches as graph branches
+        assert not g.shared_launches() and g.branches() == 30
+        g.run(steps - 8)
         for s, ref in zip(members, solos):
             assert np.array_equal(s.ir(), ref)
     for s in members:
