@@ -301,16 +301,37 @@ cudaError_t flat_stage_launches(fz_group* g, const FlatBranch& fb, int st, cudaS
   return cudaSuccess;
 }
 
-// The three stage kernels of every member for the current roles (the autotuner's trial of the
-// shared-launch path), n times, on the branches.
+// The stage and band kernels of every member for the current roles, n times, on the branches: the
+// autotuner's trial of the shared-launch path. The band kernels write only band cells of the stage
+// outputs and the ADE sets the next real step writes before it reads them, so a trial changes
+// nothing the solve goes on from (the tuner restores the rest).
 template <class R>
-cudaError_t flat_stage_kernels(fz_group* g, const FlatTables& t, int n) {
+cudaError_t flat_trial_kernels(fz_group* g, const FlatTables& t, int n) {
   cudaError_t e = branches_fork(g);
-  for (int b = 0; b < g->nbranch && e == cudaSuccess; b++)
+  for (int b = 0; b < g->nbranch && e == cudaSuccess; b++) {
+    const FlatBranch& fb = t.br[(size_t)b];
+    const fz::GroupBandArgs<R>* gb = reinterpret_cast<const fz::GroupBandArgs<R>*>(fb.gband.data());
     for (int r = 0; r < n && e == cudaSuccess; r++)
-      for (int st = 0; st < 3 && e == cudaSuccess; st++)
-        e = flat_stage_launches<R>(g, t.br[(size_t)b], st, branch_stream(g, b));
+      for (int st = 0; st < 3 && e == cudaSuccess; st++) {
+        e = flat_stage_launches<R>(g, fb, st, branch_stream(g, b));
+        if (e == cudaSuccess) e = fz::launch_band_group<R>(st, gb[st], fb.band_blocks, fb.band_fit, branch_stream(g, b));
+      }
+  }
   if (e == cudaSuccess) e = branches_join(g);
+  return e;
+}
+
+// The same trial for each member's own launches, side by side on the members' streams.
+cudaError_t member_trial_kernels(fz_group* g, int n) {
+  cudaError_t e = cudaEventRecord(g->fork, g->stream);
+  for (size_t q = 0; q < g->m.size() && e == cudaSuccess; q++) {
+    fz_handle* h = g->m[q];
+    e = cudaStreamWaitEvent(h->stream, g->fork, 0);
+    for (int r = 0; r < n && e == cudaSuccess; r++)
+      for (int st = 0; st < 3 && e == cudaSuccess; st++) e = fzi::enqueue_stage(h, st);
+    if (e == cudaSuccess) e = cudaEventRecord(g->join[q], h->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(g->stream, g->join[q], 0);
+  }
   return e;
 }
 
@@ -541,19 +562,20 @@ int fz_group_autotune(fz_group* g, int32_t reps, int32_t* kz_chunk, double* ms_p
     set_mode(g, mode);
     fzi::ZPlan b{0, 0};
     double ms = 0.0;
+    // trials: the stage and band kernels of every member in this arrangement (the overlap of one
+    // room's band kernels with another's stage kernels is what tells the arrangements apart)
+    fzi::TuneHooks hooks;
     if (g->flat) {
-      // trials of the shared path: the stage launches of all members, on the branches
-      fzi::TuneHooks hooks;
       hooks.on_plan = [g]() { return ensure_flat_tables(g); };
       hooks.round = [g](int nrep) -> cudaError_t {
         auto it = g->tables.find(parity_key(g));
         if (it == g->tables.end()) return cudaErrorInvalidValue;
-        return g->fp64 ? flat_stage_kernels<double>(g, it->second, nrep) : flat_stage_kernels<float>(g, it->second, nrep);
+        return g->fp64 ? flat_trial_kernels<double>(g, it->second, nrep) : flat_trial_kernels<float>(g, it->second, nrep);
       };
-      rc = fzi::tune(g->m, g->stream, cand, reps, &b, &ms, &hooks);
     } else {
-      rc = fzi::tune(g->m, g->stream, cand, reps, &b, &ms);
+      hooks.round = [g](int nrep) { return member_trial_kernels(g, nrep); };
     }
+    rc = fzi::tune(g->m, g->stream, cand, reps, &b, &ms, &hooks);
     if (rc != FZ_OK) break;
     if (best_ms < 0.0 || ms < best_ms) {
       best_ms = ms;
