@@ -63,6 +63,26 @@ def test_graph_and_direct_launches_agree():
         assert np.array_equal(x, y)
 
 
+def test_prepared_graphs_give_the_same_solve():
+    """fz_prepare instantiates the step graphs of both buffer parities without stepping: the solve
+    after it (an odd first run, so both graphs are used) equals one that captured its graphs on
+    the way, and preparing again after a tuning pass changes nothing either."""
+    cfg = small_room(seed=14, steps=35)
+    a = run_gpu(cfg, "fp32", run=False)
+    a.prepare()
+    assert a.steps_done() == 0
+    a.run(5)
+    a.autotune(reps=1)
+    a.prepare()
+    a.run(30)
+    b = run_gpu(cfg, "fp32")
+    assert np.array_equal(a.ir(), b.ir())
+    for x, y in zip(a.fields(), b.fields()):
+        assert np.array_equal(x, y)
+    a.close()
+    b.close()
+
+
 def test_no_pml_no_source_pulse_only():
     cfg = small_room(seed=5, pml=(0, 0, 0, 0, 0, 0), source=None, steps=40)
     s = run_gpu(cfg, "fp64")
