@@ -204,15 +204,14 @@ __device__ __forceinline__ void stage_body(const StageArgs<R>& A, const StageMap
     tma_load_3d(clsb(b), &M.cls, &mbar[b], tma_x + HX, j0, z);
   };
   // Error path of a wait that ran out: every thread leaves through the same exit after the
-  // block-wide barrier; thread 0 first waits (bounded, drain_ring) for the copies this block still
+  // block-wide barrier (which ORs the threads' failures); thread 0 first waits (bounded, drain_ring) for the copies this block still
   // has in flight -- plane it_fail (if it was issued) and plane it_fail + 1 (issued one iteration
   // earlier; plane it_fail + 2 is issued only after the abort check) -- so that no copy lands in
   // shared memory after the block has gone. If that wait runs out as well, the block exits
   // anyway and the error word already says that the results are invalid.
-  __shared__ int s_abort;
-
 #if defined(FZ_V_SPLITBAR)
   __shared__ __align__(8) uint64_t cbar[2];  // centre buffers: one arrival per warp
+  __shared__ int s_abort;
 #endif
   if (lt == 0) {
     for (int b = 0; b < NBUF; ++b) mbar_init(&mbar[b], 1);
@@ -221,7 +220,9 @@ __device__ __forceinline__ void stage_body(const StageArgs<R>& A, const StageMap
     mbar_init(&cbar[1], NTHREADS / 32);
 #endif
     fence_mbar_init();
+#if defined(FZ_V_SPLITBAR)
     s_abort = 0;
+#endif
   }
   __syncthreads();
   if (lt == 0) {
@@ -232,9 +233,11 @@ __device__ __forceinline__ void stage_body(const StageArgs<R>& A, const StageMap
   const P kA = pmk(A.frc2, A.firho);
   const P kC = psplat<R>(-A.fc);
 
+  // z-queue loads: a column outside the grid (a ragged tile edge) reads the grid's last column
+  // instead, so the loads need no test; such a thread stores nothing
+  const int64_t colz = col_ok ? col : (XOFF + (int64_t)min(i, A.Nx - 1) + Sx * (int64_t)min(j, A.Ny - 1));
   auto ld_pw = [&](int kk) -> P {
-    if (!col_ok) return psplat<R>(R(0));
-    const int64_t g = col + plane * kk;
+    const int64_t g = colz + plane * kk;
     if (!fz_inb(A.err, g, A.nfield)) return psplat<R>(R(0));
     return pmk(A.pi[g], A.wi[g]);
   };
@@ -264,7 +267,8 @@ __device__ __forceinline__ void stage_body(const StageArgs<R>& A, const StageMap
   int buf = 0;
   uint32_t parity = 0;
   int64_t gk = col + plane * kb;  // offset of (i, j, k)
-  for (int it = 0; it < nplanes; ++it, gk += plane) {
+  int64_t gz = colz + plane * (kb + 4);  // z-queue load of the next iteration (plane k + 4)
+  for (int it = 0; it < nplanes; ++it, gk += plane, gz += plane) {
     const int k = kb + it;
     P* XCm = reinterpret_cast<P*>(cbase + (it & 1) * (2 * L::XC + 2 * L::YC));
     P* XCp = XCm + TY * (TX + 2);
@@ -275,7 +279,7 @@ __device__ __forceinline__ void stage_body(const StageArgs<R>& A, const StageMap
     const P qe = qe_next;
     P vmC = zero, Fz_hi = zero;
     if (!DIM2) {
-      if (it + 1 < nplanes) qe_next = ld_pw(k + 4);
+      if (it + 1 < nplanes && fz_inb(A.err, gz, A.nfield)) qe_next = pmk(A.pi[gz], A.wi[gz]);
 #if !defined(FZ_V_ZAFTER) && !defined(FZ_V_SPLITBAR)
       // ---- z: centre k+1 -> flux through face k+1/2
       P vpC;
@@ -285,9 +289,13 @@ __device__ __forceinline__ void stage_body(const StageArgs<R>& A, const StageMap
     }
 
     // ---- plane k tile
+    bool wait_failed = false;  // the block leaves after the barrier below; the tile is not stored
     if (!mbar_wait_bounded(&mbar[buf], parity)) {
       atomicOr(A.err, KERR_TMA_TIMEOUT);
-      s_abort = 1;  // the block leaves after the barrier below; the tile is not used for stores
+      wait_failed = true;
+#if defined(FZ_V_SPLITBAR)
+      s_abort = 1;
+#endif
     }
     const R* Tp = field(buf, 0);
     const R* Tu = field(buf, 1);
@@ -350,10 +358,12 @@ __device__ __forceinline__ void stage_body(const StageArgs<R>& A, const StageMap
       atomicOr(A.err, KERR_TMA_TIMEOUT);
       return;
     }
+    const bool abort_block = s_abort != 0;
 #else
-    __syncthreads();
+    // the per-plane barrier, with the OR of the threads' wait failures folded into it
+    const bool abort_block = __syncthreads_or(wait_failed) != 0;
 #endif
-    if (s_abort) {
+    if (abort_block) {
 #ifdef FZ_WAIT_TEST
       if (lt == 0) drain_ring(mbar, it, nplanes, A.test_skip_plane);
 #else
