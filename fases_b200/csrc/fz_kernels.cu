@@ -301,6 +301,11 @@ __device__ __forceinline__ void stage_body(const StageArgs<R>& A, const StageMap
     const R* Tu = field(buf, 1);
     const R* Tv = field(buf, 2);
     const uint8_t cls = clsb(buf)[lt];
+    const bool pml_plane = pml_zc && fz_inb(A.err, k, A.npc[2]) && A.pcz[k].tile >= 0;
+    // a warp whose 32 cells are all plain updates (in the room, no cPML, no source) updates them
+    // after the barrier in one warp-uniform branch, without per-cell tests
+    const bool warp_plain = __all_sync(0xffffffffu, valid && ((cls & (CLS_UPDATE | CLS_SOURCE)) == CLS_UPDATE) &&
+                                                        !pml_xy && !pml_plane && fz_inb(A.err, gk, A.nfield));
 #if defined(FZ_V_ZAFTER)
     if (!DIM2) {
       P vpC;
@@ -377,42 +382,49 @@ __device__ __forceinline__ void stage_body(const StageArgs<R>& A, const StageMap
       issue(it + 2);
     }
 
-    if (valid && (cls & (CLS_UPDATE | CLS_SOURCE)) && fz_inb(A.err, gk, A.nfield)) {
+    // ---- the RK update of this cell before its cPML and source terms: face fluxes and flux
+    //      differences (times h; .x pressure, .y velocity), stage combination
+    auto rk_update = [&](int64_t g, P& Lx, P& Ly, P& Lz, R& pn, R& un, R& vn, R& wn) {
+      Lx = godunov_diff<R>(XCm[ty * (TX + 2) + tx], xp, xm, XCp[ty * (TX + 2) + tx + 2], kA, kC);
+      Ly = godunov_diff<R>(YCm[ty * TX + tx], yp, ym, YCp[(ty + 2) * TX + tx], kA, kC);
+      Lz = psub(Fz_lo, Fz_hi);
+      const R Lp = Lx.x + Ly.x + Lz.x;
+      const int c0 = (ty + HY) * PW + (tx + HX);
+      const R p_in = DIM2 ? Tp[c0] : qb.x, w_in = DIM2 ? A.wi[g] : qb.y;
+      const R u_in = Tu[c0], v_in = Tv[c0];
+      if (STAGE == 0) {
+        pn = p_in + A.dt_h * Lp;
+        un = u_in + A.dt_h * Lx.y;
+        vn = v_in + A.dt_h * Ly.y;
+        wn = w_in + A.dt_h * Lz.y;
+      } else {
+        // the stage combination a U0 + b (U_in + dt L) with a + b = 1, written as
+        // U0 + b ((U_in + dt L) - U0): the weights sum to one exactly. In FP32 the rounded
+        // 1/3 and 2/3 sum to 1 + 3e-8, a gain the whole field would pick up every step (the
+        // reference divides by 3 instead, functions3D.cuh:1311-1314, which is unbiased too).
+        const R bp = own(buf, 0)[lt], bu = own(buf, 1)[lt], bv = own(buf, 2)[lt], bw = own(buf, 3)[lt];
+        const R wb = (STAGE == 1) ? R(0.25) : R(2.0 / 3.0);
+        pn = bp + wb * ((p_in + A.dt_h * Lp) - bp);
+        un = bu + wb * ((u_in + A.dt_h * Lx.y) - bu);
+        vn = bv + wb * ((v_in + A.dt_h * Ly.y) - bv);
+        wn = bw + wb * ((w_in + A.dt_h * Lz.y) - bw);
+      }
+    };
+    if (warp_plain) {
+      P Lx, Ly, Lz;
+      R pn, un, vn, wn;
+      rk_update(gk, Lx, Ly, Lz, pn, un, vn, wn);
+      A.po[gk] = pn;
+      A.uo[gk] = un;
+      A.vo[gk] = vn;
+      A.wo[gk] = wn;
+    } else if (valid && (cls & (CLS_UPDATE | CLS_SOURCE)) && fz_inb(A.err, gk, A.nfield)) {
       const int64_t g = gk;
       if (cls & CLS_UPDATE) {
-        // ---- face fluxes of this cell; flux differences (times h): .x pressure, .y velocity
-        const P Lx = godunov_diff<R>(XCm[ty * (TX + 2) + tx], xp, xm, XCp[ty * (TX + 2) + tx + 2], kA, kC);
-        const P Ly = godunov_diff<R>(YCm[ty * TX + tx], yp, ym, YCp[(ty + 2) * TX + tx], kA, kC);
-        const P Lz = psub(Fz_lo, Fz_hi);
-        const R Lp = Lx.x + Ly.x + Lz.x;
-        const int c0 = (ty + HY) * PW + (tx + HX);
-        const R p_in = DIM2 ? Tp[c0] : qb.x, w_in = DIM2 ? A.wi[g] : qb.y;
-        const R u_in = Tu[c0], v_in = Tv[c0];
+        P Lx, Ly, Lz;
         R pn, un, vn, wn;
-        R bp = R(0), bu = R(0), bv = R(0), bw = R(0);
-        if (STAGE > 0) {
-          bp = own(buf, 0)[lt];
-          bu = own(buf, 1)[lt];
-          bv = own(buf, 2)[lt];
-          bw = own(buf, 3)[lt];
-        }
-        if (STAGE == 0) {
-          pn = p_in + A.dt_h * Lp;
-          un = u_in + A.dt_h * Lx.y;
-          vn = v_in + A.dt_h * Ly.y;
-          wn = w_in + A.dt_h * Lz.y;
-        } else {
-          // the stage combination a U0 + b (U_in + dt L) with a + b = 1, written as
-          // U0 + b ((U_in + dt L) - U0): the weights sum to one exactly. In FP32 the rounded
-          // 1/3 and 2/3 sum to 1 + 3e-8, a gain the whole field would pick up every step (the
-          // reference divides by 3 instead, functions3D.cuh:1311-1314, which is unbiased too).
-          const R wb = (STAGE == 1) ? R(0.25) : R(2.0 / 3.0);
-          pn = bp + wb * ((p_in + A.dt_h * Lp) - bp);
-          un = bu + wb * ((u_in + A.dt_h * Lx.y) - bu);
-          vn = bv + wb * ((v_in + A.dt_h * Ly.y) - bv);
-          wn = bw + wb * ((w_in + A.dt_h * Lz.y) - bw);
-        }
-        if (pml_xy || (pml_zc && fz_inb(A.err, k, A.npc[2]) && A.pcz[k].tile >= 0)) {
+        rk_update(g, Lx, Ly, Lz, pn, un, vn, wn);
+        if (pml_xy || pml_plane) {
           // cPML (functions3D.cuh:725-755): field += w dt ((1/kappa - 1) D + psi), psi frozen
           // within the step and advanced once, in stage 2, by recursive convolution.
           const PmlCoef<R> cx = A.pcx[i], cy = A.pcy[j], cz = A.pcz[k];
