@@ -340,14 +340,32 @@ __device__ __forceinline__ void stage_body(const StageArgs<R>& A, const StageMap
       XCp[slot] = ep;
     } else if (lt >= 32 && lt < 32 + 2 * TX) {
       const int e = lt - 32;
-      const int r = (e < TX) ? -1 : TY;
       const int c = e & (TX - 1);
-      const int c0 = (r + HY) * PW + (c + HX);
       P em, ep;
-      weno_center<R>(pmk(Tp[c0 - 2 * PW], Tv[c0 - 2 * PW]), pmk(Tp[c0 - PW], Tv[c0 - PW]), pmk(Tp[c0], Tv[c0]),
-                     pmk(Tp[c0 + PW], Tv[c0 + PW]), pmk(Tp[c0 + 2 * PW], Tv[c0 + 2 * PW]), em, ep);
-      YCm[(r + 1) * TX + c] = em;
-      YCp[(r + 1) * TX + c] = ep;
+      if constexpr (STAGE == 0 && sizeof(R) == 4) {
+        // the fluxes use only V- of row j0-1 and only V+ of row j0+TY (elsewhere the two-branch
+        // form costs the kernel a register spill, so the other instances compute both faces)
+        if (e < TX) {
+          const int c0 = (HY - 1) * PW + (c + HX);
+          weno_center<R, WENO_LO>(pmk(Tp[c0 - 2 * PW], Tv[c0 - 2 * PW]), pmk(Tp[c0 - PW], Tv[c0 - PW]),
+                                  pmk(Tp[c0], Tv[c0]), pmk(Tp[c0 + PW], Tv[c0 + PW]),
+                                  pmk(Tp[c0 + 2 * PW], Tv[c0 + 2 * PW]), em, ep);
+          YCm[c] = em;
+        } else {
+          const int c0 = (TY + HY) * PW + (c + HX);
+          weno_center<R, WENO_HI>(pmk(Tp[c0 - 2 * PW], Tv[c0 - 2 * PW]), pmk(Tp[c0 - PW], Tv[c0 - PW]),
+                                  pmk(Tp[c0], Tv[c0]), pmk(Tp[c0 + PW], Tv[c0 + PW]),
+                                  pmk(Tp[c0 + 2 * PW], Tv[c0 + 2 * PW]), em, ep);
+          YCp[(TY + 1) * TX + c] = ep;
+        }
+      } else {
+        const int r = (e < TX) ? -1 : TY;
+        const int c0 = (r + HY) * PW + (c + HX);
+        weno_center<R>(pmk(Tp[c0 - 2 * PW], Tv[c0 - 2 * PW]), pmk(Tp[c0 - PW], Tv[c0 - PW]), pmk(Tp[c0], Tv[c0]),
+                       pmk(Tp[c0 + PW], Tv[c0 + PW]), pmk(Tp[c0 + 2 * PW], Tv[c0 + 2 * PW]), em, ep);
+        YCm[(r + 1) * TX + c] = em;
+        YCp[(r + 1) * TX + c] = ep;
+      }
     }
 #if defined(FZ_V_SPLITBAR)
     // split barrier: each warp arrives once its centres are in shared memory, computes the z centre

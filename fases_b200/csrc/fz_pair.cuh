@@ -60,7 +60,10 @@ __device__ __forceinline__ typename Pair<R>::T psplat(R x) {
 //   12/13 beta_r = (second difference)^2 + 3/13 (one-sided first-derivative term)^2
 // (the 12/13 scaling is absorbed into eps).
 // ------------------------------------------------------------------------------------------
-template <class R>
+// FACES selects the face values computed: WENO_BOTH, or only V- (WENO_LO) or V+ (WENO_HI) where a
+// caller uses one of them (the tile's halo rows); the value computed is the same either way.
+constexpr int WENO_LO = 1, WENO_HI = 2, WENO_BOTH = 3;
+template <class R, int FACES = WENO_BOTH>
 __device__ __forceinline__ void weno_core(typename Pair<R>::T a, typename Pair<R>::T b, typename Pair<R>::T c,
                                           typename Pair<R>::T d, typename Pair<R>::T D2, typename Pair<R>::T D1,
                                           typename Pair<R>::T D0, typename Pair<R>::T q0, typename Pair<R>::T& vm,
@@ -91,34 +94,37 @@ __device__ __forceinline__ void weno_core(typename Pair<R>::T a, typename Pair<R
   const P q2w = pfma(tau, prcp(B2), one);
 #endif
   // normalisers: V- uses d = (3/10, 3/5, 1/10), V+ the mirrored (1/10, 3/5, 3/10)
+  constexpr bool LO = (FACES & WENO_LO) != 0, HI = (FACES & WENO_HI) != 0;
   const P t1 = pmul(q1w, psplat<R>(R(0.6)));
-  const P Sm = pfma(q0w, psplat<R>(R(0.3)), pfma(q2w, psplat<R>(R(0.1)), t1));
-  const P Sp = pfma(q0w, psplat<R>(R(0.1)), pfma(q2w, psplat<R>(R(0.3)), t1));
+  P Sm, Sp, em0, ep0, em1, ep1, em2, ep2;
+  if constexpr (LO) Sm = pfma(q0w, psplat<R>(R(0.3)), pfma(q2w, psplat<R>(R(0.1)), t1));
+  if constexpr (HI) Sp = pfma(q0w, psplat<R>(R(0.1)), pfma(q2w, psplat<R>(R(0.3)), t1));
   // d_r * delta_r for both faces, written on the first and second differences:
   //   em0 = 0.15 c - 0.05 D0      ep0 = -0.05 c + D0/30
   //   em1 = 0.15 E1 + 0.05 D1     ep1 = -0.15 E1 + 0.05 D1
   //   em2 = 0.05 b + D2/30        ep2 = -0.15 b - 0.05 D2
   const P h1 = pmul(D1, psplat<R>(R(0.05)));
-  const P em0 = pfma(c, psplat<R>(R(0.15)), pmul(D0, psplat<R>(R(-0.05))));
-  const P ep0 = pfma(c, psplat<R>(R(-0.05)), pmul(D0, psplat<R>(R(1.0 / 30.0))));
-  const P em1 = pfma(E1, psplat<R>(R(0.15)), h1);
-  const P ep1 = pfma(E1, psplat<R>(R(-0.15)), h1);
-  const P em2 = pfma(b, psplat<R>(R(0.05)), pmul(D2, psplat<R>(R(1.0 / 30.0))));
-  const P ep2 = pfma(b, psplat<R>(R(-0.15)), pmul(D2, psplat<R>(R(-0.05))));
-  const P Nm = pfma(q2w, em2, pfma(q1w, em1, pmul(q0w, em0)));
-  const P Np = pfma(q2w, ep2, pfma(q1w, ep1, pmul(q0w, ep0)));
-  vm = pfma(Nm, prcp(Sm), q0);
-  vp = pfma(Np, prcp(Sp), q0);
+  if constexpr (LO) em0 = pfma(c, psplat<R>(R(0.15)), pmul(D0, psplat<R>(R(-0.05))));
+  if constexpr (HI) ep0 = pfma(c, psplat<R>(R(-0.05)), pmul(D0, psplat<R>(R(1.0 / 30.0))));
+  if constexpr (LO) em1 = pfma(E1, psplat<R>(R(0.15)), h1);
+  if constexpr (HI) ep1 = pfma(E1, psplat<R>(R(-0.15)), h1);
+  if constexpr (LO) em2 = pfma(b, psplat<R>(R(0.05)), pmul(D2, psplat<R>(R(1.0 / 30.0))));
+  if constexpr (HI) ep2 = pfma(b, psplat<R>(R(-0.15)), pmul(D2, psplat<R>(R(-0.05))));
+  P Nm, Np;
+  if constexpr (LO) Nm = pfma(q2w, em2, pfma(q1w, em1, pmul(q0w, em0)));
+  if constexpr (HI) Np = pfma(q2w, ep2, pfma(q1w, ep1, pmul(q0w, ep0)));
+  if constexpr (LO) vm = pfma(Nm, prcp(Sm), q0);
+  if constexpr (HI) vp = pfma(Np, prcp(Sp), q0);
 }
 
-template <class R>
+template <class R, int FACES = WENO_BOTH>
 __device__ __forceinline__ void weno_center(typename Pair<R>::T qm2, typename Pair<R>::T qm1,
                                             typename Pair<R>::T q0, typename Pair<R>::T qp1,
                                             typename Pair<R>::T qp2, typename Pair<R>::T& vm,
                                             typename Pair<R>::T& vp) {
   typedef typename Pair<R>::T P;
   const P a = psub(qm1, qm2), b = psub(q0, qm1), c = psub(qp1, q0), d = psub(qp2, qp1);
-  weno_core<R>(a, b, c, d, psub(b, a), psub(c, b), psub(d, c), q0, vm, vp);
+  weno_core<R, FACES>(a, b, c, d, psub(b, a), psub(c, b), psub(d, c), q0, vm, vp);
 }
 
 // Godunov (exact Riemann) flux of linear acoustics for a (pressure, normal velocity) pair
