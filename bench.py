@@ -612,17 +612,30 @@ def main():
     m = b["packed"]
     ne = args.e2e_steps
     t0 = time.perf_counter()
+    phases, t_mark = {}, [t0]
+
+    def mark(name):  # host wall time of each part of the job (the calls below return when done)
+        t = time.perf_counter()
+        phases[name] = round(t - t_mark[0], 4)
+        t_mark[0] = t
+
     prm = params(h=b["h"], c=b["c"], rho=b["rho"], dt=b["dt"], pml=b["pml"], pml_cells=20, precision=args.precision,
                  device=local)
     e = Solver(prm)
+    mark("create")
     e.load_geometry(sc.S, sc.oid)
+    mark("geometry_and_band")
     e.set_materials(m["Rinf"], m["A"], m["zeta"], m["B"], m["Cc"], m["alpha"], m["beta"])
     e.set_receivers(b["receivers"], ne)
     e.set_fields(p=b["p0"])
+    mark("materials_receivers_fields")
     e.autotune()
+    mark("autotune")
     e.run(ne)
     ir = e.ir()
+    mark("steps")
     vel = e.vel()
+    mark("readback")
     t_e2e = time.perf_counter() - t0
     e.close()
     t_e2e = max_over_ranks(pg, t_e2e)
@@ -651,7 +664,7 @@ def main():
     h2d = sc.S.nbytes + sc.oid.nbytes + b["p0"].nbytes + sum(np.asarray(v).nbytes for v in m.values())
     d2h = ir.nbytes + vel.nbytes
     e2e = {"value": world * room_cells * ne / t_e2e / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d / ne,
-           "d2h_bytes_per_step": d2h / ne, "steps": ne, "seconds": t_e2e,
+           "d2h_bytes_per_step": d2h / ne, "steps": ne, "seconds": t_e2e, "phases_s": phases,
            "timer": "host wall clock around create, geometry/material/field upload, autotune, run, IR/VEL readback"}
 
     cpu = None
