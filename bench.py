@@ -164,14 +164,20 @@ class Clocks:
         if self.th:
             self.th.join(timeout=5)
 
-    def summary(self):
+    def summary(self, quarters=False):
         if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
         sm = [r[0] for r in self.rows]
         reasons = sorted({nm for r in self.rows for nm, bit in self.REASONS if r[3] & bit})
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(r[1] for r in self.rows),
-                "sm_mhz_min": min(sm), "power_w_max": max(r[2] for r in self.rows), "reasons": reasons,
-                "samples": len(self.rows), "sampler": self.source}
+        out = {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(r[1] for r in self.rows),
+               "sm_mhz_min": min(sm), "power_w_max": max(r[2] for r in self.rows), "reasons": reasons,
+               "samples": len(self.rows), "sampler": self.source}
+        if quarters and len(self.rows) >= 8:
+            # medians over each quarter of a long run: a drift of clock or power shows here
+            q = np.array_split(np.array([(r[0], r[2]) for r in self.rows]), 4)
+            out["sm_mhz_by_quarter"] = [float(np.median(x[:, 0])) for x in q]
+            out["power_w_by_quarter"] = [round(float(np.median(x[:, 1])), 1) for x in q]
+        return out
 
 
 def workload(room):
@@ -631,8 +637,9 @@ def main():
     mark("materials_receivers_fields")
     e.autotune()
     mark("autotune")
-    e.run(ne)
-    ir = e.ir()
+    with Clocks(local, interval_s=0.05) as clk_e2e:
+        e.run(ne)
+        ir = e.ir()
     mark("steps")
     vel = e.vel()
     mark("readback")
@@ -665,6 +672,7 @@ def main():
     d2h = ir.nbytes + vel.nbytes
     e2e = {"value": world * room_cells * ne / t_e2e / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d / ne,
            "d2h_bytes_per_step": d2h / ne, "steps": ne, "seconds": t_e2e, "phases_s": phases,
+           "clocks": clk_e2e.summary(quarters=True),
            "timer": "host wall clock around create, geometry/material/field upload, autotune, run, IR/VEL readback"}
 
     cpu = None
