@@ -270,7 +270,7 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
   sa.pcz = (const fz::PmlCoef<R>*)h->d_pml_coef[2];
   // launch geometry of the fused stage adjoint: z chunks that fill whole waves, each chunk paying
   // four extra centre planes
-  const int ntx = (h->Nx - 2 * GHOST + fz::TX - 1) / fz::TX, nty = (h->Ny - 2 * GHOST + fz::TY - 1) / fz::TY;
+  const int ntx = (h->Nx - 2 * GHOST + fz::ATX - 1) / fz::ATX, nty = (h->Ny - 2 * GHOST + fz::ATY - 1) / fz::ATY;
   const int nzi = h->Nz - 2 * GHOST;
   const size_t smem_max = fz::adj_stage_smem<R>(nzi);
   FZ_ACUDA(h, fz::adj_stage_setup<R>(smem_max), "adjoint setup");

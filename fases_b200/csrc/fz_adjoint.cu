@@ -129,20 +129,20 @@ __device__ __forceinline__ int64_t psi_index(const AdjStageArgs<R>& A, int d, in
 // its 2-cell halo.
 template <class R>
 struct AdjSmem {
-  static constexpr int TW = TX + 8, TH = TY + 8, TN = TW * TH;
-  static constexpr int GXW = TX + 6, GYH = TY + 6;
-  static constexpr int XCW = TX + 4, YCH = TY + 4;
-  static constexpr int NX_C = XCW * TY, NY_C = TX * YCH;
+  static constexpr int TW = ATX + 8, TH = ATY + 8, TN = TW * TH;
+  static constexpr int GXW = ATX + 6, GYH = ATY + 6;
+  static constexpr int XCW = ATX + 4, YCH = ATY + 4;
+  static constexpr int NX_C = XCW * ATY, NY_C = ATX * YCH;
   static constexpr int RAW = 6 * TN;  // p, u, v, lp, lu, lv of one plane
   static constexpr int G_X = 2 * RAW;
-  static constexpr int G_Y = G_X + 2 * GXW * TY;
-  static constexpr int X_C = G_Y + 2 * TX * GYH;
+  static constexpr int G_Y = G_X + 2 * GXW * ATY;
+  static constexpr int X_C = G_Y + 2 * ATX * GYH;
   static constexpr int Y_C = X_C + 2 * 5 * NX_C;
   static constexpr int END = Y_C + 2 * 5 * NY_C;
   static constexpr size_t CLS_OFF = (size_t)END * sizeof(R);  // two class-byte tiles
   static constexpr size_t PML_OFF = (CLS_OFF + 2 * TN + 31) & ~(size_t)31;
   // cPML coefficients of the tile's x range (38), y range (22) and the chunk's z range (chunk + 6)
-  static size_t bytes(int kz_chunk) { return PML_OFF + (size_t)(TX + 6 + TY + 6 + kz_chunk + 6) * sizeof(PmlCoef<R>); }
+  static size_t bytes(int kz_chunk) { return PML_OFF + (size_t)(ATX + 6 + ATY + 6 + kz_chunk + 6) * sizeof(PmlCoef<R>); }
 };
 
 // Weighted output adjoint of cell (i, j, k) for the flux differences along axis d, as the pair
@@ -181,7 +181,7 @@ __device__ __forceinline__ void adj_g_local(const AdjStageArgs<R>& A, int d, int
 // global loads of the next plane, of the z queues and of the flush are issued at the top of the
 // iteration and consumed after the x/y work.
 template <class R>
-__global__ void __launch_bounds__(NTHREADS, 1) k_adj_stage(const AdjStageArgs<R> A) {
+__global__ void __launch_bounds__(ANTHREADS, 1) k_adj_stage(const AdjStageArgs<R> A) {
   typedef typename Pair<R>::T P;
   typedef AdjSmem<R> S;
   extern __shared__ __align__(16) unsigned char adj_smem[];
@@ -192,11 +192,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_adj_stage(const AdjStageArgs<R>
   P* yC = reinterpret_cast<P*>(sm + S::Y_C);
   uint8_t* clsT = adj_smem + S::CLS_OFF;
   PmlCoef<R>* sPx = reinterpret_cast<PmlCoef<R>*>(adj_smem + S::PML_OFF);  // x = i0 - 3 + q
-  PmlCoef<R>* sPy = sPx + (TX + 6);                                         // y = j0 - 3 + q
-  PmlCoef<R>* sPz = sPy + (TY + 6);                                         // k = kb - 3 + q
+  PmlCoef<R>* sPy = sPx + (ATX + 6);                                         // y = j0 - 3 + q
+  PmlCoef<R>* sPz = sPy + (ATY + 6);                                         // k = kb - 3 + q
 
-  const int tx = threadIdx.x, ty = threadIdx.y, lt = ty * TX + tx;
-  const int i0 = GHOST + blockIdx.x * TX, j0 = GHOST + blockIdx.y * TY;
+  const int tx = threadIdx.x, ty = threadIdx.y, lt = ty * ATX + tx;
+  const int i0 = GHOST + blockIdx.x * ATX, j0 = GHOST + blockIdx.y * ATY;
   const int i = i0 + tx, j = j0 + ty;
   const int kb = GHOST + blockIdx.z * A.kz_chunk;
   const int ke = min(kb + A.kz_chunk, A.Nz - GHOST);
@@ -208,12 +208,12 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_adj_stage(const AdjStageArgs<R>
   const int64_t col = XOFF + i + Sx * (int64_t)j;
 
   // raw-tile elements of this thread: e = lt and e = lt + 512 (when < 960)
-  constexpr int NE = (S::TN + NTHREADS - 1) / NTHREADS;
+  constexpr int NE = (S::TN + ANTHREADS - 1) / ANTHREADS;
   int64_t roff[NE];
   bool rin[NE];
 #pragma unroll
   for (int q = 0; q < NE; q++) {
-    const int e = lt + q * NTHREADS;
+    const int e = lt + q * ANTHREADS;
     const int r = e / S::TW, ci = e - r * S::TW;
     const int x = i0 - 4 + ci, y = j0 - 4 + r;
     rin[q] = (e < S::TN) && x >= 0 && x < Nx && y >= 0 && y < Ny;
@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_adj_stage(const AdjStageArgs<R>
     R* raw = sm + buf * S::RAW;
 #pragma unroll
     for (int q = 0; q < NE; q++) {
-      const int e = lt + q * NTHREADS;
+      const int e = lt + q * ANTHREADS;
       if (e < S::TN) {
 #pragma unroll
         for (int f = 0; f < 6; f++) raw[f * S::TN + e] = pre[q][f];
@@ -261,16 +261,16 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_adj_stage(const AdjStageArgs<R>
     none.tile = -1;
     none.kinv1 = none.b = none.ca = R(0);
     const int nz_t = A.kz_chunk + 6;
-    for (int e = lt; e < TX + 6 + TY + 6 + nz_t; e += NTHREADS) {
+    for (int e = lt; e < ATX + 6 + ATY + 6 + nz_t; e += ANTHREADS) {
       PmlCoef<R> c = none;
-      if (e < TX + 6) {
+      if (e < ATX + 6) {
         const int x = i0 - 3 + e;
         if (x >= 0 && x < Nx) c = A.pcx[x];
-      } else if (e < TX + 6 + TY + 6) {
-        const int y = j0 - 3 + (e - (TX + 6));
+      } else if (e < ATX + 6 + ATY + 6) {
+        const int y = j0 - 3 + (e - (ATX + 6));
         if (y >= 0 && y < Ny) c = A.pcy[y];
       } else {
-        const int k = kb - 3 + (e - (TX + 6 + TY + 6));
+        const int k = kb - 3 + (e - (ATX + 6 + ATY + 6));
         if (k >= 0 && k < Nz) c = A.pcz[k];
       }
       sPx[e] = c;
@@ -344,23 +344,23 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_adj_stage(const AdjStageArgs<R>
       const R* tLu = raw + 4 * S::TN;
       const R* tLv = raw + 5 * S::TN;
       const uint8_t* tC = clsT + (kc & 1) * S::TN;
-      for (int e = lt; e < S::GXW * TY + TX * S::GYH; e += NTHREADS) {
+      for (int e = lt; e < S::GXW * ATY + ATX * S::GYH; e += ANTHREADS) {
         R a, b;
-        if (e < S::GXW * TY) {
+        if (e < S::GXW * ATY) {
           const int r = e / S::GXW, ci = e - r * S::GXW;
           const int t = (r + 4) * S::TW + ci + 1;
           adj_g_local(A, 0, i0 - 3 + ci, j0 + r, kc, tC[t], tLp[t], tLu[t], sPx[ci], a, b);
           gX[e] = pmk(a, b);
         } else {
-          const int f = e - S::GXW * TY;
-          const int r = f / TX, ci = f - r * TX;
+          const int f = e - S::GXW * ATY;
+          const int r = f / ATX, ci = f - r * ATX;
           const int t = (r + 1) * S::TW + ci + 4;
           adj_g_local(A, 1, i0 + ci, j0 - 3 + r, kc, tC[t], tLp[t], tLv[t], sPy[r], a, b);
           gY[f] = pmk(a, b);
         }
       }
       __syncthreads();
-      for (int e = lt; e < S::NX_C + S::NY_C; e += NTHREADS) {
+      for (int e = lt; e < S::NX_C + S::NY_C; e += ANTHREADS) {
         P cc[5];
 #pragma unroll
         for (int q = 0; q < 5; q++) cc[q] = psplat<R>(R(0));
@@ -377,13 +377,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_adj_stage(const AdjStageArgs<R>
           g0 = gX[r * S::GXW + ci + 1];
           gp = gX[r * S::GXW + ci + 2];
         } else {
-          r = f / TX;
-          ci = f - r * TX;
+          r = f / ATX;
+          ci = f - r * ATX;
           cpos = j0 - 2 + r;
           npos = Ny;
-          gm = gY[r * TX + ci];
-          g0 = gY[(r + 1) * TX + ci];
-          gp = gY[(r + 2) * TX + ci];
+          gm = gY[r * ATX + ci];
+          g0 = gY[(r + 1) * ATX + ci];
+          gp = gY[(r + 2) * ATX + ci];
         }
         if (cpos >= 2 && cpos <= npos - 3) {
           // face adjoints: F(c+1/2) enters L(c) with -1 and L(c+1) with +1
@@ -410,7 +410,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_adj_stage(const AdjStageArgs<R>
 #pragma unroll
       for (int q = 0; q < 5; q++) {
         const P a = xC[(ty * S::XCW + tx + 4 - q) * 5 + q];
-        const P b = yC[((ty + 4 - q) * TX + tx) * 5 + q];
+        const P b = yC[((ty + 4 - q) * ATX + tx) * 5 + q];
         xyp += a.x + b.x;
         xyu += a.y;
         xyv += b.y;
@@ -733,12 +733,12 @@ cudaError_t adj_stage_setup(size_t smem_bytes) {
 
 template <class R>
 cudaError_t adj_stage_occupancy(int* blocks_per_sm, size_t smem_bytes) {
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_adj_stage<R>, NTHREADS, smem_bytes);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_adj_stage<R>, ANTHREADS, smem_bytes);
 }
 
 template <class R>
 cudaError_t launch_adj_stage(const AdjStageArgs<R>& a, dim3 grid, cudaStream_t s) {
-  k_adj_stage<R><<<grid, dim3(TX, TY, 1), AdjSmem<R>::bytes(a.kz_chunk), s>>>(a);
+  k_adj_stage<R><<<grid, dim3(ATX, ATY, 1), AdjSmem<R>::bytes(a.kz_chunk), s>>>(a);
   return cudaGetLastError();
 }
 

@@ -13,17 +13,24 @@ namespace fz {
 constexpr int XOFF = 29;
 constexpr int GHOST = 3;
 
-// Stage-kernel tile: 32 x 16 cells per CTA, one thread per (i, j) column, streaming along z.
-constexpr int TX = 32;
+// Stage-kernel tile: 32 x 16 cells per CTA, one thread per (i, j) column, streaming along z
+// (build options FZ_TX = 16 / FZ_TY = 8 select the other measured tile shapes).
+#ifndef FZ_TX
+#define FZ_TX 32
+#endif
 #ifndef FZ_TY
 #define FZ_TY 16
 #endif
+constexpr int TX = FZ_TX;
 constexpr int TY = FZ_TY;
+static_assert(TX == 32 || (TX == 16 && TY % 4 == 0), "stage tile: 32 x TY, or 16 x TY with TY a multiple of 4");
 constexpr int HX = 4;  // x halo held in shared memory (3 needed; 4 keeps rows 16-byte aligned)
 constexpr int HY = 3;  // y halo
 constexpr int PW = TX + 2 * HX;  // 40 tile columns
 constexpr int PH = TY + 2 * HY;  // 22 tile rows
 constexpr int NTHREADS = TX * TY;
+// The adjoint stage kernel's tile (its shared-memory layout and work split are written for it).
+constexpr int ATX = 32, ATY = 16, ANTHREADS = ATX * ATY;
 constexpr int NBUF = 3;  // plane tiles in flight (TMA ring)
 
 // Cell-class bits (one byte per cell, replaces the reference's 4-byte S read per stage).

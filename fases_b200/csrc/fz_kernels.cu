@@ -157,8 +157,20 @@ __device__ __forceinline__ void stage_body(const StageArgs<R>& A, const StageMap
   unsigned char* cbase = smem_raw + L::TILES;
   uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + L::TILES + L::CENTRES);
 
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int lt = ty * TX + tx;
+  const int lt = threadIdx.y * TX + threadIdx.x;  // linear thread index (warps: 32 consecutive)
+  // this thread's column (tx, ty) of the tile. 32-wide tiles: a warp is one row. 16-wide tiles: a
+  // warp takes rows r and r + 2, whose halo-tile rows (24 floats apart x 2) fall in disjoint
+  // halves of the shared-memory banks
+  int tx, ty;
+  if constexpr (TX == 32) {
+    tx = threadIdx.x;
+    ty = threadIdx.y;
+  } else {
+    const int w = lt >> 5, l = lt & 31;
+    tx = l & (TX - 1);
+    ty = 4 * (w >> 1) + (w & 1) + 2 * (l >> 4);
+  }
+  const int lo = ty * TX + tx;  // this cell in the own tiles and the class-byte tile
   const int i0 = GHOST + CTA::x() * TX, j0 = GHOST + CTA::y() * TY;
   const int i = i0 + tx, j = j0 + ty;
   // batch members are stacked along z (member m owns planes [m Nz, (m+1) Nz)); the cPML z table,
@@ -300,7 +312,7 @@ __device__ __forceinline__ void stage_body(const StageArgs<R>& A, const StageMap
     const R* Tp = field(buf, 0);
     const R* Tu = field(buf, 1);
     const R* Tv = field(buf, 2);
-    const uint8_t cls = clsb(buf)[lt];
+    const uint8_t cls = clsb(buf)[lo];
     const bool pml_plane = pml_zc && fz_inb(A.err, k, A.npc[2]) && A.pcz[k].tile >= 0;
     // a warp whose 32 cells are all plain updates (in the room, no cPML, no source) updates them
     // after the barrier in one warp-uniform branch, without per-cell tests
@@ -342,7 +354,7 @@ __device__ __forceinline__ void stage_body(const StageArgs<R>& A, const StageMap
       const int e = lt - 32;
       const int c = e & (TX - 1);
       P em, ep;
-      if constexpr (STAGE == 0 && sizeof(R) == 4) {
+      if constexpr (STAGE == 0 && sizeof(R) == 4 && TX == 32) {  // (16-wide tiles: both rows in one warp)
         // the fluxes use only V- of row j0-1 and only V+ of row j0+TY (elsewhere the two-branch
         // form costs the kernel a register spill, so the other instances compute both faces)
         if (e < TX) {
@@ -420,7 +432,7 @@ __device__ __forceinline__ void stage_body(const StageArgs<R>& A, const StageMap
         // U0 + b ((U_in + dt L) - U0): the weights sum to one exactly. In FP32 the rounded
         // 1/3 and 2/3 sum to 1 + 3e-8, a gain the whole field would pick up every step (the
         // reference divides by 3 instead, functions3D.cuh:1311-1314, which is unbiased too).
-        const R bp = own(buf, 0)[lt], bu = own(buf, 1)[lt], bv = own(buf, 2)[lt], bw = own(buf, 3)[lt];
+        const R bp = own(buf, 0)[lo], bu = own(buf, 1)[lo], bv = own(buf, 2)[lo], bw = own(buf, 3)[lo];
         const R wb = (STAGE == 1) ? R(0.25) : R(2.0 / 3.0);
         pn = bp + wb * ((p_in + A.dt_h * Lp) - bp);
         un = bu + wb * ((u_in + A.dt_h * Lx.y) - bu);
