@@ -179,7 +179,8 @@ __device__ __forceinline__ void adj_g_local(const AdjStageArgs<R>& A, int d, int
 // they land on), the z centre of every column (register queues of p, w and of the z weights),
 // and the flush of plane kc - 2, whose z contributions are complete once centre kc is done. The
 // global loads of the next plane, of the z queues and of the flush are issued at the top of the
-// iteration and consumed after the x/y work.
+// iteration and consumed after the x/y work. Two barriers per plane: after the face weights, and
+// after the centres (which also publishes the next plane's raw tiles, stashed just before it).
 template <class R>
 __global__ void __launch_bounds__(ANTHREADS, 1) k_adj_stage(const AdjStageArgs<R> A) {
   typedef typename Pair<R>::T P;
@@ -294,6 +295,7 @@ __global__ void __launch_bounds__(ANTHREADS, 1) k_adj_stage(const AdjStageArgs<R
 
   prefetch(kb);
   stash(kb & 1);
+  __syncthreads();  // raw tiles of plane kb stashed
 
   const int nit = (ke - kb) + 4;
   for (int it = 0; it < nit; ++it) {
@@ -335,7 +337,6 @@ __global__ void __launch_bounds__(ANTHREADS, 1) k_adj_stage(const AdjStageArgs<R
     // ---- x and y centres of plane kc
     R xyp = R(0), xyu = R(0), xyv = R(0);
     if (xy) {
-      __syncthreads();  // raw tiles of plane kc stashed; previous plane's shared data consumed
       const R* raw = sm + (kc & 1) * S::RAW;
       const R* tP = raw;
       const R* tU = raw + S::TN;
@@ -405,6 +406,11 @@ __global__ void __launch_bounds__(ANTHREADS, 1) k_adj_stage(const AdjStageArgs<R
 #pragma unroll
         for (int q = 0; q < 5; q++) dst[q] = cc[q];
       }
+      // the next plane's raw tiles go into the other buffer (last read before the previous plane's
+      // second barrier); the barrier below publishes them, so the next plane's weights (the first
+      // phase) need no barrier of their own and share a phase with this plane's gather, z centre
+      // and flush
+      if (nxt) stash((kc + 1) & 1);
       __syncthreads();
       // cell (i, j) receives offset q - 2 of the x centre i - (q - 2) and of the y centre j - (q - 2)
 #pragma unroll
@@ -481,8 +487,6 @@ __global__ void __launch_bounds__(ANTHREADS, 1) k_adj_stage(const AdjStageArgs<R
         A.bw[cf] = bq[3];
       }
     }
-    // ---- the next plane's raw tiles (its buffer was last read before this iteration's barriers)
-    if (nxt) stash((kc + 1) & 1);
     // ---- advance the queues
     d2p = d1p; d2u = d1u; d2v = d1v;
     d1p = xyp; d1u = xyu; d1v = xyv;
