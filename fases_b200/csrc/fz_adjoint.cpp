@@ -90,7 +90,7 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
   }
   const int64_t nseg = (nsteps + seg - 1) / seg;
   const size_t state_b = 4 * round256(fb) + ade_sum + psi_sum;
-  const size_t seg_b = (size_t)seg * (3 * 4 * round256(fb) + 4 * ade_sum + (want_pml ? psi_sum : 0));
+  const size_t seg_b = (size_t)seg * (3 * 4 * round256(fb) + 3 * ade_sum + (want_pml ? psi_sum : 0)) + ade_sum;
   const int d = h->prm.pml_cells;
   const size_t extra_b = round256((size_t)std::max(1, nsrc) * 8) * 2 + round256((size_t)std::max(1, nsrc) * std::max<int64_t>(1, n_us) * 8) +
                          round256((size_t)3 * 6 * d * 8);
@@ -119,15 +119,16 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
   std::vector<State> ck((size_t)nseg + 1);
   for (auto& st : ck) take_state(st);
   // per-step storage of one segment: stage inputs U0, U1, U2 and ADE sets phi^n, phi^(1), phi^(2),
-  // phi^{n+1}
+  // phi^{n+1}; phi^n of step t > 0 is phi^{n+1} of step t - 1 (the same array)
   std::vector<void*> S[3];
   std::vector<double*> Ad[4][3];
   std::vector<void*> Ps[3];  // psi^n of every step of the segment (cPML gradient only)
   for (int t = 0; t < seg; t++) {
     for (int q = 0; q < 3; q++)
       for (int f = 0; f < 4; f++) S[q].push_back(ar.take(fb));
-    for (int q = 0; q < 4; q++)
+    for (int q = 1; q < 4; q++)
       for (int a = 0; a < 3; a++) Ad[q][a].push_back((double*)ar.take(ade_b[a]));
+    for (int a = 0; a < 3; a++) Ad[0][a].push_back(t == 0 ? (double*)ar.take(ade_b[a]) : Ad[3][a][(size_t)t - 1]);
     if (want_pml)
       for (int a = 0; a < 3; a++) Ps[a].push_back(psi_b[a] ? ar.take(psi_b[a]) : nullptr);
   }
@@ -150,11 +151,17 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
   double* d_gpml = (double*)ar.take((size_t)3 * 6 * d * 8);
   if (!d_gpml) return fzi::set_error(h, FZ_ENOMEM, "fz_misfit_gradient: arena layout overflow");
 
-  // the handle's own field arrays by set, put back after every recompute
+  // the handle's own field arrays by set and ADE arrays by role slot, put back after every
+  // recompute (which points them at the segment storage)
   void* own[3][4];
   for (int q = 0; q < 3; q++)
     for (int f = 0; f < 4; f++) own[q][f] = h->U[q][f];
+  double* own_ade[3][3];
+  for (int r = 0; r < 3; r++)
+    for (int a = 0; a < 3; a++) own_ade[r][a] = h->d_ade[r][a];
   auto unbind = [&]() -> int {
+    for (int r = 0; r < 3; r++)
+      for (int a = 0; a < 3; a++) h->d_ade[r][a] = own_ade[r][a];
     for (int q = 0; q < 3; q++) {
       const int rc = fzi::bind_field_set(h, q, own[q]);
       if (rc != FZ_OK) return rc;
@@ -335,33 +342,37 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
     FZ_ACUDA(h, restore(ck[(size_t)q], q * seg), "restore");
     // recompute the segment with the stage kernels writing straight into the segment storage
     // (field sets bound to the stored arrays): the step input is S[0][t], stage 0 writes S[1][t],
-    // stage 1 S[2][t], stage 2 the next step's S[0][t+1]; ADE sets are copied
+    // stage 1 S[2][t], stage 2 the next step's S[0][t+1]. Likewise the band kernels' ADE outputs:
+    // the role slots the band arguments name point at Ad[1][t] (stage 0), Ad[2][t] (stage 1) and
+    // Ad[3][t] (stage 2), which the step's role swap makes the next step's input Ad[0][t+1]; only
+    // the segment's first input set (the restored checkpoint) is copied
     {
       cudaError_t e = cudaSuccess;
       for (int f = 0; f < 4 && e == cudaSuccess; f++)
         e = cudaMemcpyAsync(S[0][f], h->U[h->i0][f], fb, cudaMemcpyDeviceToDevice, s);
+      for (int a = 0; a < 3 && e == cudaSuccess; a++)
+        if (ade_b[a]) e = cudaMemcpyAsync(Ad[0][a][0], h->d_ade[h->ph_old][a], ade_b[a], cudaMemcpyDeviceToDevice, s);
       if (e != cudaSuccess) return fzi::cuda_fail(h, e, "adjoint recompute");
     }
     FZ_ARC(fzi::bind_field_set(h, h->i0, &S[0][0]));
+    auto point_ade = [&](int role, int q, int t) {
+      for (int a = 0; a < 3; a++) h->d_ade[role][a] = Ad[q][a][(size_t)t];
+    };
+    point_ade(h->ph_old, 0, 0);
     for (int t = 0; t < len; t++) {
       cudaError_t e = cudaSuccess;
-      for (int a = 0; a < 3 && e == cudaSuccess; a++)
-        if (ade_b[a]) e = cudaMemcpyAsync(Ad[0][a][(size_t)t], h->d_ade[h->ph_old][a], ade_b[a], cudaMemcpyDeviceToDevice, s);
       for (int a = 0; a < 3 && e == cudaSuccess && want_pml; a++)
         if (psi_b[a]) e = cudaMemcpyAsync(Ps[a][(size_t)t], h->d_psi[a], psi_b[a], cudaMemcpyDeviceToDevice, s);
       FZ_ARC(fzi::bind_field_set(h, h->i1, &S[1][(size_t)t * 4]));
+      point_ade(h->ph_cur, 1, t);
       if (e == cudaSuccess) e = fzi::enqueue_stage(h, 0);
-      for (int a = 0; a < 3 && e == cudaSuccess; a++)
-        if (ade_b[a]) e = cudaMemcpyAsync(Ad[1][a][(size_t)t], h->d_ade[h->ph_cur][a], ade_b[a], cudaMemcpyDeviceToDevice, s);
       FZ_ARC(fzi::bind_field_set(h, h->i2, &S[2][(size_t)t * 4]));
+      point_ade(h->ph_nu, 2, t);
       if (e == cudaSuccess) e = fzi::enqueue_stage(h, 1);
-      for (int a = 0; a < 3 && e == cudaSuccess; a++)
-        if (ade_b[a]) e = cudaMemcpyAsync(Ad[2][a][(size_t)t], h->d_ade[h->ph_nu][a], ade_b[a], cudaMemcpyDeviceToDevice, s);
       // the last step's output is the next segment's checkpoint, not stored: a free own set takes it
       FZ_ARC(fzi::bind_field_set(h, h->i1, (t + 1 < len) ? &S[0][(size_t)(t + 1) * 4] : own[0]));
+      point_ade(h->ph_cur, 3, t);
       if (e == cudaSuccess) e = fzi::enqueue_stage(h, 2);
-      for (int a = 0; a < 3 && e == cudaSuccess; a++)
-        if (ade_b[a]) e = cudaMemcpyAsync(Ad[3][a][(size_t)t], h->d_ade[h->ph_cur][a], ade_b[a], cudaMemcpyDeviceToDevice, s);
       if (e == cudaSuccess) e = fzi::enqueue_finish(h);
       if (e != cudaSuccess) {
         unbind();
