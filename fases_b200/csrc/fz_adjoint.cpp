@@ -384,9 +384,8 @@ int misfit_gradient(fz_handle* h, int64_t nsteps, int seg, const double* target,
     fz_range sweep_range("adjoint: reverse sweep of a segment");
     for (int t = len - 1; t >= 0; t--) {
       const int64_t n = q * seg + t;
-      for (int qq : {jO, j1, j2})
-        for (int a = 0; a < 3; a++)
-          if (ade_b[a]) FZ_ACUDA(h, cudaMemsetAsync(lade[qq][a], 0, ade_b[a], s), "memset");
+      // the ADE adjoint sets jO, j1, j2 need no zeroing: the band adjoint's first write to each in a
+      // step assigns (k_adj_band)
       FZ_ACUDA(h, fz::launch_adj_receivers<R>(lam[iA][0], h->d_rec_cell, h->nrec, h->d_ir, h->rec_cap, d_target,
                                                tsteps, n, o.cotangent ? 1 : 0, s), "adjoint receivers");
       const void* const* in_st[3] = {&S[0][(size_t)t * 4], &S[1][(size_t)t * 4], &S[2][(size_t)t * 4]};

@@ -533,6 +533,12 @@ __global__ void __launch_bounds__(256) k_adj_band(const AdjBandArgs<R> B) {
   const R un = uD * nx + vD * ny + wD * nz;
   const double Z0 = B.Z0, dt = B.dt;
   const double wout = (double)pD + Z0 * (double)un;
+  // The ADE-state adjoints of the step (sweep order: stage 2, 1, 0): stage 2 writes the right set
+  // (after stage 1) and the middle set (step start) first, stage 1 its right set (after stage 0)
+  // first, so those writes assign and nothing has to zero the sets between steps; the others add.
+  constexpr bool R_FIRST = STAGE > 0, M_FIRST = STAGE == 2;
+  auto acc_r = [](double& x, double v) { x = R_FIRST ? v : x + v; };
+  auto acc_m = [](double& x, double v) { x = M_FIRST ? v : x + v; };
   constexpr double aa = (STAGE == 0) ? 0.0 : (STAGE == 1) ? 3.0 : 1.0;
   constexpr double bb = (STAGE == 2) ? 2.0 : 1.0;
   constexpr double ic = (STAGE == 0) ? 1.0 : (STAGE == 1) ? 0.25 : 1.0 / 3.0;
@@ -557,8 +563,8 @@ __global__ void __launch_bounds__(256) k_adj_band(const AdjBandArgs<R> B) {
     const double phR = B.phR[si];
     gadd(1 + k, B.phL[si] * lwin);
     gadd(1 + B.K + k, -bb * dt * phR * ic * lphi);
-    B.gphR[si] += bb * (1.0 - dt * B.zeta[mi]) * ic * lphi;
-    if (STAGE > 0) B.gphM[si] += aa * ic * lphi;
+    acc_r(B.gphR[si], bb * (1.0 - dt * B.zeta[mi]) * ic * lphi);
+    if (STAGE > 0) acc_m(B.gphM[si], aa * ic * lphi);
     lwout += bb * dt * ic * lphi;
   }
   const int o = 1 + 2 * B.K;
@@ -574,11 +580,11 @@ __global__ void __launch_bounds__(256) k_adj_band(const AdjBandArgs<R> B) {
     gadd(o + B.L + l, B.s2L[si] * lwin);
     gadd(o + 2 * B.L + l, kd * (-r1 * l1 - r2 * l2));
     gadd(o + 3 * B.L + l, kd * (-r2 * l1 + r1 * l2));
-    B.gs1R[si] += bb * ic * l1 - kd * al * l1 + kd * be * l2;
-    B.gs2R[si] += -kd * be * l1 + bb * ic * l2 - kd * al * l2;
+    acc_r(B.gs1R[si], bb * ic * l1 - kd * al * l1 + kd * be * l2);
+    acc_r(B.gs2R[si], -kd * be * l1 + bb * ic * l2 - kd * al * l2);
     if (STAGE > 0) {
-      B.gs1M[si] += aa * ic * l1;
-      B.gs2M[si] += aa * ic * l2;
+      acc_m(B.gs1M[si], aa * ic * l1);
+      acc_m(B.gs2M[si], aa * ic * l2);
     }
     lwout += kd * l1;
   }
